@@ -1,0 +1,160 @@
+/*
+ * vfv_gpu.h - C ABI of libvfvgpu, the B200 (sm_100a) assemble-and-solve path of vfvchem-vfvm3d.
+ *
+ * Plain C types only: opaque handles, pointers and sizes. Every entry point returns a status code
+ * (VFV_OK = 0); the message of the last failure is vfv_last_error(ctx) (or vfv_last_error(NULL)
+ * for failures before a context exists). No entry point falls back to a CPU implementation: when
+ * no CUDA device is usable, vfv_ctx_create fails with VFV_CUDA_ERROR.
+ *
+ * Reference interfaces replaced (paths are within the vfvchem-vfvm3d project):
+ *   trait LinearBase                      src/linear/linear_base.rs:5-10
+ *     update_sparse  -> vfv_pattern_from_triplets
+ *     build_matrix   -> vfv_values_from_triplets
+ *     solve_matrix   -> vfv_solve / vfv_solve_device
+ *   LinearGmres::new_with_options          src/linear/linear_gmres.rs:24-49  -> vfv_gmres_opts
+ *   trait OperatorBase::apply (heat ops)    src/operator/operator_base.rs:5-7, driven by
+ *   SteadyHeat::assemble_matrix             src/steady/core/steady_heat.rs:143-171 -> vfv_heat_assemble
+ *   ScalarDomain::update_grad               src/base/scl_dom.rs:146-164 -> vfv_update_grad
+ *   Tetrahedron::update_tet (geometry)      src/base/geom_tet.rs:58-350 -> vfv_mesh_* (host, once)
+ *
+ * Threading: a context owns one CUDA stream; calls on one context must not overlap (like the
+ * reference's single-threaded `&mut dyn LinearBase`). Different contexts are independent.
+ */
+#ifndef VFV_GPU_H
+#define VFV_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (a non-zero code maps onto VFVChemError::LinearGmresDidNotConverge or a
+ *      new variant on the Rust side; src/base/error.rs:265-268) */
+#define VFV_OK 0
+#define VFV_NOT_CONVERGED 1 /* max_outer restart cycles without reaching tol */
+#define VFV_NONFINITE 2     /* NaN/Inf in the residual or the Arnoldi process */
+#define VFV_BAD_INPUT 3     /* invalid argument (sizes, indices, options) */
+#define VFV_CUDA_ERROR 4    /* CUDA runtime failure or no device */
+#define VFV_TIMEOUT 5       /* reserved for bounded device waits */
+
+/* ---- preconditioners / precisions / orderings */
+#define VFV_PRECOND_NONE 0
+#define VFV_PRECOND_JACOBI 1 /* the reference's JacobiPreconLinOp (linear_gmres.rs:79) */
+#define VFV_PRECOND_ILU0 2   /* added: ILU(0) on A's pattern */
+#define VFV_FP64 0           /* all Krylov vectors, SpMV and preconditioner in double */
+#define VFV_MIXED 1          /* float inner GMRES cycles inside double iterative refinement */
+#define VFV_ILU_MULTICOLOR 0 /* ILU(0) of the greedy-multicolour permutation (few levels) */
+#define VFV_ILU_NATURAL 1    /* ILU(0) in the given order, level scheduled */
+
+/* ---- boundary-condition kinds of the heat operator (SteadyHeat::add_temp_bnd / add_hflx_bnd) */
+#define VFV_BC_TEMP 0 /* Dirichlet: OpSclBndDirichlet */
+#define VFV_BC_FLUX 1 /* flux: OpSclBndDiffusion + Production + Source + Neumann */
+
+typedef struct vfv_ctx vfv_ctx;
+typedef struct vfv_pattern vfv_pattern;
+typedef struct vfv_mesh vfv_mesh;
+typedef struct vfv_heat vfv_heat;
+
+/* Options of LinearGmres::new_with_options(num_thread, tol, restart, max_outer)
+ * (linear_gmres.rs:24; defaults tol 1e-6, restart 50, max_outer 200 at :20-22).
+ * Convergence: ||b - A x||_2 <= tol * ||b||_2, checked on the true double residual after every
+ * restart cycle; right preconditioning, so the Arnoldi estimate is of the same residual. */
+typedef struct {
+    double tol;
+    int32_t restart;   /* Krylov dimension m, 1 <= m <= 127 */
+    int32_t max_outer; /* maximum number of restart cycles */
+    int32_t precond;   /* VFV_PRECOND_* */
+    int32_t precision; /* VFV_FP64 or VFV_MIXED */
+    int32_t ilu_order; /* VFV_ILU_* (ILU(0) only) */
+    int32_t pad;
+    double inner_rtol; /* VFV_MIXED: an inner cycle also ends once its estimate drops by this factor (0 = full cycles) */
+} vfv_gmres_opts;
+
+typedef struct {
+    int32_t status;   /* VFV_OK / VFV_NOT_CONVERGED / VFV_NONFINITE */
+    int32_t iters;    /* total Arnoldi steps */
+    int32_t cycles;   /* restart (refinement) cycles */
+    int32_t levels;   /* ILU(0) levels of the chosen ordering (0 without ILU) */
+    double relres;    /* final ||b - A x|| / ||b|| (double) */
+    double bnorm;     /* ||b|| */
+} vfv_solve_info;
+
+/* Fills opts with the reference defaults: tol 1e-6, restart 50, max_outer 200, Jacobi, FP64. */
+void vfv_gmres_default_opts(vfv_gmres_opts* opts);
+
+/* ---- context */
+int vfv_ctx_create(int device, vfv_ctx** out);
+void vfv_ctx_destroy(vfv_ctx* ctx);
+const char* vfv_last_error(const vfv_ctx* ctx);
+int vfv_ctx_synchronize(vfv_ctx* ctx);
+/* the context's CUDA stream (cudaStream_t) for callers that enqueue work around the library */
+void* vfv_ctx_stream(vfv_ctx* ctx);
+
+/* ---- sparse pattern: LinearBase::update_sparse (linear_gmres.rs:53-64).
+ * rows/cols[ntrip] are the (row, col) pairs of the triplet list in push order. The pattern is
+ * the sorted, de-duplicated set (explicit zeros kept); a slot map remembers which triplets fall
+ * into each slot so build_matrix sums them in push order. */
+int vfv_pattern_from_triplets(vfv_ctx* ctx, int64_t n, int64_t ntrip, const uint64_t* rows, const uint64_t* cols, vfv_pattern** out);
+/* a pattern given directly as CSR (rowptr[n+1], colind[nnz] ascending per row); no slot map */
+int vfv_pattern_from_csr(vfv_ctx* ctx, int64_t n, const int32_t* rowptr, const int32_t* colind, vfv_pattern** out);
+void vfv_pattern_destroy(vfv_pattern* p);
+int vfv_pattern_info(const vfv_pattern* p, int64_t* n, int64_t* nnz, int64_t* ntrip);
+
+/* ---- values: LinearBase::build_matrix (linear_gmres.rs:66-74); vals[ntrip] in push order (host) */
+int vfv_values_from_triplets(vfv_ctx* ctx, vfv_pattern* p, const double* vals);
+/* values given per CSR slot (host or device pointer) */
+int vfv_values_set(vfv_ctx* ctx, vfv_pattern* p, const double* vals, int on_device);
+/* copy the matrix out (any pointer may be NULL) */
+int vfv_csr_export(vfv_ctx* ctx, const vfv_pattern* p, int32_t* rowptr, int32_t* colind, double* vals);
+
+/* ---- solve: LinearBase::solve_matrix (linear_gmres.rs:76-84). b, x0, x are HOST arrays of
+ * length n; x0 is the warm start (the previous Picard iterate). x may alias x0. */
+int vfv_solve(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* opts,
+              vfv_solve_info* info);
+/* same with DEVICE arrays on the context's device */
+int vfv_solve_device(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* opts,
+                     vfv_solve_info* info);
+/* y = A x (device arrays); SpMV of the solver, exposed for measurement */
+int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double* y);
+/* y = A x with float values/vectors (the mixed-precision inner SpMV); the float copy of the
+ * values is made on first use and refreshed by every vfv_values_* call */
+int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y);
+/* z = M^-1 r for the ILU(0) preconditioner of the pattern's current values (device arrays, double) */
+int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels);
+
+/* ---- mesh (host, once per mesh): jittered unit cube, Delaunay, Voronoi dual */
+int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out);
+/* a mesh from given vertices (points first, then nodes with a boundary id each) */
+int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out);
+void vfv_mesh_destroy(vfv_mesh* m);
+/* counts: vertices split, tetrahedra, directed faces (2 x Voronoi faces), boundary sub-faces */
+int vfv_mesh_info(const vfv_mesh* m, int64_t* n_pts, int64_t* n_nds, int64_t* n_tet, int64_t* n_dir, int64_t* n_bsub);
+/* copy arrays out; any pointer may be NULL. Vector quantities are component-major [3][count]. */
+int vfv_mesh_export(const vfv_mesh* m, double* pos, int32_t* node_bnd, int32_t* tets);
+int vfv_mesh_export_dual(const vfv_mesh* m, int64_t* nbr_ptr, int32_t* nbr_idx, double* dist, double* area, double* norm,
+                         double* skew, double* grad_wgt, double* cvol, double* cskew, int64_t* bnd_ptr, int32_t* bnd_j,
+                         int32_t* bnd_k, double* bnd_area, double* bnd_norm, double* bnd_wgt);
+
+/* ---- steady heat operator on the device (SteadyHeat with one domain, steady_heat.rs:80-171).
+ * bnd_kind[b] is VFV_BC_TEMP or VFV_BC_FLUX for every boundary id used by the mesh nodes. The
+ * matrix pattern is fixed at creation; vfv_heat_pattern returns it (owned by the heat handle). */
+int vfv_heat_create(vfv_ctx* ctx, const vfv_mesh* m, int32_t n_bnd, const int32_t* bnd_kind, vfv_heat** out);
+void vfv_heat_destroy(vfv_heat* h);
+vfv_pattern* vfv_heat_pattern(vfv_heat* h);
+/* Gradients of k (conductivity), q (source), s (production) and T (unknown), then the matrix
+ * values and b. k, q, s, T, bc_val are arrays of n_tot doubles (bc_val: Dirichlet value or outward
+ * flux on nodes, ignored on points); on_device selects device (1) or host (0) pointers. b_out may
+ * be NULL (b stays on the device, see vfv_heat_rhs_device). */
+int vfv_heat_assemble(vfv_ctx* ctx, vfv_heat* h, const double* k, const double* q, const double* s, const double* T,
+                      const double* bc_val, int on_device, double* b_out);
+/* device pointer of the assembled right-hand side (n_tot doubles, owned by h) */
+const double* vfv_heat_rhs_device(vfv_heat* h);
+/* gradient of one field on the heat mesh: grad[3][n_tot] (host arrays) */
+int vfv_update_grad(vfv_ctx* ctx, vfv_heat* h, const double* f, double* grad);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VFV_GPU_H */

@@ -1,0 +1,993 @@
+// C ABI of libvfvgpu: contexts, sparse patterns, the graph-captured GMRES driver, mesh and heat
+// operator handles. Host orchestration only; the kernels live in kernels/*.
+//
+// Reference interfaces mirrored (src/linear/linear_base.rs:5-10, src/linear/linear_gmres.rs:8-85):
+//   update_sparse -> vfv_pattern_from_triplets (sorted de-duplicated pattern + slot map, once)
+//   build_matrix  -> vfv_values_from_triplets  (device scatter summing duplicates in push order)
+//   solve_matrix  -> vfv_solve                 (restarted right-preconditioned GMRES, warm start)
+#include "../../include/vfv_gpu.h"
+#include "common.cuh"
+#include "host/mesh.hpp"
+#include "kernels/assemble.cuh"
+#include "kernels/ilu0.cuh"
+#include "kernels/krylov.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <vector>
+
+using namespace vfv;
+
+// ================================================================ errors / buffers
+static thread_local std::string g_err;
+
+struct vfv_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    DevStatus* h_status = nullptr;  // pinned
+    double* h_scalar = nullptr;     // pinned scratch for small reads
+};
+
+namespace {
+
+int set_err(vfv_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                           \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return set_err(ctx, VFV_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+struct DBuf {  // device buffer, freed with its owner
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(&p, count * sizeof(T));
+    }
+    cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
+        cudaError_t e = alloc(count);
+        if (e != cudaSuccess || count == 0) return e;
+        e = cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return e;
+        return cudaStreamSynchronize(s);
+    }
+};
+
+inline int grid_for(int64_t threads, int block = 256) { return (int)std::max<int64_t>(1, (threads + block - 1) / block); }
+
+// LSD radix sort of (key, index) by key, stable; keys < 2^bits.
+void radix_sort_pairs(std::vector<uint64_t>& key, std::vector<int64_t>& idx, int bits) {
+    const size_t n = key.size();
+    std::vector<uint64_t> k2(n);
+    std::vector<int64_t> i2(n);
+    for (int shift = 0; shift < bits; shift += 16) {
+        std::vector<size_t> cnt(65537, 0);
+        for (size_t i = 0; i < n; ++i) cnt[((key[i] >> shift) & 0xffff) + 1]++;
+        for (int d = 0; d < 65536; ++d) cnt[d + 1] += cnt[d];
+        for (size_t i = 0; i < n; ++i) {
+            const size_t p = cnt[(key[i] >> shift) & 0xffff]++;
+            k2[p] = key[i];
+            i2[p] = idx[i];
+        }
+        key.swap(k2);
+        idx.swap(i2);
+    }
+}
+
+}  // namespace
+
+// ================================================================ ILU structure (host-built)
+struct IluStruct {
+    int order = -1;
+    int nlev = 0;
+    std::vector<int32_t> lev_ptr;  // [nlev+1] row ranges in the permuted numbering
+    DBuf<int32_t> perm, rp, ci, dg, src;
+    DBuf<double> lu64;
+    DBuf<float> lu32;
+    DBuf<int> bad;
+    uint64_t version64 = ~0ull, version32 = ~0ull;
+};
+
+struct SolverBase {
+    virtual ~SolverBase() = default;
+};
+
+struct vfv_pattern {
+    vfv_ctx* ctx = nullptr;
+    int64_t n = 0, nnz = 0, ntrip = 0;
+    std::vector<int32_t> h_rp, h_ci;
+    DBuf<int32_t> rp, ci, diag_pos;
+    DBuf<double> val;
+    DBuf<float> val32;
+    uint64_t version = 0, version32 = ~0ull;
+    DBuf<int64_t> slot_ptr, slot_trip;
+    DBuf<double> trip_vals;
+    std::map<int, std::unique_ptr<IluStruct>> ilu;
+    std::map<std::tuple<int, int, int, int>, std::unique_ptr<SolverBase>> solvers;
+    DBuf<double> tmp_b, tmp_x;  // staging for host-pointer solves
+};
+
+// ================================================================ GMRES driver
+namespace {
+
+int build_ilu_struct(vfv_ctx* ctx, vfv_pattern* p, int order, IluStruct& S) {
+    const int64_t n = p->n;
+    const std::vector<int32_t>& rp = p->h_rp;
+    const std::vector<int32_t>& ci = p->h_ci;
+    // symmetrised adjacency (lower neighbours only are needed for levels / greedy colours)
+    std::vector<std::vector<int32_t>> lower(n);
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const int32_t j = ci[k];
+            if (j < i) lower[i].push_back(j);
+            else if (j > i) lower[j].push_back((int32_t)i);
+        }
+    std::vector<int32_t> lev(n, 0);
+    int nlev = 0;
+    if (order == VFV_ILU_NATURAL) {
+        for (int64_t i = 0; i < n; ++i) {
+            int32_t l = 0;
+            for (int32_t k : lower[i]) l = std::max(l, lev[k] + 1);
+            lev[i] = l;
+            nlev = std::max(nlev, l + 1);
+        }
+    } else {
+        std::vector<int64_t> mark(256, -1);
+        for (int64_t i = 0; i < n; ++i) {
+            for (int32_t k : lower[i]) {
+                if (lev[k] >= (int32_t)mark.size()) mark.resize(lev[k] + 1, -1);
+                mark[lev[k]] = i;
+            }
+            int32_t c = 0;
+            while (c < (int32_t)mark.size() && mark[c] == i) ++c;
+            lev[i] = c;
+            nlev = std::max(nlev, c + 1);
+        }
+    }
+    std::vector<std::vector<int32_t>>().swap(lower);
+    std::vector<int32_t> perm(n), iperm(n);
+    std::vector<int64_t> cnt(nlev + 1, 0);
+    for (int64_t i = 0; i < n; ++i) cnt[lev[i] + 1]++;
+    for (int l = 0; l < nlev; ++l) cnt[l + 1] += cnt[l];
+    S.lev_ptr.assign(cnt.begin(), cnt.end());
+    {
+        std::vector<int64_t> cur(cnt.begin(), cnt.end() - 1);
+        for (int64_t i = 0; i < n; ++i) {
+            const int64_t q = cur[lev[i]]++;
+            perm[q] = (int32_t)i;
+            iperm[i] = (int32_t)q;
+        }
+    }
+    std::vector<int32_t> nrp(n + 1, 0), nci(p->nnz), nsrc(p->nnz), ndg(n, -1);
+    for (int64_t q = 0; q < n; ++q) nrp[q + 1] = nrp[q] + (rp[perm[q] + 1] - rp[perm[q]]);
+    std::vector<std::pair<int32_t, int32_t>> row;
+    for (int64_t q = 0; q < n; ++q) {
+        const int32_t i = perm[q];
+        row.clear();
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) row.push_back({iperm[ci[k]], k});
+        std::sort(row.begin(), row.end());
+        for (size_t t = 0; t < row.size(); ++t) {
+            nci[nrp[q] + t] = row[t].first;
+            nsrc[nrp[q] + t] = row[t].second;
+            if (row[t].first == q) ndg[q] = nrp[q] + (int32_t)t;
+        }
+        if (ndg[q] < 0) return set_err(ctx, VFV_BAD_INPUT, "ILU(0) needs a diagonal entry in every row of the pattern");
+    }
+    cudaStream_t s = ctx->stream;
+    CK(S.perm.upload(perm.data(), n, s));
+    CK(S.rp.upload(nrp.data(), n + 1, s));
+    CK(S.ci.upload(nci.data(), p->nnz, s));
+    CK(S.dg.upload(ndg.data(), n, s));
+    CK(S.src.upload(nsrc.data(), p->nnz, s));
+    CK(S.lu64.alloc(p->nnz));
+    CK(S.bad.alloc(1));
+    S.order = order;
+    S.nlev = nlev;
+    return VFV_OK;
+}
+
+// numeric ILU(0) of the pattern's current values (double), cast to float when asked
+int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
+    cudaStream_t s = ctx->stream;
+    if (S.version64 != p->version) {
+        k_gather_vals<double><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, S.src.p, p->val.p, S.lu64.p);
+        CK(cudaMemsetAsync(S.bad.p, 0, sizeof(int), s));
+        for (int l = 0; l < S.nlev; ++l) {
+            const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
+            k_ilu0_factor_level<<<grid_for(r1 - r0, 128), 128, 0, s>>>(r0, r1, S.rp.p, S.ci.p, S.dg.p, S.lu64.p, S.bad.p);
+        }
+        int bad = 0;
+        CK(cudaMemcpyAsync(&bad, S.bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        CK(cudaGetLastError());
+        if (bad) return set_err(ctx, VFV_NONFINITE, "ILU(0): zero pivot");
+        S.version64 = p->version;
+    }
+    if (want32 && S.version32 != p->version) {
+        if (!S.lu32.p) CK(S.lu32.alloc(p->nnz));
+        k_cast<double, float><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, S.lu64.p, S.lu32.p);
+        S.version32 = p->version;
+    }
+    return VFV_OK;
+}
+
+template <typename T>
+void ilu_apply(cudaStream_t s, const IluStruct& S, const T* lu, const T* in, T* t, T* out, const DevStatus* st) {
+    constexpr int G = 8;
+    for (int l = 0; l < S.nlev; ++l) {
+        const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
+        k_ilu0_lower<T, G><<<grid_for((int64_t)(r1 - r0) * G), 256, 0, s>>>(r0, r1, S.rp.p, S.ci.p, S.dg.p, lu, S.perm.p, in, t, st);
+    }
+    for (int l = S.nlev - 1; l >= 0; --l) {
+        const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
+        k_ilu0_upper<T, G><<<grid_for((int64_t)(r1 - r0) * G), 256, 0, s>>>(r0, r1, S.rp.p, S.ci.p, S.dg.p, lu, S.perm.p, t, out, st);
+    }
+}
+
+template <typename T>
+struct Gmres : SolverBase {
+    int64_t n = 0, ldv = 0;
+    int m = 0, precond = 0, ilu_order = 0;
+    int nblk = 0;
+    DBuf<T> V, z, z2, valK;
+    DBuf<double> part, hacc, coef, H, cs, sn, g, beta, inv_beta, y, dinv, scal, x, b;
+    DBuf<unsigned> counter;
+    DBuf<DevStatus> st;
+    KrylovDev K{};
+    cudaGraphExec_t exec = nullptr;
+    IluStruct* ilu = nullptr;
+    ~Gmres() override {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+
+    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_) {
+        n = p->n;
+        m = m_;
+        precond = precond_;
+        ilu_order = ilu_order_;
+        ldv = (n + 63) / 64 * 64;
+        nblk = (int)((n + kBlk * kRows - 1) / (kBlk * kRows));
+        const int64_t res_blocks = (n * 8 + kBlk - 1) / kBlk;
+        CK(V.alloc((size_t)(m + 1) * ldv));
+        CK(cudaMemset(V.p, 0, sizeof(T) * (size_t)(m + 1) * ldv));
+        if (precond == VFV_PRECOND_ILU0) {
+            CK(z.alloc(n));
+            CK(z2.alloc(n));
+        }
+        CK(part.alloc(std::max<int64_t>((int64_t)kMaxBasis * nblk, res_blocks) + 16));
+        CK(hacc.alloc(kMaxBasis));
+        CK(coef.alloc(kMaxBasis));
+        CK(H.alloc((size_t)m * (m + 1)));
+        CK(cs.alloc(m));
+        CK(sn.alloc(m));
+        CK(g.alloc(m + 1));
+        CK(beta.alloc(m + 1));
+        CK(inv_beta.alloc(m + 1));
+        CK(y.alloc(m));
+        CK(dinv.alloc(n));
+        CK(scal.alloc(4));
+        CK(x.alloc(n));
+        CK(b.alloc(n));
+        CK(counter.alloc(8));
+        CK(cudaMemset(counter.p, 0, 8 * sizeof(unsigned)));
+        CK(st.alloc(1));
+        CK(cudaMemset(st.p, 0, sizeof(DevStatus)));
+        const bool need_copy = (precond == VFV_PRECOND_JACOBI) || !std::is_same<T, double>::value;
+        if (need_copy) CK(valK.alloc(p->nnz));
+        K.n = n;
+        K.ldv = ldv;
+        K.m = m;
+        K.nblk = nblk;
+        K.part = part.p;
+        K.counter = counter.p;
+        K.hacc = hacc.p;
+        K.coef = coef.p;
+        K.H = H.p;
+        K.cs = cs.p;
+        K.sn = sn.p;
+        K.g = g.p;
+        K.beta = beta.p;
+        K.inv_beta = inv_beta.p;
+        K.y = y.p;
+        K.st = st.p;
+        K.scal = scal.p;
+        if (precond == VFV_PRECOND_ILU0) {
+            auto it = p->ilu.find(ilu_order);
+            if (it == p->ilu.end()) {
+                auto S = std::make_unique<IluStruct>();
+                int rc = build_ilu_struct(ctx, p, ilu_order, *S);
+                if (rc) return rc;
+                it = p->ilu.emplace(ilu_order, std::move(S)).first;
+            }
+            ilu = it->second.get();
+        }
+        return VFV_OK;
+    }
+
+    const T* krylov_vals(vfv_pattern* p) const {
+        if (valK.p) return valK.p;
+        return reinterpret_cast<const T*>(p->val.p);
+    }
+    const T* lu_vals() const {
+        if constexpr (std::is_same<T, double>::value) return ilu->lu64.p;
+        else return ilu->lu32.p;
+    }
+
+    // one restart cycle: m Arnoldi steps, least squares, update of x, new residual
+    void enqueue_cycle(cudaStream_t s, vfv_pattern* p) {
+        constexpr int G = 8;
+        const T* vk = krylov_vals(p);
+        const int sp_blocks = grid_for(n * G);
+        for (int j = 0; j < m; ++j) {
+            const T* uj = V.p + (int64_t)j * ldv;
+            T* w = V.p + (int64_t)(j + 1) * ldv;
+            const T* in = uj;
+            if (precond == VFV_PRECOND_ILU0) {
+                ilu_apply<T>(s, *ilu, lu_vals(), uj, z2.p, z.p, st.p);
+                in = z.p;
+            }
+            k_spmv<T, T, T, T, G><<<sp_blocks, kBlk, 0, s>>>(n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
+            k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
+            k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+            k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+        }
+        k_backsolve<<<1, 32, 0, s>>>(K);
+        const int vb = grid_for(n);
+        if (precond == VFV_PRECOND_ILU0) {
+            k_combine<T, 2><<<vb, kBlk, 0, s>>>(K, V.p, x.p, nullptr, z.p);
+            ilu_apply<T>(s, *ilu, lu_vals(), z.p, z2.p, z.p, nullptr);  // out may alias in: the upper sweep starts after the lower one
+            k_add_to_x<T><<<vb, 256, 0, s>>>(n, x.p, z.p);
+        } else if (precond == VFV_PRECOND_JACOBI) {
+            k_combine<T, 1><<<vb, kBlk, 0, s>>>(K, V.p, x.p, dinv.p, nullptr);
+        } else {
+            k_combine<T, 0><<<vb, kBlk, 0, s>>>(K, V.p, x.p, nullptr, nullptr);
+        }
+        k_residual<T, G><<<sp_blocks, kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+    }
+
+    int solve(vfv_ctx* ctx, vfv_pattern* p, const double* d_b, const double* d_x0, double* d_x, const vfv_gmres_opts& o,
+              vfv_solve_info* info) {
+        cudaStream_t s = ctx->stream;
+        constexpr int G = 8;
+        const bool mixed = !std::is_same<T, double>::value;
+        CK(cudaMemcpyAsync(b.p, d_b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(x.p, d_x0, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        // matrix preparation for this solve
+        if (precond == VFV_PRECOND_JACOBI) {
+            k_jacobi_inv<<<grid_for(n), 256, 0, s>>>(n, p->diag_pos.p, p->val.p, dinv.p);
+            k_scale_cols<T><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, p->ci.p, p->val.p, dinv.p, valK.p);
+        } else if (valK.p) {
+            k_scale_cols<T><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, p->ci.p, p->val.p, nullptr, valK.p);
+        }
+        if (precond == VFV_PRECOND_ILU0) {
+            int rc = ilu_refresh(ctx, p, *ilu, mixed);
+            if (rc) return rc;
+        }
+        // ||b|| and the absolute tolerance
+        const int nb = std::min(grid_for(n), 1024);
+        k_norm2<<<nb, kBlk, 0, s>>>(n, b.p, part.p, counter.p + 4, scal.p + 2);
+        CK(cudaMemcpyAsync(ctx->h_scalar, scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        CK(cudaGetLastError());
+        const double bnorm = std::sqrt(ctx->h_scalar[0]);
+        if (info) {
+            info->bnorm = bnorm;
+            info->levels = ilu ? ilu->nlev : 0;
+        }
+        if (!std::isfinite(bnorm)) return set_err(ctx, VFV_NONFINITE, "right-hand side is not finite");
+        if (bnorm == 0.0) {
+            CK(cudaMemsetAsync(d_x, 0, n * sizeof(double), s));
+            CK(cudaStreamSynchronize(s));
+            if (info) {
+                info->status = VFV_OK;
+                info->iters = info->cycles = 0;
+                info->relres = 0.0;
+            }
+            return VFV_OK;
+        }
+        const double hs[2] = {o.tol * bnorm, mixed ? std::max(0.0, o.inner_rtol) : 0.0};
+        CK(cudaMemcpyAsync(scal.p, hs, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
+        k_residual<T, G><<<grid_for(n * G), kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+        if (!exec) {
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            enqueue_cycle(s, p);
+            CK(cudaStreamEndCapture(s, &graph));
+            cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(e);
+        }
+        int cycles = 0, rc = VFV_OK;
+        DevStatus hst{};
+        for (;;) {
+            CK(cudaMemcpyAsync(ctx->h_status, st.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            hst = *ctx->h_status;
+            if (hst.nonfinite) {
+                rc = VFV_NONFINITE;
+                break;
+            }
+            if (hst.converged) break;
+            if (cycles >= o.max_outer) {
+                rc = VFV_NOT_CONVERGED;
+                break;
+            }
+            CK(cudaGraphLaunch(exec, s));
+            ++cycles;
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(d_x, x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        if (info) {
+            info->status = rc;
+            info->iters = hst.total_steps;
+            info->cycles = cycles;
+            info->relres = hst.beta0 / bnorm;
+        }
+        if (rc == VFV_NOT_CONVERGED)
+            return set_err(ctx, rc, "GMRES did not converge in " + std::to_string(o.max_outer) + " restart cycles (relres " +
+                                        std::to_string(hst.beta0 / bnorm) + ")");
+        if (rc == VFV_NONFINITE) return set_err(ctx, rc, "GMRES: non-finite residual");
+        return VFV_OK;
+    }
+};
+
+int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
+    if (!o) return set_err(ctx, VFV_BAD_INPUT, "opts is NULL");
+    if (!(o->tol > 0.0)) return set_err(ctx, VFV_BAD_INPUT, "tol must be positive (LinearGmresNonPositiveTolerance)");
+    if (o->restart <= 0 || o->restart + 1 > kMaxBasis) return set_err(ctx, VFV_BAD_INPUT, "restart must be in [1, 127]");
+    if (o->max_outer <= 0) return set_err(ctx, VFV_BAD_INPUT, "max_outer must be positive (LinearGmresNonPositiveMaxOuter)");
+    if (o->precond < VFV_PRECOND_NONE || o->precond > VFV_PRECOND_ILU0) return set_err(ctx, VFV_BAD_INPUT, "unknown preconditioner");
+    if (o->precision != VFV_FP64 && o->precision != VFV_MIXED) return set_err(ctx, VFV_BAD_INPUT, "unknown precision");
+    if (o->ilu_order != VFV_ILU_MULTICOLOR && o->ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
+    return VFV_OK;
+}
+
+int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info) {
+    const auto key = std::make_tuple(o->precision, o->precond, o->precond == VFV_PRECOND_ILU0 ? o->ilu_order : 0, o->restart);
+    auto it = p->solvers.find(key);
+    if (it == p->solvers.end()) {
+        std::unique_ptr<SolverBase> sb;
+        int rc;
+        if (o->precision == VFV_MIXED) {
+            auto g = std::make_unique<Gmres<float>>();
+            rc = g->init(ctx, p, o->restart, o->precond, o->ilu_order);
+            sb = std::move(g);
+        } else {
+            auto g = std::make_unique<Gmres<double>>();
+            rc = g->init(ctx, p, o->restart, o->precond, o->ilu_order);
+            sb = std::move(g);
+        }
+        if (rc) return rc;
+        it = p->solvers.emplace(key, std::move(sb)).first;
+    }
+    if (o->precision == VFV_MIXED) return static_cast<Gmres<float>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info);
+    return static_cast<Gmres<double>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info);
+}
+
+int finish_pattern(vfv_ctx* ctx, vfv_pattern* p) {
+    const int64_t n = p->n;
+    std::vector<int32_t> dpos(n, -1);
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t k = p->h_rp[i]; k < p->h_rp[i + 1]; ++k)
+            if (p->h_ci[k] == i) dpos[i] = k;
+    cudaStream_t s = ctx->stream;
+    CK(p->rp.upload(p->h_rp.data(), n + 1, s));
+    CK(p->ci.upload(p->h_ci.data(), p->nnz, s));
+    CK(p->diag_pos.upload(dpos.data(), n, s));
+    CK(p->val.alloc(p->nnz));
+    CK(cudaMemsetAsync(p->val.p, 0, p->nnz * sizeof(double), s));
+    CK(cudaStreamSynchronize(s));
+    return VFV_OK;
+}
+
+}  // namespace
+
+// ================================================================ mesh / heat handles
+struct vfv_mesh {
+    Mesh m;
+    Dual d;
+};
+
+struct vfv_heat {
+    vfv_ctx* ctx = nullptr;
+    int64_t n = 0, n_dir = 0, n_bsub = 0;
+    DBuf<int32_t> np, ni, kind, node_bnd, bp, bj, bk, dloc;
+    DBuf<double> area, dist, skew, gw, cvol, cskew, barea, bw;
+    DBuf<double> f, grad, b;  // f: [5][n] = k, q, s, T, bc_val ; grad: [4][3][n]
+    vfv_pattern* pat = nullptr;
+    ~vfv_heat() { delete pat; }
+};
+
+// ================================================================ C ABI
+extern "C" {
+
+void vfv_gmres_default_opts(vfv_gmres_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tol = 1e-6;
+    o->restart = 50;
+    o->max_outer = 200;
+    o->precond = VFV_PRECOND_JACOBI;
+    o->precision = VFV_FP64;
+    o->ilu_order = VFV_ILU_MULTICOLOR;
+    o->inner_rtol = 0.0;
+}
+
+int vfv_ctx_create(int device, vfv_ctx** out) {
+    vfv_ctx* ctx = nullptr;
+    if (!out) return set_err(nullptr, VFV_BAD_INPUT, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return set_err(nullptr, VFV_CUDA_ERROR, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= count) return set_err(nullptr, VFV_BAD_INPUT, "device index out of range");
+    CK(cudaSetDevice(device));
+    ctx = new vfv_ctx();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_status, sizeof(DevStatus)) != cudaSuccess || cudaMallocHost(&ctx->h_scalar, 64) != cudaSuccess) {
+        vfv_ctx_destroy(ctx);
+        return set_err(nullptr, VFV_CUDA_ERROR, "context allocation failed");
+    }
+    *out = ctx;
+    return VFV_OK;
+}
+
+void vfv_ctx_destroy(vfv_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->h_scalar) cudaFreeHost(ctx->h_scalar);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* vfv_last_error(const vfv_ctx* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+int vfv_ctx_synchronize(vfv_ctx* ctx) {
+    if (!ctx) return set_err(nullptr, VFV_BAD_INPUT, "ctx is NULL");
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    return VFV_OK;
+}
+
+void* vfv_ctx_stream(vfv_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int vfv_pattern_from_triplets(vfv_ctx* ctx, int64_t n, int64_t ntrip, const uint64_t* rows, const uint64_t* cols, vfv_pattern** out) {
+    if (!ctx || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    *out = nullptr;
+    if (n <= 0 || n >= (int64_t)1 << 31 || ntrip < 0 || (ntrip > 0 && (!rows || !cols)))
+        return set_err(ctx, VFV_BAD_INPUT, "invalid matrix size or triplet arrays");
+    std::vector<uint64_t> key(ntrip);
+    std::vector<int64_t> idx(ntrip);
+    for (int64_t t = 0; t < ntrip; ++t) {
+        if (rows[t] >= (uint64_t)n || cols[t] >= (uint64_t)n)
+            return set_err(ctx, VFV_BAD_INPUT, "triplet index out of range at " + std::to_string(t));
+        key[t] = rows[t] * (uint64_t)n + cols[t];
+        idx[t] = t;
+    }
+    int bits = 1;
+    while (bits < 64 && ((uint64_t)n * (uint64_t)n - 1) >> bits) ++bits;
+    radix_sort_pairs(key, idx, bits);
+    auto p = std::make_unique<vfv_pattern>();
+    p->ctx = ctx;
+    p->n = n;
+    p->ntrip = ntrip;
+    p->h_rp.assign(n + 1, 0);
+    std::vector<int64_t> sp;
+    sp.reserve(ntrip / 2 + 2);
+    for (int64_t t = 0; t < ntrip; ++t) {
+        if (t == 0 || key[t] != key[t - 1]) {
+            sp.push_back(t);
+            p->h_ci.push_back((int32_t)(key[t] % (uint64_t)n));
+            p->h_rp[key[t] / (uint64_t)n + 1]++;
+        }
+    }
+    sp.push_back(ntrip);
+    for (int64_t i = 0; i < n; ++i) p->h_rp[i + 1] += p->h_rp[i];
+    p->nnz = (int64_t)p->h_ci.size();
+    if (p->nnz >= (int64_t)1 << 31) return set_err(ctx, VFV_BAD_INPUT, "too many non-zeros for 32-bit indices");
+    int rc = finish_pattern(ctx, p.get());
+    if (rc) return rc;
+    cudaStream_t s = ctx->stream;
+    CK(p->slot_ptr.upload(sp.data(), sp.size(), s));
+    CK(p->slot_trip.upload(idx.data(), ntrip, s));
+    CK(p->trip_vals.alloc(ntrip));
+    *out = p.release();
+    return VFV_OK;
+}
+
+int vfv_pattern_from_csr(vfv_ctx* ctx, int64_t n, const int32_t* rowptr, const int32_t* colind, vfv_pattern** out) {
+    if (!ctx || !out || !rowptr) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    *out = nullptr;
+    if (n <= 0 || n >= (int64_t)1 << 31 || rowptr[0] != 0) return set_err(ctx, VFV_BAD_INPUT, "invalid CSR");
+    auto p = std::make_unique<vfv_pattern>();
+    p->ctx = ctx;
+    p->n = n;
+    p->h_rp.assign(rowptr, rowptr + n + 1);
+    p->nnz = p->h_rp[n];
+    if (p->nnz > 0 && !colind) return set_err(ctx, VFV_BAD_INPUT, "colind is NULL");
+    p->h_ci.assign(colind, colind + p->nnz);
+    for (int64_t i = 0; i < n; ++i) {
+        if (p->h_rp[i + 1] < p->h_rp[i]) return set_err(ctx, VFV_BAD_INPUT, "rowptr not monotone");
+        for (int32_t k = p->h_rp[i]; k < p->h_rp[i + 1]; ++k) {
+            if (p->h_ci[k] < 0 || p->h_ci[k] >= n) return set_err(ctx, VFV_BAD_INPUT, "column index out of range");
+            if (k > p->h_rp[i] && p->h_ci[k] <= p->h_ci[k - 1]) return set_err(ctx, VFV_BAD_INPUT, "columns not strictly ascending");
+        }
+    }
+    int rc = finish_pattern(ctx, p.get());
+    if (rc) return rc;
+    *out = p.release();
+    return VFV_OK;
+}
+
+void vfv_pattern_destroy(vfv_pattern* p) {
+    if (!p) return;
+    if (p->ctx) cudaStreamSynchronize(p->ctx->stream);
+    delete p;
+}
+
+int vfv_pattern_info(const vfv_pattern* p, int64_t* n, int64_t* nnz, int64_t* ntrip) {
+    if (!p) return set_err(nullptr, VFV_BAD_INPUT, "pattern is NULL");
+    if (n) *n = p->n;
+    if (nnz) *nnz = p->nnz;
+    if (ntrip) *ntrip = p->ntrip;
+    return VFV_OK;
+}
+
+int vfv_values_from_triplets(vfv_ctx* ctx, vfv_pattern* p, const double* vals) {
+    if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (!p->slot_ptr.p && p->ntrip == 0 && p->nnz > 0) return set_err(ctx, VFV_BAD_INPUT, "pattern has no triplet map");
+    if (p->ntrip > 0 && !vals) return set_err(ctx, VFV_BAD_INPUT, "vals is NULL");
+    cudaStream_t s = ctx->stream;
+    if (p->ntrip > 0) CK(cudaMemcpyAsync(p->trip_vals.p, vals, p->ntrip * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_values_from_triplets(s, p->nnz, p->slot_ptr.p, p->slot_trip.p, p->trip_vals.p, p->val.p);
+    CK(cudaGetLastError());
+    p->version++;
+    return VFV_OK;
+}
+
+int vfv_values_set(vfv_ctx* ctx, vfv_pattern* p, const double* vals, int on_device) {
+    if (!ctx || !p || !vals) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    CK(cudaMemcpyAsync(p->val.p, vals, p->nnz * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    p->version++;
+    return VFV_OK;
+}
+
+int vfv_csr_export(vfv_ctx* ctx, const vfv_pattern* p, int32_t* rowptr, int32_t* colind, double* vals) {
+    if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (rowptr) std::memcpy(rowptr, p->h_rp.data(), (p->n + 1) * sizeof(int32_t));
+    if (colind) std::memcpy(colind, p->h_ci.data(), p->nnz * sizeof(int32_t));
+    if (vals) {
+        CK(cudaMemcpyAsync(vals, p->val.p, p->nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return VFV_OK;
+}
+
+int vfv_solve_device(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* opts,
+                     vfv_solve_info* info) {
+    if (!ctx || !p || !b || !x0 || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    int rc = check_opts(ctx, opts);
+    if (rc) return rc;
+    if (info) std::memset(info, 0, sizeof(*info));
+    return solve_dev(ctx, p, b, x0, x, opts, info);
+}
+
+int vfv_solve(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* opts,
+              vfv_solve_info* info) {
+    if (!ctx || !p || !b || !x0 || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    int rc = check_opts(ctx, opts);
+    if (rc) return rc;
+    if (info) std::memset(info, 0, sizeof(*info));
+    cudaStream_t s = ctx->stream;
+    if (!p->tmp_b.p) {
+        CK(p->tmp_b.alloc(p->n));
+        CK(p->tmp_x.alloc(p->n));
+    }
+    CK(cudaMemcpyAsync(p->tmp_b.p, b, p->n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(p->tmp_x.p, x0, p->n * sizeof(double), cudaMemcpyHostToDevice, s));
+    rc = solve_dev(ctx, p, p->tmp_b.p, p->tmp_x.p, p->tmp_x.p, opts, info);
+    CK(cudaMemcpyAsync(x, p->tmp_x.p, p->n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return rc;
+}
+
+int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double* y) {
+    if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    constexpr int G = 8;
+    k_spmv<double, double, double, double, G><<<grid_for(p->n * G), kBlk, 0, ctx->stream>>>(p->n, p->rp.p, p->ci.p, p->val.p, x, y, nullptr, nullptr);
+    CK(cudaGetLastError());
+    return VFV_OK;
+}
+
+int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y) {
+    if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    constexpr int G = 8;
+    if (p->version32 != p->version) {
+        if (!p->val32.p) CK(p->val32.alloc(p->nnz));
+        k_cast<double, float><<<grid_for(p->nnz), 256, 0, ctx->stream>>>(p->nnz, p->val.p, p->val32.p);
+        p->version32 = p->version;
+    }
+    k_spmv<float, float, float, float, G><<<grid_for(p->n * G), kBlk, 0, ctx->stream>>>(p->n, p->rp.p, p->ci.p, p->val32.p, x, y, nullptr, nullptr);
+    CK(cudaGetLastError());
+    return VFV_OK;
+}
+
+int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels) {
+    if (!ctx || !p || !r || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
+    auto it = p->ilu.find(ilu_order);
+    if (it == p->ilu.end()) {
+        auto S = std::make_unique<IluStruct>();
+        int rc = build_ilu_struct(ctx, p, ilu_order, *S);
+        if (rc) return rc;
+        it = p->ilu.emplace(ilu_order, std::move(S)).first;
+    }
+    IluStruct& S = *it->second;
+    int rc = ilu_refresh(ctx, p, S, false);
+    if (rc) return rc;
+    DBuf<double> t;
+    CK(t.alloc(p->n));
+    ilu_apply<double>(ctx->stream, S, S.lu64.p, r, t.p, z, nullptr);
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    if (levels) *levels = S.nlev;
+    return VFV_OK;
+}
+
+// ---------------------------------------------------------------- mesh
+static int mesh_finish(vfv_mesh* mh, vfv_mesh** out) {
+    std::string e = delaunay(mh->m);
+    if (e.empty()) e = build_dual(mh->m, mh->d);
+    if (!e.empty()) {
+        delete mh;
+        return set_err(nullptr, VFV_BAD_INPUT, e);
+    }
+    *out = mh;
+    return VFV_OK;
+}
+
+int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out) {
+    if (!out) return set_err(nullptr, VFV_BAD_INPUT, "out is NULL");
+    *out = nullptr;
+    if (n < 3 || n > 400) return set_err(nullptr, VFV_BAD_INPUT, "grid size n must be in [3, 400]");
+    if (!(jitter >= 0.0 && jitter < 0.5)) return set_err(nullptr, VFV_BAD_INPUT, "jitter must be in [0, 0.5)");
+    auto* mh = new vfv_mesh();
+    mh->m = make_jitter_cube(n, seed, jitter);
+    return mesh_finish(mh, out);
+}
+
+int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out) {
+    if (!out || !pos || (n_nds > 0 && !node_bnd)) return set_err(nullptr, VFV_BAD_INPUT, "NULL argument");
+    *out = nullptr;
+    if (n_pts < 0 || n_nds < 0 || n_pts + n_nds < 4) return set_err(nullptr, VFV_BAD_INPUT, "need at least four vertices");
+    auto* mh = new vfv_mesh();
+    mh->m.n_pts = n_pts;
+    mh->m.n_nds = n_nds;
+    mh->m.pos.assign(pos, pos + 3 * (n_pts + n_nds));
+    mh->m.node_bnd.assign(node_bnd, node_bnd + n_nds);
+    return mesh_finish(mh, out);
+}
+
+void vfv_mesh_destroy(vfv_mesh* m) { delete m; }
+
+int vfv_mesh_info(const vfv_mesh* m, int64_t* n_pts, int64_t* n_nds, int64_t* n_tet, int64_t* n_dir, int64_t* n_bsub) {
+    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
+    if (n_pts) *n_pts = m->m.n_pts;
+    if (n_nds) *n_nds = m->m.n_nds;
+    if (n_tet) *n_tet = m->m.n_tet();
+    if (n_dir) *n_dir = m->d.n_dir;
+    if (n_bsub) *n_bsub = m->d.bnd_ptr.empty() ? 0 : m->d.bnd_ptr.back();
+    return VFV_OK;
+}
+
+int vfv_mesh_export(const vfv_mesh* m, double* pos, int32_t* node_bnd, int32_t* tets) {
+    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
+    if (pos) std::memcpy(pos, m->m.pos.data(), m->m.pos.size() * sizeof(double));
+    if (node_bnd) std::memcpy(node_bnd, m->m.node_bnd.data(), m->m.node_bnd.size() * sizeof(int32_t));
+    if (tets) std::memcpy(tets, m->m.tets.data(), m->m.tets.size() * sizeof(int32_t));
+    return VFV_OK;
+}
+
+int vfv_mesh_export_dual(const vfv_mesh* m, int64_t* nbr_ptr, int32_t* nbr_idx, double* dist, double* area, double* norm, double* skew,
+                         double* grad_wgt, double* cvol, double* cskew, int64_t* bnd_ptr, int32_t* bnd_j, int32_t* bnd_k,
+                         double* bnd_area, double* bnd_norm, double* bnd_wgt) {
+    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
+    const Dual& d = m->d;
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(nbr_ptr, d.nbr_ptr);
+    cp(nbr_idx, d.nbr_idx);
+    cp(dist, d.dist);
+    cp(area, d.area);
+    cp(norm, d.norm);
+    cp(skew, d.skew);
+    cp(grad_wgt, d.gw);
+    cp(cvol, d.cvol);
+    cp(cskew, d.cskew);
+    cp(bnd_ptr, d.bnd_ptr);
+    cp(bnd_j, d.bnd_j);
+    cp(bnd_k, d.bnd_k);
+    cp(bnd_area, d.bnd_area);
+    cp(bnd_norm, d.bnd_norm);
+    cp(bnd_wgt, d.bnd_wgt);
+    return VFV_OK;
+}
+
+// ---------------------------------------------------------------- heat operator
+int vfv_heat_create(vfv_ctx* ctx, const vfv_mesh* mh, int32_t n_bnd, const int32_t* bnd_kind, vfv_heat** out) {
+    if (!ctx || !mh || !out || (n_bnd > 0 && !bnd_kind)) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    *out = nullptr;
+    const Mesh& m = mh->m;
+    const Dual& d = mh->d;
+    const int64_t n = d.n_tot;
+    if (d.n_dir >= (int64_t)1 << 31 || n + d.n_dir >= (int64_t)1 << 31) return set_err(ctx, VFV_BAD_INPUT, "mesh too large for 32-bit indices");
+    std::vector<int32_t> kind(n, ROW_POINT), nb(n, -1);
+    for (int64_t v = m.n_pts; v < n; ++v) {
+        const int32_t b = m.node_bnd[v - m.n_pts];
+        if (b < 0 || b >= n_bnd) return set_err(ctx, VFV_BAD_INPUT, "node boundary id without a boundary condition");
+        if (bnd_kind[b] != VFV_BC_TEMP && bnd_kind[b] != VFV_BC_FLUX) return set_err(ctx, VFV_BAD_INPUT, "unknown boundary kind");
+        kind[v] = bnd_kind[b] == VFV_BC_TEMP ? ROW_DIRICHLET : ROW_FLUX;
+        nb[v] = b;
+    }
+    // matrix pattern: row v = its neighbours and itself (ascending); Dirichlet rows only the diagonal
+    std::vector<int32_t> np(n + 1), dloc(n, 0), rp(n + 1, 0), ci;
+    ci.reserve(d.n_dir + n);
+    for (int64_t v = 0; v < n; ++v) {
+        np[v] = (int32_t)d.nbr_ptr[v];
+        const int64_t b0 = d.nbr_ptr[v], e0 = d.nbr_ptr[v + 1];
+        if (kind[v] == ROW_DIRICHLET) {
+            ci.push_back((int32_t)v);
+        } else {
+            int32_t dl = 0;
+            while (b0 + dl < e0 && d.nbr_idx[b0 + dl] < v) ++dl;
+            dloc[v] = dl;
+            for (int64_t i = b0; i < b0 + dl; ++i) ci.push_back(d.nbr_idx[i]);
+            ci.push_back((int32_t)v);
+            for (int64_t i = b0 + dl; i < e0; ++i) ci.push_back(d.nbr_idx[i]);
+        }
+        rp[v + 1] = (int32_t)ci.size();
+    }
+    np[n] = (int32_t)d.nbr_ptr[n];
+    auto h = std::make_unique<vfv_heat>();
+    h->ctx = ctx;
+    h->n = n;
+    h->n_dir = d.n_dir;
+    h->n_bsub = d.bnd_ptr[n];
+    vfv_pattern* pat = nullptr;
+    int rc = vfv_pattern_from_csr(ctx, n, rp.data(), ci.data(), &pat);
+    if (rc) return rc;
+    h->pat = pat;
+    cudaStream_t s = ctx->stream;
+    std::vector<int32_t> bp(n + 1);
+    for (int64_t v = 0; v <= n; ++v) bp[v] = (int32_t)d.bnd_ptr[v];
+    CK(h->np.upload(np.data(), n + 1, s));
+    CK(h->ni.upload(d.nbr_idx.data(), d.n_dir, s));
+    CK(h->kind.upload(kind.data(), n, s));
+    CK(h->node_bnd.upload(nb.data(), n, s));
+    CK(h->dloc.upload(dloc.data(), n, s));
+    CK(h->bp.upload(bp.data(), n + 1, s));
+    CK(h->bj.upload(d.bnd_j.data(), d.bnd_j.size(), s));
+    CK(h->bk.upload(d.bnd_k.data(), d.bnd_k.size(), s));
+    CK(h->area.upload(d.area.data(), d.area.size(), s));
+    CK(h->dist.upload(d.dist.data(), d.dist.size(), s));
+    CK(h->skew.upload(d.skew.data(), d.skew.size(), s));
+    CK(h->gw.upload(d.gw.data(), d.gw.size(), s));
+    CK(h->cvol.upload(d.cvol.data(), d.cvol.size(), s));
+    CK(h->cskew.upload(d.cskew.data(), d.cskew.size(), s));
+    CK(h->barea.upload(d.bnd_area.data(), d.bnd_area.size(), s));
+    CK(h->bw.upload(d.bnd_wgt.data(), d.bnd_wgt.size(), s));
+    CK(h->f.alloc(5 * n));
+    CK(h->grad.alloc(12 * n));
+    CK(h->b.alloc(n));
+    *out = h.release();
+    return VFV_OK;
+}
+
+void vfv_heat_destroy(vfv_heat* h) {
+    if (!h) return;
+    if (h->ctx) cudaStreamSynchronize(h->ctx->stream);
+    delete h;
+}
+
+vfv_pattern* vfv_heat_pattern(vfv_heat* h) { return h ? h->pat : nullptr; }
+
+const double* vfv_heat_rhs_device(vfv_heat* h) { return h ? h->b.p : nullptr; }
+
+int vfv_heat_assemble(vfv_ctx* ctx, vfv_heat* h, const double* k, const double* q, const double* s_, const double* T,
+                      const double* bc_val, int on_device, double* b_out) {
+    if (!ctx || !h || !k || !q || !s_ || !T || !bc_val) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    const int64_t n = h->n;
+    cudaStream_t s = ctx->stream;
+    const double* src[5] = {k, q, s_, T, bc_val};
+    const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int f = 0; f < 5; ++f) CK(cudaMemcpyAsync(h->f.p + f * n, src[f], n * sizeof(double), kd, s));
+    const double* fl[4] = {h->f.p, h->f.p + n, h->f.p + 2 * n, h->f.p + 3 * n};
+    launch_grad(s, n, h->np.p, h->ni.p, h->gw.p, h->n_dir, 4, fl, h->grad.p);
+    HeatDev H{};
+    H.n = n;
+    H.n_dir = h->n_dir;
+    H.n_bsub = h->n_bsub;
+    H.np = h->np.p;
+    H.ni = h->ni.p;
+    H.area = h->area.p;
+    H.dist = h->dist.p;
+    H.skew = h->skew.p;
+    H.cvol = h->cvol.p;
+    H.cskew = h->cskew.p;
+    H.kind = h->kind.p;
+    H.node_bnd = h->node_bnd.p;
+    H.bp = h->bp.p;
+    H.bj = h->bj.p;
+    H.bk = h->bk.p;
+    H.barea = h->barea.p;
+    H.bw = h->bw.p;
+    H.rp = h->pat->rp.p;
+    H.dloc = h->dloc.p;
+    H.k = fl[0];
+    H.q = fl[1];
+    H.s = fl[2];
+    H.T = fl[3];
+    H.bcv = h->f.p + 4 * n;
+    H.gk = h->grad.p;
+    H.gq = h->grad.p + 3 * n;
+    H.gs = h->grad.p + 6 * n;
+    H.gT = h->grad.p + 9 * n;
+    H.val = h->pat->val.p;
+    H.b = h->b.p;
+    launch_assemble_heat(s, H);
+    CK(cudaGetLastError());
+    h->pat->version++;
+    if (b_out) {
+        CK(cudaMemcpyAsync(b_out, h->b.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    return VFV_OK;
+}
+
+int vfv_update_grad(vfv_ctx* ctx, vfv_heat* h, const double* f, double* grad) {
+    if (!ctx || !h || !f || !grad) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    const int64_t n = h->n;
+    cudaStream_t s = ctx->stream;
+    DBuf<double> fd, gd;
+    CK(fd.alloc(n));
+    CK(gd.alloc(3 * n));
+    CK(cudaMemcpyAsync(fd.p, f, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    const double* fl[1] = {fd.p};
+    launch_grad(s, n, h->np.p, h->ni.p, h->gw.p, h->n_dir, 1, fl, gd.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(grad, gd.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return VFV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,652 @@
+// Jittered-cube mesh generator, exact Bowyer-Watson Delaunay and the Voronoi dual.
+//
+// This is one-time CPU set-up that produces the inputs of the device assembly kernels.
+// Reference behaviour restated here:
+//   * delaunay():   src/base/delaunay.rs:6-170 (super-tetrahedron, Morton insertion order,
+//                   visibility walk, in-sphere cavity grown until star-shaped, exact predicates);
+//   * build_dual(): src/base/geom_tet.rs:101-293 (boundary faces, Voronoi face pieces, sorted
+//                   edge list, control-volume volumes and skews, boundary sub-faces, least-squares
+//                   gradient weights). Step 6 (pressure-gradient coefficients) is not needed by the
+//                   heat path and is not built here.
+// The geometric formulas (circumcentres, face pieces, sub-faces) are the reference's, evaluated
+// in the same operation order so that results agree to round-off; the data structures are not.
+#include "mesh.hpp"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace vfv {
+namespace {
+
+// ---------------------------------------------------------------- random numbers
+struct SplitMix64 {  // Steele, Lea & Flood 2014 (public-domain reference constants)
+    uint64_t s;
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    }
+    double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }
+};
+
+inline double quantize(double x) { return std::nearbyint(std::ldexp(x, kQuantBits)) * std::ldexp(1.0, -kQuantBits); }
+
+// ---------------------------------------------------------------- exact predicates
+struct IP { int64_t x, y, z; };
+typedef __int128 i128;
+
+// det[a-d; b-d; c-d]; > 0 when d lies below the plane of a, b, c seen counterclockwise from above
+inline i128 orient_i(const IP& a, const IP& b, const IP& c, const IP& d) {
+    const i128 ax = a.x - d.x, ay = a.y - d.y, az = a.z - d.z;
+    const i128 bx = b.x - d.x, by = b.y - d.y, bz = b.z - d.z;
+    const i128 cx = c.x - d.x, cy = c.y - d.y, cz = c.z - d.z;
+    return ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx);
+}
+
+inline i128 det3(i128 ax, i128 ay, i128 az, i128 bx, i128 by, i128 bz, i128 cx, i128 cy, i128 cz) {
+    return ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx);
+}
+
+// > 0 when e is strictly inside the sphere through a, b, c, d (a, b, c, d positively oriented).
+// Laplace expansion of the 4x4 lifted determinant along the lifted column; magnitudes stay below
+// 2^118 for coordinates within 20 * 2^18 of each other.
+inline i128 insphere_i(const IP& a, const IP& b, const IP& c, const IP& d, const IP& e) {
+    const i128 ax = a.x - e.x, ay = a.y - e.y, az = a.z - e.z;
+    const i128 bx = b.x - e.x, by = b.y - e.y, bz = b.z - e.z;
+    const i128 cx = c.x - e.x, cy = c.y - e.y, cz = c.z - e.z;
+    const i128 dx = d.x - e.x, dy = d.y - e.y, dz = d.z - e.z;
+    const i128 la = ax * ax + ay * ay + az * az;
+    const i128 lb = bx * bx + by * by + bz * bz;
+    const i128 lc = cx * cx + cy * cy + cz * cz;
+    const i128 ld = dx * dx + dy * dy + dz * dz;
+    const i128 m_bcd = det3(bx, by, bz, cx, cy, cz, dx, dy, dz);
+    const i128 m_acd = det3(ax, ay, az, cx, cy, cz, dx, dy, dz);
+    const i128 m_abd = det3(ax, ay, az, bx, by, bz, dx, dy, dz);
+    const i128 m_abc = det3(ax, ay, az, bx, by, bz, cx, cy, cz);
+    // cofactor expansion of det[a-e, |a-e|^2; ...; d-e, |d-e|^2] along the lifted column
+    return lb * m_acd - la * m_bcd + ld * m_abc - lc * m_abd;
+}
+
+inline IP to_ip(const double* p) {
+    return IP{(int64_t)std::llround(std::ldexp(p[0], kQuantBits)), (int64_t)std::llround(std::ldexp(p[1], kQuantBits)),
+              (int64_t)std::llround(std::ldexp(p[2], kQuantBits))};
+}
+
+inline int sgn(i128 v) { return (v > 0) - (v < 0); }
+
+// ---------------------------------------------------------------- vector helpers (geom formulas)
+struct V3 { double x, y, z; };
+inline V3 add3(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 sub3(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 scale3(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross3(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline double len3(V3 a) { return std::sqrt(dot3(a, a)); }
+
+// centre of the circle through a, b, c (delaunay.rs:207-214)
+inline V3 circumcircle3(V3 a, V3 b, V3 c) {
+    const V3 u = sub3(b, a), v = sub3(c, a);
+    const V3 w = cross3(u, v);
+    const V3 num = add3(scale3(dot3(u, u), cross3(v, w)), scale3(dot3(v, v), cross3(w, u)));
+    return add3(a, scale3(0.5 / dot3(w, w), num));
+}
+
+// centre of the sphere through a, b, c, d (delaunay.rs:216-221)
+inline V3 circumsphere3(V3 a, V3 b, V3 c, V3 d) {
+    const V3 u = sub3(b, a), v = sub3(c, a), w = sub3(d, a);
+    const V3 num = add3(add3(scale3(dot3(u, u), cross3(v, w)), scale3(dot3(v, v), cross3(w, u))), scale3(dot3(w, w), cross3(u, v)));
+    return add3(a, scale3(0.5 / dot3(u, cross3(v, w)), num));
+}
+
+inline uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
+    v &= 0x1fffffULL;
+    v = (v | (v << 32)) & 0x1f00000000ffffULL;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffULL;
+    v = (v | (v << 8)) & 0x100f00f00f00f00fULL;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ULL;
+    v = (v | (v << 2)) & 0x1249249249249249ULL;
+    return v;
+}
+
+}  // namespace
+
+int orient_sign(const double* a, const double* b, const double* c, const double* d) {
+    return sgn(orient_i(to_ip(a), to_ip(b), to_ip(c), to_ip(d)));
+}
+int insphere_sign(const double* a, const double* b, const double* c, const double* d, const double* e) {
+    return sgn(insphere_i(to_ip(a), to_ip(b), to_ip(c), to_ip(d), to_ip(e)));
+}
+
+// ---------------------------------------------------------------- mesh generator
+Mesh make_jitter_cube(int n, uint64_t seed, double jitter) {
+    Mesh m;
+    if (n < 3) return m;
+    const double h = 1.0 / (double)(n - 1);
+    SplitMix64 rng{seed};
+    std::vector<double> pts;
+    std::vector<double> nds[NUM_BND];
+    for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const double u0 = rng.uniform(), u1 = rng.uniform(), u2 = rng.uniform();
+                const bool fx = (i == 0 || i == n - 1), fy = (j == 0 || j == n - 1), fz = (k == 0 || k == n - 1);
+                double x = (double)i / (double)(n - 1), y = (double)j / (double)(n - 1), z = (double)k / (double)(n - 1);
+                if (!fx) x += (2.0 * u0 - 1.0) * jitter * h;
+                if (!fy) y += (2.0 * u1 - 1.0) * jitter * h;
+                if (!fz) z += (2.0 * u2 - 1.0) * jitter * h;
+                x = quantize(x);
+                y = quantize(y);
+                z = quantize(z);
+                if (!fx && !fy && !fz) {
+                    pts.insert(pts.end(), {x, y, z});
+                } else {
+                    const int b = fx ? (i == 0 ? BND_L : BND_R) : fy ? (j == 0 ? BND_F : BND_K) : (k == 0 ? BND_B : BND_T);
+                    nds[b].insert(nds[b].end(), {x, y, z});
+                }
+            }
+    m.n_pts = (int64_t)pts.size() / 3;
+    m.pos = std::move(pts);
+    for (int b = 0; b < NUM_BND; ++b) {
+        m.pos.insert(m.pos.end(), nds[b].begin(), nds[b].end());
+        m.node_bnd.insert(m.node_bnd.end(), nds[b].size() / 3, b);
+    }
+    m.n_nds = (int64_t)m.node_bnd.size();
+    return m;
+}
+
+// ---------------------------------------------------------------- Delaunay
+std::string delaunay(Mesh& mesh) {
+    const int64_t N = mesh.n_tot();
+    if (N < 4) return "delaunay: fewer than four vertices";
+    if (N > (int64_t)0x7ffffff0) return "delaunay: too many vertices for 32-bit ids";
+    std::vector<IP> P(N + 4);
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t v = 0; v < N; ++v) {
+        const double* p = &mesh.pos[3 * v];
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = std::min(lo[c], p[c]);
+            hi[c] = std::max(hi[c], p[c]);
+            if (!(std::fabs(p[c]) < 8.0)) return "delaunay: coordinates must lie within [-8, 8]";
+        }
+        P[v] = to_ip(p);
+    }
+    const double size = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
+    const double cen[3] = {0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2])};
+    const double dirs[4][3] = {{1, 1, 1}, {1, -1, -1}, {-1, 1, -1}, {-1, -1, 1}};
+    for (int s = 0; s < 4; ++s) {
+        const double q[3] = {cen[0] + 10.0 * size * dirs[s][0], cen[1] + 10.0 * size * dirs[s][1], cen[2] + 10.0 * size * dirs[s][2]};
+        P[N + s] = to_ip(q);
+    }
+
+    std::vector<std::array<int32_t, 4>> tv, ta;
+    std::vector<uint8_t> alive, incav;
+    std::vector<int32_t> freel;
+    tv.reserve(7 * N + 64);
+    ta.reserve(7 * N + 64);
+    tv.push_back({(int32_t)N, (int32_t)N + 1, (int32_t)N + 2, (int32_t)N + 3});
+    if (orient_i(P[N], P[N + 1], P[N + 2], P[N + 3]) < 0) std::swap(tv[0][0], tv[0][1]);
+    ta.push_back({-1, -1, -1, -1});
+    alive.push_back(1);
+    incav.push_back(0);
+
+    // insertion order: Morton code of the quantised position, ties by vid
+    std::vector<std::pair<uint64_t, int32_t>> order(N);
+    for (int64_t v = 0; v < N; ++v) {
+        uint64_t q[3];
+        for (int c = 0; c < 3; ++c) {
+            double t = (mesh.pos[3 * v + c] - lo[c]) / size * 2097151.0;
+            q[c] = (uint64_t)std::min(2097151.0, std::max(0.0, t));
+        }
+        order[v] = {spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2), (int32_t)v};
+    }
+    std::sort(order.begin(), order.end());
+
+    auto tet_pts = [&](int32_t t, IP q[4]) {
+        for (int c = 0; c < 4; ++c) q[c] = P[tv[t][c]];
+    };
+
+    std::vector<int32_t> cav;
+    struct BF { int32_t t, k; };
+    std::vector<BF> bfaces;
+    struct OpenEdge { int32_t a, b, t, m; };
+    std::vector<OpenEdge> open;
+    std::vector<int32_t> newt;
+    int32_t last = 0;
+    unsigned turn = 0;
+    IP q[4];
+    for (int64_t oi = 0; oi < N; ++oi) {
+        const int32_t vid = order[oi].second;
+        const IP p = P[vid];
+        // locate by a visibility walk; fall back to a scan if the walk runs long
+        int32_t t = last;
+        int64_t steps = 0;
+        for (;;) {
+            if (++steps > 4 * (int64_t)tv.size() + 16) {
+                t = -1;
+                for (int32_t s = 0; s < (int32_t)tv.size() && t < 0; ++s) {
+                    if (!alive[s]) continue;
+                    bool in = true;
+                    for (int k = 0; k < 4 && in; ++k) {
+                        tet_pts(s, q);
+                        q[k] = p;
+                        in = orient_i(q[0], q[1], q[2], q[3]) >= 0;
+                    }
+                    if (in) t = s;
+                }
+                if (t < 0) return "delaunay: point location failed";
+                break;
+            }
+            turn = (turn + 1) & 3u;
+            bool moved = false;
+            for (int l = 0; l < 4; ++l) {
+                const int k = (int)((l + turn) & 3u);
+                tet_pts(t, q);
+                q[k] = p;
+                if (orient_i(q[0], q[1], q[2], q[3]) < 0) {
+                    const int32_t o = ta[t][k];
+                    if (o < 0) return "delaunay: point outside the super tetrahedron";
+                    t = o;
+                    moved = true;
+                    break;
+                }
+            }
+            if (!moved) break;
+        }
+        for (int k = 0; k < 4; ++k) {
+            const IP& w = P[tv[t][k]];
+            if (w.x == p.x && w.y == p.y && w.z == p.z) return "delaunay: duplicate vertex";
+        }
+        // cavity: tetrahedra whose circumsphere strictly contains p
+        cav.clear();
+        cav.push_back(t);
+        incav[t] = 1;
+        for (size_t i = 0; i < cav.size(); ++i) {
+            const int32_t c = cav[i];
+            for (int k = 0; k < 4; ++k) {
+                const int32_t o = ta[c][k];
+                if (o < 0 || incav[o]) continue;
+                tet_pts(o, q);
+                if (insphere_i(q[0], q[1], q[2], q[3], p) > 0) {
+                    incav[o] = 1;
+                    cav.push_back(o);
+                }
+            }
+        }
+        // grow until every boundary face sees p with positive orientation (cospherical ties)
+        for (bool star = false; !star;) {
+            star = true;
+            for (size_t i = 0; i < cav.size(); ++i) {
+                const int32_t c = cav[i];
+                for (int k = 0; k < 4; ++k) {
+                    const int32_t o = ta[c][k];
+                    if (o >= 0 && incav[o]) continue;
+                    tet_pts(c, q);
+                    q[k] = p;
+                    if (orient_i(q[0], q[1], q[2], q[3]) > 0) continue;
+                    if (o < 0) return "delaunay: cavity reaches the super tetrahedron hull";
+                    incav[o] = 1;
+                    cav.push_back(o);
+                    star = false;
+                }
+            }
+        }
+        // boundary faces of the cavity, then one new tetrahedron per face
+        bfaces.clear();
+        for (int32_t c : cav)
+            for (int k = 0; k < 4; ++k) {
+                const int32_t o = ta[c][k];
+                if (o >= 0 && incav[o]) continue;
+                bfaces.push_back({c, k});
+            }
+        newt.resize(bfaces.size());
+        for (size_t i = 0; i < bfaces.size(); ++i) {
+            if (!freel.empty()) {
+                newt[i] = freel.back();
+                freel.pop_back();
+            } else {
+                newt[i] = (int32_t)tv.size();
+                tv.push_back({0, 0, 0, 0});
+                ta.push_back({-1, -1, -1, -1});
+                alive.push_back(0);
+                incav.push_back(0);
+            }
+        }
+        open.clear();
+        for (size_t i = 0; i < bfaces.size(); ++i) {
+            const int32_t c = bfaces[i].t, k = bfaces[i].k, nt = newt[i];
+            std::array<int32_t, 4> nv = tv[c];
+            nv[k] = vid;
+            tv[nt] = nv;
+            ta[nt] = {-1, -1, -1, -1};
+            alive[nt] = 1;
+            const int32_t o = ta[c][k];
+            ta[nt][k] = o;
+            if (o >= 0)
+                for (int mm = 0; mm < 4; ++mm)
+                    if (ta[o][mm] == c) {
+                        ta[o][mm] = nt;
+                        break;
+                    }
+            for (int mm = 0; mm < 4; ++mm) {
+                if (mm == k) continue;
+                int32_t e2[2], ne = 0;
+                for (int l = 0; l < 4; ++l)
+                    if (l != k && l != mm) e2[ne++] = nv[l];
+                const int32_t a = std::min(e2[0], e2[1]), b = std::max(e2[0], e2[1]);
+                bool matched = false;
+                for (size_t s = 0; s < open.size(); ++s)
+                    if (open[s].a == a && open[s].b == b) {
+                        ta[nt][mm] = open[s].t;
+                        ta[open[s].t][open[s].m] = nt;
+                        open[s] = open.back();
+                        open.pop_back();
+                        matched = true;
+                        break;
+                    }
+                if (!matched) open.push_back({a, b, nt, mm});
+            }
+        }
+        if (!open.empty()) return "delaunay: cavity boundary is not closed";
+        for (int32_t c : cav) {
+            alive[c] = 0;
+            incav[c] = 0;
+            freel.push_back(c);
+        }
+        last = newt.back();
+    }
+
+    mesh.tets.clear();
+    double vol = 0.0;
+    for (size_t t = 0; t < tv.size(); ++t) {
+        if (!alive[t]) continue;
+        const auto& v = tv[t];
+        if (v[0] >= N || v[1] >= N || v[2] >= N || v[3] >= N) continue;
+        mesh.tets.insert(mesh.tets.end(), v.begin(), v.end());
+        const double* a = &mesh.pos[3 * v[0]];
+        const double* b = &mesh.pos[3 * v[1]];
+        const double* c = &mesh.pos[3 * v[2]];
+        const double* d = &mesh.pos[3 * v[3]];
+        const V3 ad{a[0] - d[0], a[1] - d[1], a[2] - d[2]}, bd{b[0] - d[0], b[1] - d[1], b[2] - d[2]},
+            cd{c[0] - d[0], c[1] - d[1], c[2] - d[2]};
+        vol += dot3(ad, cross3(bd, cd)) / 6.0;
+    }
+    if (mesh.tets.empty()) return "delaunay: no tetrahedra";
+    const double hull = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+    if (std::fabs(vol - hull) > 1e-9 * hull) return "delaunay: tetrahedra do not fill the bounding box (hull is not a box)";
+    return "";
+}
+
+// ---------------------------------------------------------------- Voronoi dual
+std::string build_dual(const Mesh& mesh, Dual& d) {
+    const int64_t N = mesh.n_tot(), T = mesh.n_tet();
+    const int32_t* tet = mesh.tets.data();
+    auto P = [&](int64_t v) { return V3{mesh.pos[3 * v], mesh.pos[3 * v + 1], mesh.pos[3 * v + 2]}; };
+    static const int EP[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+
+    // ---- boundary faces: faces of exactly one tetrahedron (geom_tet.rs:101-116)
+    std::vector<std::pair<std::array<int32_t, 3>, int64_t>> fk(4 * T);
+    for (int64_t t = 0; t < T; ++t)
+        for (int k = 0; k < 4; ++k) {
+            std::array<int32_t, 3> key = {tet[4 * t + (k + 1) % 4], tet[4 * t + (k + 2) % 4], tet[4 * t + (k + 3) % 4]};
+            std::sort(key.begin(), key.end());
+            fk[4 * t + k] = {key, 4 * t + k};
+        }
+    std::sort(fk.begin(), fk.end());
+    std::vector<uint8_t> is_bface(4 * T, 0);
+    for (size_t i = 0; i < fk.size();) {
+        size_t j = i + 1;
+        while (j < fk.size() && fk[j].first == fk[i].first) ++j;
+        if (j - i == 1) is_bface[fk[i].second] = 1;
+        i = j;
+    }
+    std::vector<std::pair<std::array<int32_t, 3>, int64_t>>().swap(fk);
+    static const int FO[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};  // counterclockwise from outside
+    std::vector<int32_t> surf;
+    for (int64_t t = 0; t < T; ++t)
+        for (int k = 0; k < 4; ++k)
+            if (is_bface[4 * t + k])
+                surf.insert(surf.end(), {tet[4 * t + FO[k][0]], tet[4 * t + FO[k][1]], tet[4 * t + FO[k][2]]});
+    for (int32_t v : surf)
+        if (v < mesh.n_pts) return "dual: a boundary face joins an interior point";
+
+    // ---- unique sorted edge list (geom_tet.rs:173-177)
+    std::vector<uint64_t> tkey(6 * T);
+    for (int64_t t = 0; t < T; ++t)
+        for (int e = 0; e < 6; ++e) {
+            const uint64_t a = (uint32_t)tet[4 * t + EP[e][0]], b = (uint32_t)tet[4 * t + EP[e][1]];
+            tkey[6 * t + e] = (std::min(a, b) << 32) | std::max(a, b);
+        }
+    std::vector<uint64_t> ekey(tkey);
+    std::sort(ekey.begin(), ekey.end());
+    ekey.erase(std::unique(ekey.begin(), ekey.end()), ekey.end());
+    const int64_t E = (int64_t)ekey.size();
+    std::vector<int32_t> teid(6 * T);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < 6 * T; ++i) teid[i] = (int32_t)(std::lower_bound(ekey.begin(), ekey.end(), tkey[i]) - ekey.begin());
+    std::vector<uint64_t>().swap(tkey);
+
+    // ---- Voronoi face pieces (geom_tet.rs:122-171): computed in parallel per chunk of
+    //      tetrahedra, accumulated serially in tetrahedron order
+    std::vector<double> e_area(E, 0.0), e_skew(3 * E, 0.0), cent_sum(3 * N, 0.0);
+    const int64_t CH = 1 << 16;
+    std::vector<double> pa_(CH * 12), pc_(CH * 36);
+    for (int64_t t0 = 0; t0 < T; t0 += CH) {
+        const int64_t t1 = std::min(T, t0 + CH);
+#pragma omp parallel for schedule(static)
+        for (int64_t t = t0; t < t1; ++t) {
+            const int32_t* tv = &tet[4 * t];
+            const V3 c_t = circumsphere3(P(tv[0]), P(tv[1]), P(tv[2]), P(tv[3]));
+            for (int e = 0; e < 6; ++e) {
+                const int li = EP[e][0], lj = EP[e][1];
+                int oth[2], no = 0;
+                for (int l = 0; l < 4; ++l)
+                    if (l != li && l != lj) oth[no++] = l;
+                const V3 pi = P(tv[li]), pj = P(tv[lj]);
+                const double dist = len3(sub3(pj, pi));
+                const V3 ee = scale3(1.0 / dist, sub3(pj, pi));
+                const V3 m = scale3(0.5, add3(pi, pj));
+                for (int side = 0; side < 2; ++side) {
+                    const V3 pa = P(tv[oth[side]]), pb = P(tv[oth[1 - side]]);
+                    const V3 c_f = circumcircle3(pi, pj, pa);
+                    V3 u = sub3(sub3(pa, m), scale3(dot3(sub3(pa, m), ee), ee));
+                    u = scale3(1.0 / len3(u), u);
+                    V3 n = cross3(ee, u);
+                    if (dot3(sub3(pb, m), n) < 0.0) n = scale3(-1.0, n);
+                    const double s1 = dot3(sub3(c_f, m), u);
+                    const double s2 = dot3(sub3(c_t, c_f), n);
+                    const double area = 0.5 * s1 * s2;
+                    const V3 cent = scale3(1.0 / 3.0, add3(m, add3(c_f, c_t)));
+                    const int64_t pidx = (t - t0) * 12 + e * 2 + side;
+                    pa_[pidx] = area;
+                    pc_[3 * pidx] = cent.x;
+                    pc_[3 * pidx + 1] = cent.y;
+                    pc_[3 * pidx + 2] = cent.z;
+                }
+            }
+        }
+        for (int64_t t = t0; t < t1; ++t) {
+            const int32_t* tv = &tet[4 * t];
+            for (int e = 0; e < 6; ++e) {
+                const int32_t vi = tv[EP[e][0]], vj = tv[EP[e][1]];
+                const V3 pi = P(vi), pj = P(vj);
+                const double dist = len3(sub3(pj, pi));
+                const V3 m = scale3(0.5, add3(pi, pj));
+                const int32_t eid = teid[6 * t + e];
+                for (int side = 0; side < 2; ++side) {
+                    const int64_t pidx = (t - t0) * 12 + e * 2 + side;
+                    const double area = pa_[pidx];
+                    const V3 cent{pc_[3 * pidx], pc_[3 * pidx + 1], pc_[3 * pidx + 2]};
+                    e_area[eid] += area;
+                    const V3 sk = scale3(area, sub3(cent, m));
+                    e_skew[3 * eid] += sk.x;
+                    e_skew[3 * eid + 1] += sk.y;
+                    e_skew[3 * eid + 2] += sk.z;
+                    const double vol = area * dist / 6.0;
+                    const V3 ci = scale3(vol * 0.75, sub3(cent, pi));
+                    const V3 cj = scale3(vol * 0.75, sub3(cent, pj));
+                    cent_sum[3 * vi] += ci.x;
+                    cent_sum[3 * vi + 1] += ci.y;
+                    cent_sum[3 * vi + 2] += ci.z;
+                    cent_sum[3 * vj] += cj.x;
+                    cent_sum[3 * vj + 1] += cj.y;
+                    cent_sum[3 * vj + 2] += cj.z;
+                }
+            }
+        }
+    }
+    std::vector<int32_t>().swap(teid);
+
+    // ---- neighbour CSR and per-face data (geom_tet.rs:178-206)
+    d = Dual();
+    d.n_tot = N;
+    d.n_pts = mesh.n_pts;
+    d.n_dir = 2 * E;
+    const int64_t D = 2 * E;
+    d.nbr_ptr.assign(N + 1, 0);
+    for (int64_t e = 0; e < E; ++e) {
+        d.nbr_ptr[(ekey[e] >> 32) + 1]++;
+        d.nbr_ptr[(ekey[e] & 0xffffffffULL) + 1]++;
+    }
+    for (int64_t v = 0; v < N; ++v) d.nbr_ptr[v + 1] += d.nbr_ptr[v];
+    d.nbr_idx.assign(D, 0);
+    d.nbr_rev.assign(D, 0);
+    d.dist.assign(D, 0.0);
+    d.area.assign(D, 0.0);
+    d.norm.assign(3 * D, 0.0);
+    d.skew.assign(3 * D, 0.0);
+    d.cvol.assign(N, 0.0);
+    std::vector<int64_t> cur(d.nbr_ptr.begin(), d.nbr_ptr.end() - 1);
+    for (int64_t e = 0; e < E; ++e) {
+        const int64_t a = (int64_t)(ekey[e] >> 32), b = (int64_t)(ekey[e] & 0xffffffffULL);
+        const V3 pa = P(a), pb = P(b);
+        const double dist = len3(sub3(pb, pa));
+        const V3 nrm = scale3(1.0 / dist, sub3(pb, pa));
+        const double area = e_area[e];
+        const V3 ss{e_skew[3 * e], e_skew[3 * e + 1], e_skew[3 * e + 2]};
+        const V3 skew = (std::fabs(area) > 1e-12 * dist * dist) ? scale3(1.0 / area, ss) : V3{0.0, 0.0, 0.0};
+        const int64_t ia = cur[a]++, ib = cur[b]++;
+        d.nbr_idx[ia] = (int32_t)b;
+        d.nbr_idx[ib] = (int32_t)a;
+        d.nbr_rev[ia] = ib;
+        d.nbr_rev[ib] = ia;
+        d.dist[ia] = d.dist[ib] = dist;
+        d.area[ia] = d.area[ib] = area;
+        const V3 mn = scale3(-1.0, nrm);
+        d.norm[ia] = nrm.x;
+        d.norm[D + ia] = nrm.y;
+        d.norm[2 * D + ia] = nrm.z;
+        d.norm[ib] = mn.x;
+        d.norm[D + ib] = mn.y;
+        d.norm[2 * D + ib] = mn.z;
+        d.skew[ia] = d.skew[ib] = skew.x;
+        d.skew[D + ia] = d.skew[D + ib] = skew.y;
+        d.skew[2 * D + ia] = d.skew[2 * D + ib] = skew.z;
+        d.cvol[a] += area * dist / 6.0;
+        d.cvol[b] += area * dist / 6.0;
+    }
+    d.cskew.assign(3 * N, 0.0);
+    for (int64_t v = 0; v < N; ++v) {
+        const double s = 1.0 / d.cvol[v];
+        d.cskew[v] = s * cent_sum[3 * v];
+        d.cskew[N + v] = s * cent_sum[3 * v + 1];
+        d.cskew[2 * N + v] = s * cent_sum[3 * v + 2];
+    }
+
+    // ---- boundary sub-faces (geom_tet.rs:208-259)
+    const int64_t S = (int64_t)surf.size() / 3;
+    d.bnd_ptr.assign(N + 1, 0);
+    for (int64_t s = 0; s < S; ++s)
+        for (int l = 0; l < 3; ++l) d.bnd_ptr[surf[3 * s + l] + 1]++;
+    for (int64_t v = 0; v < N; ++v) d.bnd_ptr[v + 1] += d.bnd_ptr[v];
+    const int64_t B = d.bnd_ptr[N];
+    d.bnd_j.assign(B, 0);
+    d.bnd_k.assign(B, 0);
+    d.bnd_area.assign(B, 0.0);
+    d.bnd_norm.assign(3 * B, 0.0);
+    d.bnd_wgt.assign(3 * B, 0.0);
+    d.bnd_sum.assign(N, 0.0);
+    std::vector<int64_t> bcur(d.bnd_ptr.begin(), d.bnd_ptr.end() - 1);
+    for (int64_t s = 0; s < S; ++s) {
+        const int32_t* tt = &surf[3 * s];
+        const V3 p0 = P(tt[0]), p1 = P(tt[1]), p2 = P(tt[2]);
+        V3 nrm = cross3(sub3(p1, p0), sub3(p2, p0));
+        nrm = scale3(1.0 / len3(nrm), nrm);
+        const V3 c = circumcircle3(p0, p1, p2);
+        const double sq[3] = {dot3(sub3(p2, p1), sub3(p2, p1)), dot3(sub3(p0, p2), sub3(p0, p2)), dot3(sub3(p1, p0), sub3(p1, p0))};
+        const double lraw[3] = {sq[0] * (sq[1] + sq[2] - sq[0]), sq[1] * (sq[2] + sq[0] - sq[1]), sq[2] * (sq[0] + sq[1] - sq[2])};
+        const double lsum = lraw[0] + lraw[1] + lraw[2];
+        const double lam[3] = {lraw[0] / lsum, lraw[1] / lsum, lraw[2] / lsum};
+        for (int loc = 0; loc < 3; ++loc) {
+            const int32_t vi = tt[loc], vj = tt[(loc + 1) % 3], vk = tt[(loc + 2) % 3];
+            const V3 pi = P(vi), pj = P(vj), pk = P(vk);
+            double ar[2];
+            for (int side = 0; side < 2; ++side) {
+                const V3 pa = side == 0 ? pj : pk, pb = side == 0 ? pk : pj;
+                const V3 m = scale3(0.5, add3(pi, pa));
+                const V3 e = sub3(pa, pi);
+                const double len = len3(e);
+                const V3 u = sub3(sub3(pb, m), scale3(dot3(sub3(pb, m), e) / (len * len), e));
+                ar[side] = 0.25 * len * dot3(sub3(c, m), scale3(1.0 / len3(u), u));
+            }
+            const double asum = ar[0] + ar[1];
+            const double l0 = lam[loc], l1 = lam[(loc + 1) % 3], l2 = lam[(loc + 2) % 3];
+            const V3 cj{(1.5 + l0) / 3.0, (0.5 + l1) / 3.0, l2 / 3.0};
+            const V3 ck{(1.5 + l0) / 3.0, l1 / 3.0, (0.5 + l2) / 3.0};
+            const V3 w = (std::fabs(asum) > 1e-12 * len3(sub3(pj, pi)) * len3(sub3(pk, pi)))
+                             ? scale3(1.0 / asum, add3(scale3(ar[0], cj), scale3(ar[1], ck)))
+                             : V3{1.0, 0.0, 0.0};
+            const int64_t ib = bcur[vi]++;
+            d.bnd_sum[vi] += asum;
+            d.bnd_j[ib] = vj;
+            d.bnd_k[ib] = vk;
+            d.bnd_area[ib] = asum;
+            d.bnd_norm[ib] = nrm.x;
+            d.bnd_norm[B + ib] = nrm.y;
+            d.bnd_norm[2 * B + ib] = nrm.z;
+            d.bnd_wgt[ib] = w.x;
+            d.bnd_wgt[B + ib] = w.y;
+            d.bnd_wgt[2 * B + ib] = w.z;
+        }
+    }
+
+    // ---- least-squares gradient weights (geom_tet.rs:261-293)
+    d.gw.assign(3 * D, 0.0);
+    int64_t bad = -1;
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < N; ++v) {
+        const V3 pc = P(v);
+        double m[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int64_t i = d.nbr_ptr[v]; i < d.nbr_ptr[v + 1]; ++i) {
+            const V3 dd = sub3(P(d.nbr_idx[i]), pc);
+            const double dv[3] = {dd.x, dd.y, dd.z};
+            const double omega = 1.0 / (dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+            for (int r = 0; r < 3; ++r)
+                for (int s = 0; s < 3; ++s) m[r][s] += omega * dv[r] * dv[s];
+        }
+        const double adj[3][3] = {
+            {m[1][1] * m[2][2] - m[1][2] * m[2][1], m[0][2] * m[2][1] - m[0][1] * m[2][2], m[0][1] * m[1][2] - m[0][2] * m[1][1]},
+            {m[1][2] * m[2][0] - m[1][0] * m[2][2], m[0][0] * m[2][2] - m[0][2] * m[2][0], m[0][2] * m[1][0] - m[0][0] * m[1][2]},
+            {m[1][0] * m[2][1] - m[1][1] * m[2][0], m[0][1] * m[2][0] - m[0][0] * m[2][1], m[0][0] * m[1][1] - m[0][1] * m[1][0]},
+        };
+        const double det = m[0][0] * adj[0][0] + m[0][1] * adj[1][0] + m[0][2] * adj[2][0];
+        const double tr = m[0][0] + m[1][1] + m[2][2];
+        if (!(det > 1e-12 * tr * tr * tr)) {
+#pragma omp critical
+            bad = v;
+            continue;
+        }
+        for (int64_t i = d.nbr_ptr[v]; i < d.nbr_ptr[v + 1]; ++i) {
+            const V3 dd = sub3(P(d.nbr_idx[i]), pc);
+            const double omega = 1.0 / dot3(dd, dd);
+            for (int r = 0; r < 3; ++r) d.gw[r * D + i] = omega * (adj[r][0] * dd.x + adj[r][1] * dd.y + adj[r][2] * dd.z) / det;
+        }
+    }
+    if (bad >= 0) return "dual: singular least-squares gradient at vid " + std::to_string(bad);
+    return "";
+}
+
+}  // namespace vfv

@@ -1,0 +1,178 @@
+// Device assembly of the steady heat operator into a fixed CSR pattern (sm_100a).
+//
+// Restates, per row and in the reference's push order:
+//   ScalarDomain::update_grad          src/base/scl_dom.rs:146-164
+//   OpSclDomDiffusion / OpSclBndDiffusion  src/operator/core/opscl_dom_diff.rs:40-91, opscl_bnd_diff.rs:40-96
+//   OpSclDomProduction / OpSclBndProduction opscl_dom_prod.rs:39-76, opscl_bnd_prod.rs:39-81
+//   OpSclDomSource / OpSclBndSource         opscl_dom_src.rs:37-68, opscl_bnd_src.rs:37-73
+//   OpSclBndDirichlet                       opscl_bnd_dir.rs:56-78
+//   OpSclBndNeumann                         opscl_bnd_neu.rs:36-88
+// in the order of SteadyHeat::assemble_matrix (src/steady/core/steady_heat.rs:143-171).
+// The triplets a row receives are summed in push order by LinearGmres::build_matrix
+// (src/linear/linear_gmres.rs:66-74); here each row is owned by one group of lanes, the
+// off-diagonal coefficients are written straight into their CSR slots and lane 0 of the group adds
+// the diagonal contributions in the same order, so the result is deterministic and atomic-free.
+// This file is compiled with -fmad=false: every product and sum rounds exactly like the
+// reference's scalar code.
+#include "assemble.cuh"
+
+namespace vfv {
+
+constexpr int kAG = 16;  // lanes per row
+
+__device__ __forceinline__ unsigned group_mask(int G) {
+    const int lane = threadIdx.x & 31;
+    const unsigned base = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+    return base << (lane & ~(G - 1));
+}
+
+// grad_f[v] = sum_loc w[v][loc] * (f[n] - f[v]) for up to 4 fields at once.
+// out layout: [field][3][n]
+__global__ void __launch_bounds__(256) k_grad_lsq(int64_t n, const int32_t* __restrict__ np, const int32_t* __restrict__ ni,
+                                                 const double* __restrict__ gw, int64_t n_dir, int nf,
+                                                 const double* __restrict__ f0, const double* __restrict__ f1,
+                                                 const double* __restrict__ f2, const double* __restrict__ f3,
+                                                 double* __restrict__ out) {
+    const int lane = threadIdx.x & (kAG - 1);
+    const int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kAG;
+    if (v >= n) return;  // whole groups leave together
+    const unsigned mask = group_mask(kAG);
+    const double* F[4] = {f0, f1, f2, f3};
+    double fv[4], acc[4][3];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        fv[f] = f < nf ? F[f][v] : 0.0;
+        acc[f][0] = acc[f][1] = acc[f][2] = 0.0;
+    }
+    const int32_t b = np[v], e = np[v + 1];
+    for (int32_t c0 = b; c0 < e; c0 += kAG) {
+        const int32_t i = c0 + lane;
+        double p[4][3];
+        if (i < e) {
+            const int32_t nb = ni[i];
+            const double wx = gw[i], wy = gw[n_dir + i], wz = gw[2 * n_dir + i];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                const double dlt = f < nf ? F[f][nb] - fv[f] : 0.0;
+                p[f][0] = wx * dlt;
+                p[f][1] = wy * dlt;
+                p[f][2] = wz * dlt;
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) p[f][0] = p[f][1] = p[f][2] = 0.0;
+        }
+        const int cnt = min(kAG, (int)(e - c0));
+        for (int q = 0; q < cnt; ++q) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const double t = __shfl_sync(mask, p[f][c], q, kAG);
+                    acc[f][c] += t;
+                }
+        }
+    }
+    if (lane == 0) {
+        for (int f = 0; f < nf; ++f)
+            for (int c = 0; c < 3; ++c) out[((int64_t)f * 3 + c) * n + v] = acc[f][c];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_assemble_heat(HeatDev H) {
+    const int lane = threadIdx.x & (kAG - 1);
+    const int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kAG;
+    if (v >= H.n) return;
+    const unsigned mask = group_mask(kAG);
+    const int32_t kind = H.kind[v];
+    const int32_t rb = H.rp[v];
+    if (kind == ROW_DIRICHLET) {
+        if (lane == 0) {
+            H.val[rb] = 1.0;
+            H.b[v] = 0.0 + H.bcv[v];
+        }
+        return;
+    }
+    const int64_t N = H.n, D = H.n_dir;
+    const double kv = H.k[v];
+    const double gkx = H.gk[v], gky = H.gk[N + v], gkz = H.gk[2 * N + v];
+    const int32_t b = H.np[v], e = H.np[v + 1];
+    const int32_t dl = H.dloc[v];
+    double diag = 0.0;
+    for (int32_t c0 = b; c0 < e; c0 += kAG) {
+        const int32_t i = c0 + lane;
+        double cf = 0.0;
+        if (i < e) {
+            const int32_t nb = H.ni[i];
+            const double kn = H.k[nb];
+            const double sx = H.skew[i], sy = H.skew[D + i], sz = H.skew[2 * D + i];
+            const double km = (kv + kn != 0.0) ? 2.0 * kv * kn / (kv + kn) : 0.0;
+            double kf = km + 0.5 * (sx * (gkx + H.gk[nb]) + sy * (gky + H.gk[N + nb]) + sz * (gkz + H.gk[2 * N + nb]));
+            kf = kf > 0.0 ? kf : km;
+            cf = kf * H.area[i] / H.dist[i];
+            const int32_t loc = i - b;
+            H.val[rb + loc + (loc >= dl ? 1 : 0)] = cf;
+        }
+        const int cnt = min(kAG, (int)(e - c0));
+        for (int q = 0; q < cnt; ++q) {
+            const double t = __shfl_sync(mask, cf, q, kAG);
+            diag += -t;
+        }
+    }
+    if (lane != 0) return;
+    // production (implicit diagonal + lagged skew term) then source, then Neumann on flux nodes
+    const double sxc = H.cskew[v], syc = H.cskew[N + v], szc = H.cskew[2 * N + v];
+    const double vol = H.cvol[v];
+    const double sv = H.s[v];
+    const double prd_c = sv + H.gs[v] * sxc + H.gs[N + v] * syc + H.gs[2 * N + v] * szc;
+    const double unk_skew = H.gT[v] * sxc + H.gT[N + v] * syc + H.gT[2 * N + v] * szc;
+    diag += prd_c * vol;
+    H.val[rb + dl] = diag;
+    double bb = 0.0;
+    bb += -sv * unk_skew * vol;
+    const double src_c = H.q[v] + H.gq[v] * sxc + H.gq[N + v] * syc + H.gq[2 * N + v] * szc;
+    bb += -src_c * vol;
+    if (kind == ROW_FLUX) {
+        const int64_t B = H.n_bsub;
+        const double fv = H.bcv[v];
+        const int32_t my = H.node_bnd[v];
+        for (int32_t s = H.bp[v]; s < H.bp[v + 1]; ++s) {
+            const int32_t j = H.bj[s], k = H.bk[s];
+            const double fj = H.node_bnd[j] == my ? H.bcv[j] : fv;
+            const double fk = H.node_bnd[k] == my ? H.bcv[k] : fv;
+            bb += H.barea[s] * (H.bw[s] * fv + H.bw[B + s] * fj + H.bw[2 * B + s] * fk);
+        }
+    }
+    H.b[v] = bb;
+}
+
+// build_matrix from triplets: slot s receives the triplet values of its run, summed in push order.
+__global__ void k_values_from_triplets(int64_t nnz, const int64_t* __restrict__ sp, const int64_t* __restrict__ st,
+                                       const double* __restrict__ tv, double* __restrict__ val) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nnz) return;
+    double acc = 0.0;
+    for (int64_t t = sp[s]; t < sp[s + 1]; ++t) acc += tv[st[t]];
+    val[s] = acc;
+}
+
+void launch_grad(cudaStream_t s, int64_t n, const int32_t* np, const int32_t* ni, const double* gw, int64_t n_dir, int nf,
+                 const double* const* f, double* out) {
+    const int64_t threads = n * kAG;
+    const int blocks = (int)((threads + 255) / 256);
+    k_grad_lsq<<<blocks, 256, 0, s>>>(n, np, ni, gw, n_dir, nf, f[0], nf > 1 ? f[1] : nullptr, nf > 2 ? f[2] : nullptr,
+                                       nf > 3 ? f[3] : nullptr, out);
+}
+
+void launch_assemble_heat(cudaStream_t s, const HeatDev& H) {
+    const int64_t threads = H.n * kAG;
+    const int blocks = (int)((threads + 255) / 256);
+    k_assemble_heat<<<blocks, 256, 0, s>>>(H);
+}
+
+void launch_values_from_triplets(cudaStream_t s, int64_t nnz, const int64_t* sp, const int64_t* st, const double* tv, double* val) {
+    const int blocks = (int)((nnz + 255) / 256);
+    if (blocks > 0) k_values_from_triplets<<<blocks, 256, 0, s>>>(nnz, sp, st, tv, val);
+}
+
+}  // namespace vfv

@@ -1,0 +1,366 @@
+// Krylov-subspace kernels for the restarted GMRES (sm_100a).
+//
+// The reference solves with faer_gmres::restarted_gmres + JacobiPreconLinOp
+// (src/linear/linear_gmres.rs:76-84). Restated here from the published algorithm
+// (Saad & Schultz 1986, right preconditioning, Givens least squares) with these device choices:
+//   * basis vectors u_i are stored UNNORMALISED, with their norms beta_i in a device array;
+//     v_i = u_i / beta_i. The SpMV of step j multiplies by 1/beta_j on the way out, so no separate
+//     normalisation pass over the basis is ever made;
+//   * orthogonalisation is classical Gram-Schmidt with one re-orthogonalisation (CGS2), which has
+//     the stability of modified Gram-Schmidt; each pass is one multi-vector kernel that streams the
+//     block's rows of every basis vector once, accumulates per-warp partial dots, and reduces them
+//     deterministically (fixed order, no float atomics) in the last block to finish;
+//   * the Hessenberg column, the Givens rotation and the residual estimate are finished by that last
+//     block, so a whole restart cycle runs without a host synchronisation and is captured in a CUDA
+//     graph. Every kernel first reads DevStatus::done and returns at once after convergence.
+// Vectors are of type T (double, or float in the mixed-precision inner solve); all dots, norms,
+// the Hessenberg matrix and the rotations are double.
+#pragma once
+#include "../common.cuh"
+
+namespace vfv {
+
+constexpr int kBlk = 256;        // threads per block of the vector kernels
+constexpr int kRows = 4;         // rows per thread in the multi-vector kernels
+constexpr int kMaxBasis = 128;   // m + 1 <= kMaxBasis
+
+// Per-solve device workspace pointers used by the Krylov kernels.
+struct KrylovDev {
+    int64_t n;          // rows
+    int64_t ldv;        // stride between basis vectors (elements)
+    int m;              // restart length
+    int nblk;           // blocks of the multi-vector kernels
+    double* part;       // [kMaxBasis][nblk] per-block partial dots
+    unsigned* counter;  // [4] last-block counters
+    double* hacc;       // [kMaxBasis] current Hessenberg column (accumulated over the CGS passes)
+    double* coef;       // [kMaxBasis] update coefficients d_i / beta_i^2
+    double* H;          // [m][m+1] column-major Hessenberg (rotated in place)
+    double* cs;         // [m]
+    double* sn;         // [m]
+    double* g;          // [m+1]
+    double* beta;       // [m+1] norms of the stored basis vectors
+    double* inv_beta;   // [m+1]
+    double* y;          // [m] least-squares solution scaled by 1/beta_i
+    DevStatus* st;
+    const double* scal; // [0] tol_abs: converged when ||r|| <= tol_abs
+                        // [1] inner_floor_rel: a cycle also stops once resid_est <= inner_floor_rel * beta0
+};
+
+// ---------------------------------------------------------------- last-block helper
+__device__ __forceinline__ bool last_block_arrive(unsigned* counter) {
+    __shared__ bool s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(counter, 1u);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last;
+}
+
+// Sum column c of part[c][0..nblk) with all threads of the block, in a fixed order; valid in thread 0.
+__device__ __forceinline__ double reduce_partials(const double* part, int nblk, double* red) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += __ldcg(part + b);
+    return block_sum(s, red);
+}
+
+// ---------------------------------------------------------------- SpMV (CSR, G lanes per row)
+// y = scale * (A x). Accumulation in TA. `scale` may be null (= 1).
+template <typename TV, typename TX, typename TY, typename TA, int G>
+__global__ void __launch_bounds__(kBlk) k_spmv(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                              const TV* __restrict__ val, const TX* __restrict__ x, TY* __restrict__ y,
+                                              const double* __restrict__ scale, const DevStatus* __restrict__ st) {
+    if (st && st->done) return;
+    const int lane = threadIdx.x & (G - 1);
+    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    TA s = TA(0);
+    if (row < n) {
+        const int32_t b = __ldg(rp + row), e = __ldg(rp + row + 1);
+        for (int32_t k = b + lane; k < e; k += G) s += (TA)__ldcs(val + k) * (TA)__ldg(x + __ldcs(ci + k));
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
+    if (lane == 0 && row < n) {
+        const double sc = scale ? *scale : 1.0;
+        y[row] = (TY)((double)s * sc);
+    }
+}
+
+// ---------------------------------------------------------------- residual r = b - A x (FP64)
+// Writes u0 = r (type T), accumulates ||r||^2, and in the last block starts a new cycle:
+// beta[0] = ||r||, g = (beta0, 0, ...), done/converged flags.
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlk) k_residual(KrylovDev K, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                  const double* __restrict__ val, const double* __restrict__ x,
+                                                  const double* __restrict__ b, T* __restrict__ u0) {
+    __shared__ double red[kBlk / 32];
+    const int lane = threadIdx.x & (G - 1);
+    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    double s = 0.0;
+    if (row < K.n) {
+        const int32_t b0 = __ldg(rp + row), e = __ldg(rp + row + 1);
+        for (int32_t k = b0 + lane; k < e; k += G) s += __ldcs(val + k) * __ldg(x + __ldcs(ci + k));
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
+    double r2 = 0.0;
+    if (lane == 0 && row < K.n) {
+        const double r = b[row] - s;
+        u0[row] = (T)r;
+        r2 = r * r;
+    }
+    const double bs = block_sum(r2, red);
+    if (threadIdx.x == 0) K.part[blockIdx.x] = bs;
+    if (!last_block_arrive(K.counter)) return;
+    const double tot = reduce_partials(K.part, gridDim.x, red);
+    if (threadIdx.x == 0) {
+        *K.counter = 0u;
+        const double beta0 = sqrt(tot);
+        K.beta[0] = beta0;
+        K.inv_beta[0] = 1.0 / beta0;
+        K.g[0] = beta0;
+        DevStatus* st = K.st;
+        st->steps = 0;
+        st->beta0 = beta0;
+        st->resid_est = beta0;
+        const bool fin = isfinite(beta0);
+        st->nonfinite = fin ? 0 : 1;
+        const bool conv = fin && beta0 <= K.scal[0];
+        st->converged = conv ? 1 : 0;
+        st->done = (conv || !fin || beta0 == 0.0) ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------- multi-dot (first CGS pass)
+// d_i = <u_i, w> for i < nvec. Last block: hacc[i] = d_i / beta_i, coef[i] = d_i / beta_i^2.
+template <typename T>
+__global__ void __launch_bounds__(kBlk) k_mdot(KrylovDev K, const T* __restrict__ V, const T* __restrict__ w, int nvec) {
+    if (K.st->done) return;
+    __shared__ double red[kMaxBasis][kBlk / 32];
+    __shared__ double red2[kBlk / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t base = (int64_t)blockIdx.x * (kBlk * kRows) + threadIdx.x;
+    double wr[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+        const int64_t row = base + r * kBlk;
+        wr[r] = row < K.n ? (double)w[row] : 0.0;
+    }
+    for (int i = 0; i < nvec; ++i) {
+        const T* u = V + (int64_t)i * K.ldv;
+        double s = 0.0;
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+            const int64_t row = base + r * kBlk;
+            if (row < K.n) s += (double)u[row] * wr[r];
+        }
+        s = warp_sum(s);
+        if (lane == 0) red[i][wid] = s;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+        double s = 0.0;
+        for (int q = 0; q < nw; ++q) s += red[i][q];
+        K.part[(int64_t)i * K.nblk + blockIdx.x] = s;
+    }
+    if (!last_block_arrive(K.counter + 1)) return;
+    for (int i = 0; i < nvec; ++i) {
+        const double d = reduce_partials(K.part + (int64_t)i * K.nblk, gridDim.x, red2);
+        if (threadIdx.x == 0) {
+            K.hacc[i] = d * K.inv_beta[i];
+            K.coef[i] = d * K.inv_beta[i] * K.inv_beta[i];
+        }
+    }
+    if (threadIdx.x == 0) K.counter[1] = 0u;
+}
+
+// ---------------------------------------------------------------- update + second pass
+// w <- w - sum_i coef_i u_i. Then, with FINAL == false, the second CGS pass d'_i = <u_i, w>
+// (last block adds d'_i/beta_i into hacc and sets coef); with FINAL == true, ||w||^2 and the
+// last block finishes the Hessenberg column j, the Givens rotation and the convergence test.
+template <typename T, bool FINAL>
+__global__ void __launch_bounds__(kBlk) k_update(KrylovDev K, const T* __restrict__ V, T* __restrict__ w, int nvec, int j) {
+    if (K.st->done) return;
+    __shared__ double red[kMaxBasis][kBlk / 32];
+    __shared__ double red2[kBlk / 32];
+    __shared__ double s_coef[kMaxBasis];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) s_coef[i] = K.coef[i];
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * (kBlk * kRows) + threadIdx.x;
+    double acc[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) acc[r] = 0.0;
+    for (int i = 0; i < nvec; ++i) {
+        const T* u = V + (int64_t)i * K.ldv;
+        const double c = s_coef[i];
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+            const int64_t row = base + r * kBlk;
+            if (row < K.n) acc[r] += c * (double)u[row];
+        }
+    }
+    double wr[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+        const int64_t row = base + r * kBlk;
+        if (row < K.n) {
+            const T nv = (T)((double)w[row] - acc[r]);
+            w[row] = nv;
+            wr[r] = (double)nv;
+        } else {
+            wr[r] = 0.0;
+        }
+    }
+    if (!FINAL) {
+        for (int i = 0; i < nvec; ++i) {
+            const T* u = V + (int64_t)i * K.ldv;
+            double s = 0.0;
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) {
+                const int64_t row = base + r * kBlk;
+                if (row < K.n) s += (double)u[row] * wr[r];
+            }
+            s = warp_sum(s);
+            if (lane == 0) red[i][wid] = s;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+            double s = 0.0;
+            for (int q = 0; q < nw; ++q) s += red[i][q];
+            K.part[(int64_t)i * K.nblk + blockIdx.x] = s;
+        }
+        if (!last_block_arrive(K.counter + 2)) return;
+        for (int i = 0; i < nvec; ++i) {
+            const double d = reduce_partials(K.part + (int64_t)i * K.nblk, gridDim.x, red2);
+            if (threadIdx.x == 0) {
+                K.hacc[i] += d * K.inv_beta[i];
+                K.coef[i] = d * K.inv_beta[i] * K.inv_beta[i];
+            }
+        }
+        if (threadIdx.x == 0) K.counter[2] = 0u;
+    } else {
+        double s = 0.0;
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) s += wr[r] * wr[r];
+        s = block_sum(s, red2);
+        if (threadIdx.x == 0) K.part[blockIdx.x] = s;
+        if (!last_block_arrive(K.counter + 3)) return;
+        const double tot = reduce_partials(K.part, gridDim.x, red2);
+        if (threadIdx.x == 0) {
+            K.counter[3] = 0u;
+            const int m1 = K.m + 1;
+            double* col = K.H + (int64_t)j * m1;
+            const double bnext = sqrt(tot);
+            for (int i = 0; i <= j; ++i) col[i] = K.hacc[i];
+            col[j + 1] = bnext;
+            K.beta[j + 1] = bnext;
+            K.inv_beta[j + 1] = 1.0 / bnext;
+            for (int i = 0; i < j; ++i) {
+                const double a = col[i], bb = col[i + 1];
+                col[i] = K.cs[i] * a + K.sn[i] * bb;
+                col[i + 1] = -K.sn[i] * a + K.cs[i] * bb;
+            }
+            const double a = col[j], bb = col[j + 1];
+            const double rr = hypot(a, bb);
+            double c = 1.0, sgn = 0.0;
+            if (rr > 0.0) {
+                c = a / rr;
+                sgn = bb / rr;
+            }
+            K.cs[j] = c;
+            K.sn[j] = sgn;
+            col[j] = rr;
+            col[j + 1] = 0.0;
+            const double gj = K.g[j];
+            K.g[j] = c * gj;
+            K.g[j + 1] = -sgn * gj;
+            const double est = fabs(K.g[j + 1]);
+            DevStatus* st = K.st;
+            st->steps = j + 1;
+            st->total_steps += 1;
+            st->resid_est = est;
+            const bool fin = isfinite(est) && isfinite(bnext) && isfinite(rr);
+            if (!fin) st->nonfinite = 1;
+            const double floor_abs = K.scal[1] * st->beta0;
+            const bool stop = !fin || rr == 0.0 || bnext == 0.0 || est <= K.scal[0] || est <= floor_abs || j + 1 >= K.m;
+            if (stop) st->done = 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- end of cycle
+// Back substitution R y = g on the rotated Hessenberg (k = steps), y_i scaled by 1/beta_i.
+__global__ void k_backsolve(KrylovDev K) {
+    if (threadIdx.x != 0) return;
+    const int k = K.st->steps;
+    const int m1 = K.m + 1;
+    for (int i = k - 1; i >= 0; --i) {
+        double s = K.g[i];
+        for (int q = i + 1; q < k; ++q) s -= K.H[(int64_t)q * m1 + i] * K.y[q];
+        K.y[i] = s / K.H[(int64_t)i * m1 + i];
+    }
+    for (int i = 0; i < k; ++i) K.y[i] *= K.inv_beta[i];
+    for (int i = k; i < K.m; ++i) K.y[i] = 0.0;
+}
+
+// z = sum_i y_i u_i (i < steps). MODE 0: x += z; MODE 1: x += dinv .* z; MODE 2: zt = (T)z for a preconditioner.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kBlk) k_combine(KrylovDev K, const T* __restrict__ V, double* __restrict__ x,
+                                                 const double* __restrict__ dinv, T* __restrict__ zt) {
+    __shared__ double s_y[kMaxBasis];
+    const int k = K.st->steps;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) s_y[i] = K.y[i];
+    __syncthreads();
+    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= K.n) return;
+    double z = 0.0;
+    for (int i = 0; i < k; ++i) z += s_y[i] * (double)V[(int64_t)i * K.ldv + row];
+    if (MODE == 0) x[row] += z;
+    if (MODE == 1) x[row] += dinv[row] * z;
+    if (MODE == 2) zt[row] = (T)z;
+}
+
+template <typename T>
+__global__ void k_add_to_x(int64_t n, double* __restrict__ x, const T* __restrict__ z) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += (double)z[i];
+}
+
+// ||v||^2 into out (single pass, last-block reduction)
+__global__ void __launch_bounds__(kBlk) k_norm2(int64_t n, const double* __restrict__ v, double* part, unsigned* counter, double* out) {
+    __shared__ double red[kBlk / 32];
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += v[i] * v[i];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (!last_block_arrive(counter)) return;
+    const double tot = reduce_partials(part, gridDim.x, red);
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        *out = tot;
+    }
+}
+
+// ---------------------------------------------------------------- matrix preparation
+// dinv[i] = 1 / a_ii (diag_pos[i] = slot of the diagonal, -1 if absent -> 1)
+__global__ void k_jacobi_inv(int64_t n, const int32_t* __restrict__ diag_pos, const double* __restrict__ val, double* __restrict__ dinv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t p = diag_pos[i];
+    const double d = p >= 0 ? val[p] : 0.0;
+    dinv[i] = d != 0.0 ? 1.0 / d : 1.0;
+}
+
+// out[k] = (T)(val[k] * dinv[col[k]])  (right Jacobi scaling folded into the Krylov matrix)
+template <typename T>
+__global__ void k_scale_cols(int64_t nnz, const int32_t* __restrict__ ci, const double* __restrict__ val,
+                             const double* __restrict__ dinv, T* __restrict__ out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nnz) out[k] = (T)(val[k] * (dinv ? dinv[ci[k]] : 1.0));
+}
+
+}  // namespace vfv

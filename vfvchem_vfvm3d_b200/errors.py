@@ -1,0 +1,52 @@
+"""Error types mirroring the reference's ``VFVChemError`` variants for the linear solver
+(src/base/error.rs:219-268). Non-zero status codes of the C ABI map onto them."""
+from __future__ import annotations
+
+
+class VFVChemError(RuntimeError):
+    """Base class (the reference's ``#[non_exhaustive] enum VFVChemError``, error.rs:1-5)."""
+
+    code = -1
+
+
+class LinearGmresDidNotConverge(VFVChemError):
+    """``LinearGmresDidNotConverge { message }`` (error.rs:265-268; raised at linear_gmres.rs:81)."""
+
+    code = 1
+
+
+class LinearGmresNonFinite(VFVChemError):
+    code = 2
+
+
+class LinearGmresBadInput(VFVChemError, ValueError):
+    code = 3
+
+
+class LinearGmresCudaError(VFVChemError):
+    code = 4
+
+
+class LinearGmresNonPositiveThreads(LinearGmresBadInput):
+    """``LinearGmresNonPositiveThreads { num_thread }`` (linear_gmres.rs:26-28)."""
+
+
+class LinearGmresNonPositiveTolerance(LinearGmresBadInput):
+    """``LinearGmresNonPositiveTolerance { tol }`` (linear_gmres.rs:29-31)."""
+
+
+class LinearGmresNonPositiveRestart(LinearGmresBadInput):
+    """``LinearGmresNonPositiveRestart { restart }`` (linear_gmres.rs:32-34)."""
+
+
+class LinearGmresNonPositiveMaxOuter(LinearGmresBadInput):
+    """``LinearGmresNonPositiveMaxOuter { max_outer }`` (linear_gmres.rs:35-37)."""
+
+
+_BY_CODE = {1: LinearGmresDidNotConverge, 2: LinearGmresNonFinite, 3: LinearGmresBadInput, 4: LinearGmresCudaError}
+
+
+def raise_for(code: int, message: str) -> None:
+    if code == 0:
+        return
+    raise _BY_CODE.get(code, VFVChemError)(message)
