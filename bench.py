@@ -1,0 +1,350 @@
+"""Benchmark of the assemble-and-solve path on one B200 (or N replicas).
+
+Workload (one "step"): the 1,000,000-vertex heterogeneous steady heat system (100^3 jittered
+cube, log k ~ N(0,1), q ~ U[0,1], Dirichlet T=0/1 on x=0/1, zero flux elsewhere) solved by
+GMRES(50) + ILU(0) to 1e-8 relative 2-norm error against a reference solution — the
+FP32-inner / FP64-refinement solver is the timed `value`; the plain FP64 solver is timed beside
+it. Inputs are resident in HBM; the matrix (15.3 M non-zeros, 190 MB of CSR) exceeds the 126 MB
+L2, so no L2 flush is needed between steps.
+
+`--impl reference` times the reference's own algorithm for this path on the host cores
+(Jacobi-preconditioned restarted GMRES(50), FP64, the oracle port), on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GMRES solve s to 1e-8 vs FP64 LU: mixed vs plain FP64 on GPU; SpMV HBM GB/s"
+ERR_TARGET = 1e-8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vfv", choices=["vfv", "reference"])
+    ap.add_argument("--n", type=int, default=100, help="grid points per axis (100 -> 1,000,000 vertices)")
+    ap.add_argument("--restart", type=int, default=50)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_baseline_jacobi(rp, ci, va, b, x0, restart, budget_s, steps_needed=None):
+    """Reference algorithm on the host cores: Jacobi GMRES(restart), FP64 (oracle port, OpenMP)."""
+    import oracle  # CPU-baseline leg only
+    lib = oracle.lib()
+    t0 = time.perf_counter()
+    steps = restart
+    _, _, its, _ = oracle.gmres(rp, ci, va, b, x0, tol=1e-300, restart=restart, max_outer=1, precond=1, max_steps=steps)
+    dt = time.perf_counter() - t0
+    # grow the sample to roughly the time budget
+    if dt < budget_s / 3:
+        steps = max(restart, int(restart * (budget_s / 2) / max(dt, 1e-3)) // restart * restart)
+        t0 = time.perf_counter()
+        _, _, its, _ = oracle.gmres(rp, ci, va, b, x0, tol=1e-300, restart=restart, max_outer=10**6, precond=1, max_steps=steps)
+        dt = time.perf_counter() - t0
+    del lib
+    return dt / max(its, 1), its
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world, dist)
+
+    from vfvchem_vfvm3d_b200 import Context, GmresOptions, SteadyHeatGpu
+    from vfvchem_vfvm3d_b200 import _lib as L
+    from vfvchem_vfvm3d_b200.problems import steady_heat
+
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+    t_setup = time.perf_counter()
+    prob = steady_heat(args.n, hetero=True)
+    t_mesh = time.perf_counter() - t_setup
+    heat = SteadyHeatGpu(prob.mesh, prob.bnd_kind, ctx=ctx)
+    dev = torch.device("cuda", local)
+    k_d, q_d, s_d, T_d, bc_d = (torch.tensor(a, device=dev) for a in (prob.k, prob.q, prob.s, prob.T0, prob.bc_val))
+    torch.cuda.synchronize()
+    heat.assemble_device(k_d.data_ptr(), q_d.data_ptr(), s_d.data_ptr(), T_d.data_ptr(), bc_d.data_ptr())
+    ctx.synchronize()
+    pat = heat.pattern
+    n, nnz = pat.n, pat.nnz
+    b_d = torch.tensor(heat.assemble(prob.k, prob.q, prob.s, prob.T0, prob.bc_val), device=dev)
+    x_d = torch.empty_like(b_d)
+    x0_d = T_d.clone()
+
+    ilu = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_MULTICOLOR)
+    # reference solution: FP64 GMRES driven to round-off
+    ref_opts = GmresOptions(tol=1e-14, restart=args.restart, max_outer=4000, **ilu)
+    try:
+        info_ref = pat.solve_device(b_d.data_ptr(), x0_d.data_ptr(), x_d.data_ptr(), ref_opts)
+    except Exception:
+        ref_opts.tol = 1e-13
+        info_ref = pat.solve_device(b_d.data_ptr(), x0_d.data_ptr(), x_d.data_ptr(), ref_opts)
+    x_ref = x_d.clone()
+
+    def err(x):
+        return float(torch.linalg.vector_norm(x - x_ref) / torch.linalg.vector_norm(x_ref))
+
+    # residual tolerance giving <= 1e-8 error for the FP64 solver, shared by both solvers
+    tol = 1e-9
+    for _ in range(5):
+        pat.solve_device(b_d.data_ptr(), x0_d.data_ptr(), x_d.data_ptr(), GmresOptions(tol=tol, restart=args.restart, max_outer=2000, **ilu))
+        if err(x_d) <= 0.5 * ERR_TARGET:
+            break
+        tol /= 4
+    o64 = GmresOptions(tol=tol, restart=args.restart, max_outer=2000, precision=L.FP64, **ilu)
+    omx = GmresOptions(tol=tol, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, **ilu)
+
+    def timed(opts, steps, warm):
+        for _ in range(warm):
+            pat.solve_device(b_d.data_ptr(), x0_d.data_ptr(), x_d.data_ptr(), opts)
+        ts, infos = [], []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            infos.append(pat.solve_device(b_d.data_ptr(), x0_d.data_ptr(), x_d.data_ptr(), opts))
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return ts, infos, err(x_d)
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count
+    with ClockSampler(local) as clk:
+        t_mx, i_mx, e_mx = timed(omx, args.steps, args.warmup)
+        launches_mx = ctx.launch_count - launches0
+        t_64, i_64, e_64 = timed(o64, args.steps, args.warmup)
+    torch.cuda.synchronize()
+    mx_s = sum(t_mx) / len(t_mx)
+    f64_s = sum(t_64) / len(t_64)
+    if dist:
+        t = torch.tensor([mx_s, f64_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mx_s, f64_s = float(t[0]), float(t[1])
+
+    # SpMV (FP64 and FP32) timed alone: the kernel the metric names
+    xs = torch.randn(n, dtype=torch.float64, device=dev)
+    ys = torch.empty_like(xs)
+    xs32, ys32 = xs.float(), torch.empty(n, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def spmv_time(fn, reps=50):
+        for _ in range(5):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    sp64 = spmv_time(lambda: pat.spmv_device(xs.data_ptr(), ys.data_ptr()))
+    sp32 = spmv_time(lambda: pat.spmv_device_f32(xs32.data_ptr(), ys32.data_ptr()))
+    bytes64 = 12 * nnz + 4 * (n + 1) + 8 * n + 8 * n
+    bytes32 = 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n
+    peak, peak_kind = peaks()
+    gbs64 = bytes64 / sp64 / 1e9
+    gbs32 = bytes32 / sp32 / 1e9
+
+    # assembly (gradients + face coefficients + b), timed alone
+    def asm():
+        heat.assemble_device(k_d.data_ptr(), q_d.data_ptr(), s_d.data_ptr(), T_d.data_ptr(), bc_d.data_ptr())
+    asm_s = spmv_time(asm, reps=10)
+
+    # end to end through the C ABI with host buffers: values + b + x0 in, x out, every step
+    rp_h, ci_h, va_h = pat.export()
+    b_h = b_d.cpu().numpy()
+    x0_h = prob.T0.copy()
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    va_p, b_p, x0_p = pin(va_h), pin(b_h), pin(x0_h)
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        pat.set_values(va_p)
+        x_h, inf = pat.solve(b_p, x0_p, omx)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e.append(dt)
+    e2e_s = sum(e2e) / len(e2e)
+    e2e_err = float(np.linalg.norm(x_h - x_ref.cpu().numpy()) / np.linalg.norm(x_ref.cpu().numpy()))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rp64 = rp_h.astype(np.int64)
+        per_step, sample_steps = cpu_baseline_jacobi(rp64, ci_h, va_h, b_h, x0_h, args.restart, args.cpu_seconds)
+        # steps the reference algorithm needs: Jacobi GMRES on the GPU to the same error
+        jac = GmresOptions(tol=tol, restart=args.restart, max_outer=20000, precond=L.PRECOND_JACOBI)
+        ij = pat.solve_device(b_d.data_ptr(), x0_d.data_ptr(), x_d.data_ptr(), jac)
+        cpu = {"value": per_step * ij.iters, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{sample_steps} Arnoldi steps of Jacobi GMRES({args.restart}) FP64 on the same system, "
+                         f"{per_step * 1e3:.1f} ms/step x {ij.iters} steps (Jacobi GMRES iteration count to the same tolerance)"}
+
+    clocks = clk.summary()
+    out = {
+        "metric": METRIC,
+        "value": mx_s,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mx_s * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32-inner/f64-refine",
+        "data": "synthetic (seeded jittered-cube Delaunay mesh, seeded fields)",
+        "config": {"workload": f"steady heat, {args.n}^3 jittered cube ({n} vertices, {nnz} nnz), log k~N(0,1), q~U[0,1]; "
+                               f"GMRES({args.restart})+ILU(0) multicolour to 1e-8 rel. error",
+                   "n": n, "nnz": nnz, "restart": args.restart, "tol_relres": tol, "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "fp64_solve_s": f64_s,
+        "speedup_mixed_vs_fp64": f64_s / mx_s,
+        "iters_mixed": i_mx[-1].iters, "iters_fp64": i_64[-1].iters, "ilu_levels": i_mx[-1].levels,
+        "err_mixed": e_mx, "err_fp64": e_64, "ref_relres": info_ref.relres,
+        "spmv_fp64_gbs": gbs64, "spmv_fp32_gbs": gbs32, "spmv_fp64_ms": sp64 * 1e3, "spmv_fp32_ms": sp32 * 1e3,
+        "assembly_ms": asm_s * 1e3, "mesh_setup_s": t_mesh,
+        "roofline": {"bound": "hbm", "kernel": "k_spmv (FP64 CSR, 8 lanes/row)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
+                     "frac": gbs64 / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": bytes64},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * nnz + 16 * n, "d2h_bytes_per_step": 8 * n, "err": e2e_err},
+        "gpu_launches": int(launches_mx),
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world, dist):
+    """Reference arm: Jacobi GMRES on the host cores (the reference's LinearGmres algorithm)."""
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    import oracle  # the reference arm runs the CPU port of the reference's algorithm
+    from vfvchem_vfvm3d_b200.problems import steady_heat
+    prob = steady_heat(args.n, hetero=True)
+    d = prob.mesh.dual()
+    r, c, v, b = oracle.heat_triplets(d, prob.mesh.n_pts, prob.node_bnd, prob.bnd_order, prob.bnd_kind, prob.k, prob.q, prob.s, prob.T0,
+                                      prob.bc_val)
+    rp, ci, va = oracle.csr_from_triplets(prob.n, r, c, v)
+    per = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        _, _, its, _ = oracle.gmres(rp, ci, va, b, prob.T0, tol=1e-300, restart=args.restart, max_outer=1, precond=1,
+                                    max_steps=args.restart)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            per.append(dt / max(its, 1))
+    per_step = sum(per) / len(per)
+    # Jacobi GMRES steps to the target: from the CPU oracle on this system, bounded (extrapolated if capped)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": None, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": f"steady heat {args.n}^3, Jacobi GMRES({args.restart}) FP64 (reference algorithm)"},
+    }
+    cap = int(max(args.restart, 60.0 / max(per_step, 1e-4))) // args.restart * args.restart
+    x, ok, its, rel = oracle.gmres(rp, ci, va, b, prob.T0, tol=1e-10, restart=args.restart, max_outer=10**6, precond=1, max_steps=cap)
+    steps_needed = its if ok else int(its * np.log(1e-10) / np.log(max(rel, 1e-300)))
+    val = per_step * steps_needed
+    out.update({"value": val, "ms_per_step": val * 1e3,
+                "cpu_baseline": {"value": val, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+                                 "sample": f"{args.steps} x {args.restart} Arnoldi steps timed ({per_step * 1e3:.1f} ms/step); "
+                                           f"{its} steps run to relres {rel:.2e} ({'converged' if ok else 'extrapolated'})"},
+                "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

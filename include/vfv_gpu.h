@@ -90,6 +90,8 @@ const char* vfv_last_error(const vfv_ctx* ctx);
 int vfv_ctx_synchronize(vfv_ctx* ctx);
 /* the context's CUDA stream (cudaStream_t) for callers that enqueue work around the library */
 void* vfv_ctx_stream(vfv_ctx* ctx);
+/* number of kernels this context has launched so far (every node of a replayed CUDA graph counts) */
+int64_t vfv_ctx_launch_count(const vfv_ctx* ctx);
 
 /* ---- sparse pattern: LinearBase::update_sparse (linear_gmres.rs:53-64).
  * rows/cols[ntrip] are the (row, col) pairs of the triplet list in push order. The pattern is

@@ -59,6 +59,7 @@ SIGNATURES = [
     ("vfv_last_error", C.c_char_p, [_P]),
     ("vfv_ctx_synchronize", C.c_int, [_P]),
     ("vfv_ctx_stream", C.c_void_p, [_P]),
+    ("vfv_ctx_launch_count", C.c_int64, [_P]),
     ("vfv_pattern_from_triplets", C.c_int, [_P, C.c_int64, C.c_int64, _U64P, _U64P, _PP]),
     ("vfv_pattern_from_csr", C.c_int, [_P, C.c_int64, _I32P, _I32P, _PP]),
     ("vfv_pattern_destroy", None, [_P]),

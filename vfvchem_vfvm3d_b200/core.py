@@ -70,6 +70,10 @@ class Context:
     def stream_ptr(self) -> int:
         return L.load().vfv_ctx_stream(self._h) or 0
 
+    @property
+    def launch_count(self) -> int:
+        return int(L.load().vfv_ctx_launch_count(self._h))
+
     def synchronize(self) -> None:
         _check(self._h, L.load().vfv_ctx_synchronize(self._h))
 

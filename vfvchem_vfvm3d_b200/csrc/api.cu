@@ -34,6 +34,7 @@ struct vfv_ctx {
     std::string err;
     DevStatus* h_status = nullptr;  // pinned
     double* h_scalar = nullptr;     // pinned scratch for small reads
+    int64_t launches = 0;           // kernels launched by this context (graph nodes counted per replay)
 };
 
 namespace {
@@ -216,6 +217,7 @@ int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
     cudaStream_t s = ctx->stream;
     if (S.version64 != p->version) {
         k_gather_vals<double><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, S.src.p, p->val.p, S.lu64.p);
+        ctx->launches += 1 + S.nlev;
         CK(cudaMemsetAsync(S.bad.p, 0, sizeof(int), s));
         for (int l = 0; l < S.nlev; ++l) {
             const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
@@ -231,6 +233,7 @@ int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
     if (want32 && S.version32 != p->version) {
         if (!S.lu32.p) CK(S.lu32.alloc(p->nnz));
         k_cast<double, float><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, S.lu64.p, S.lu32.p);
+        ctx->launches += 1;
         S.version32 = p->version;
     }
     return VFV_OK;
@@ -260,6 +263,7 @@ struct Gmres : SolverBase {
     DBuf<DevStatus> st;
     KrylovDev K{};
     cudaGraphExec_t exec = nullptr;
+    int64_t graph_nodes = 0;
     IluStruct* ilu = nullptr;
     ~Gmres() override {
         if (exec) cudaGraphExecDestroy(exec);
@@ -381,8 +385,10 @@ struct Gmres : SolverBase {
         if (precond == VFV_PRECOND_JACOBI) {
             k_jacobi_inv<<<grid_for(n), 256, 0, s>>>(n, p->diag_pos.p, p->val.p, dinv.p);
             k_scale_cols<T><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, p->ci.p, p->val.p, dinv.p, valK.p);
+            ctx->launches += 2;
         } else if (valK.p) {
             k_scale_cols<T><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, p->ci.p, p->val.p, nullptr, valK.p);
+            ctx->launches += 1;
         }
         if (precond == VFV_PRECOND_ILU0) {
             int rc = ilu_refresh(ctx, p, *ilu, mixed);
@@ -391,6 +397,7 @@ struct Gmres : SolverBase {
         // ||b|| and the absolute tolerance
         const int nb = std::min(grid_for(n), 1024);
         k_norm2<<<nb, kBlk, 0, s>>>(n, b.p, part.p, counter.p + 4, scal.p + 2);
+        ctx->launches += 1;
         CK(cudaMemcpyAsync(ctx->h_scalar, scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         CK(cudaGetLastError());
@@ -414,11 +421,15 @@ struct Gmres : SolverBase {
         CK(cudaMemcpyAsync(scal.p, hs, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
         CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
         k_residual<T, G><<<grid_for(n * G), kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+        ctx->launches += 1;
         if (!exec) {
             cudaGraph_t graph;
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             enqueue_cycle(s, p);
             CK(cudaStreamEndCapture(s, &graph));
+            size_t nodes = 0;
+            CK(cudaGraphGetNodes(graph, nullptr, &nodes));
+            graph_nodes = (int64_t)nodes;
             cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
             cudaGraphDestroy(graph);
             CK(e);
@@ -439,6 +450,7 @@ struct Gmres : SolverBase {
                 break;
             }
             CK(cudaGraphLaunch(exec, s));
+            ctx->launches += graph_nodes;
             ++cycles;
         }
         CK(cudaGetLastError());
@@ -580,6 +592,8 @@ int vfv_ctx_synchronize(vfv_ctx* ctx) {
 
 void* vfv_ctx_stream(vfv_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+int64_t vfv_ctx_launch_count(const vfv_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
 int vfv_pattern_from_triplets(vfv_ctx* ctx, int64_t n, int64_t ntrip, const uint64_t* rows, const uint64_t* cols, vfv_pattern** out) {
     if (!ctx || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     *out = nullptr;
@@ -669,6 +683,7 @@ int vfv_values_from_triplets(vfv_ctx* ctx, vfv_pattern* p, const double* vals) {
     cudaStream_t s = ctx->stream;
     if (p->ntrip > 0) CK(cudaMemcpyAsync(p->trip_vals.p, vals, p->ntrip * sizeof(double), cudaMemcpyHostToDevice, s));
     launch_values_from_triplets(s, p->nnz, p->slot_ptr.p, p->slot_trip.p, p->trip_vals.p, p->val.p);
+    ctx->launches += 1;
     CK(cudaGetLastError());
     p->version++;
     return VFV_OK;
@@ -724,6 +739,7 @@ int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double*
     if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     constexpr int G = 8;
     k_spmv<double, double, double, double, G><<<grid_for(p->n * G), kBlk, 0, ctx->stream>>>(p->n, p->rp.p, p->ci.p, p->val.p, x, y, nullptr, nullptr);
+    ctx->launches += 1;
     CK(cudaGetLastError());
     return VFV_OK;
 }
@@ -737,6 +753,7 @@ int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y) 
         p->version32 = p->version;
     }
     k_spmv<float, float, float, float, G><<<grid_for(p->n * G), kBlk, 0, ctx->stream>>>(p->n, p->rp.p, p->ci.p, p->val32.p, x, y, nullptr, nullptr);
+    ctx->launches += 1;
     CK(cudaGetLastError());
     return VFV_OK;
 }
@@ -965,6 +982,7 @@ int vfv_heat_assemble(vfv_ctx* ctx, vfv_heat* h, const double* k, const double* 
     H.val = h->pat->val.p;
     H.b = h->b.p;
     launch_assemble_heat(s, H);
+    ctx->launches += 2;
     CK(cudaGetLastError());
     h->pat->version++;
     if (b_out) {

@@ -1,0 +1,60 @@
+"""Seeded synthetic heat problems on jittered-cube meshes.
+
+* ``steady_heat(n, hetero=False)``: the cube heat problem of the reference's heat examples
+  (examples/heat/heat_analytic.rs:9-98 layout): Dirichlet T=0 on bnd_l (x=0) and T=1 on bnd_r
+  (x=1), zero flux on the four other faces. With ``hetero=False``: k=1, q=0, s=0 (8,000 vertices
+  at n=20). With ``hetero=True``: log k ~ N(0,1) i.i.d. per vertex and q ~ U[0,1] (1,000,000
+  vertices at n=100), from numpy's PCG64 generator seeded with ``field_seed``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from .mesh import Mesh
+
+# boundary ids of the cube meshes in registration order: l, r, f, k, b, t
+HEAT_BND_KIND = np.array([L.BC_TEMP, L.BC_TEMP, L.BC_FLUX, L.BC_FLUX, L.BC_FLUX, L.BC_FLUX], np.int32)
+HEAT_BND_ORDER = np.arange(6, dtype=np.int32)
+
+
+@dataclass
+class HeatProblem:
+    mesh: Mesh
+    k: np.ndarray
+    q: np.ndarray
+    s: np.ndarray
+    T0: np.ndarray        # initial guess (Dirichlet values loaded, zero elsewhere)
+    bc_val: np.ndarray    # Dirichlet value or outward flux on nodes, 0 on points
+    node_bnd: np.ndarray  # boundary id per vertex, -1 for points
+    bnd_kind: np.ndarray = field(default_factory=lambda: HEAT_BND_KIND.copy())
+    bnd_order: np.ndarray = field(default_factory=lambda: HEAT_BND_ORDER.copy())
+
+    @property
+    def n(self) -> int:
+        return self.mesh.n_tot
+
+
+def steady_heat(n: int, hetero: bool = False, mesh_seed: int = 42, field_seed: int = 7, flux_top: float = 0.0,
+                prod: float = 0.0) -> HeatProblem:
+    mesh = Mesh.jitter_cube(n, mesh_seed, 0.25)
+    N = mesh.n_tot
+    _, nb, _ = mesh.export()
+    node_bnd = np.full(N, -1, np.int32)
+    node_bnd[mesh.n_pts:] = nb
+    if hetero:
+        rng = np.random.default_rng(field_seed)
+        k = np.exp(rng.standard_normal(N))
+        q = rng.uniform(0.0, 1.0, N)
+    else:
+        k = np.ones(N)
+        q = np.zeros(N)
+    s = np.full(N, float(prod))
+    bc = np.zeros(N)
+    bc[node_bnd == 1] = 1.0          # T = 1 at x = 1
+    bc[node_bnd == 5] = flux_top     # optional outward flux on z = 1
+    T0 = np.zeros(N)
+    T0[node_bnd == 1] = 1.0           # initial_dirichlet (steady_base.rs:53-57)
+    return HeatProblem(mesh, k, q, s, T0, bc, node_bnd)
