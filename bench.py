@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--restart", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--engine", type=int, default=1, help="0 persistent cycle kernel, 1 CUDA graph of per-phase kernels")
     return ap.parse_args()
 
 
@@ -153,7 +154,7 @@ def main():
     x_d = torch.empty_like(b_d)
     x0_d = T_d.clone()
 
-    ilu = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_MULTICOLOR)
+    ilu = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_MULTICOLOR, engine=args.engine)
     # reference solution: FP64 GMRES driven to round-off
     ref_opts = GmresOptions(tol=1e-14, restart=args.restart, max_outer=4000, **ilu)
     try:

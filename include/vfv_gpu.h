@@ -46,6 +46,8 @@ extern "C" {
 #define VFV_MIXED 1          /* float inner GMRES cycles inside double iterative refinement */
 #define VFV_ILU_MULTICOLOR 0 /* ILU(0) of the greedy-multicolour permutation (few levels) */
 #define VFV_ILU_NATURAL 1    /* ILU(0) in the given order, level scheduled */
+#define VFV_ENGINE_PERSISTENT 0 /* one cooperative kernel per restart cycle, grid barriers between phases */
+#define VFV_ENGINE_GRAPH 1      /* a CUDA graph of one kernel per phase, replayed per restart cycle (default) */
 
 /* ---- boundary-condition kinds of the heat operator (SteadyHeat::add_temp_bnd / add_hflx_bnd) */
 #define VFV_BC_TEMP 0 /* Dirichlet: OpSclBndDirichlet */
@@ -67,7 +69,7 @@ typedef struct {
     int32_t precond;   /* VFV_PRECOND_* */
     int32_t precision; /* VFV_FP64 or VFV_MIXED */
     int32_t ilu_order; /* VFV_ILU_* (ILU(0) only) */
-    int32_t pad;
+    int32_t engine;    /* VFV_ENGINE_*: how a restart cycle is launched */
     double inner_rtol; /* VFV_MIXED: an inner cycle also ends once its estimate drops by this factor (0 = full cycles) */
 } vfv_gmres_opts;
 
@@ -80,7 +82,7 @@ typedef struct {
     double bnorm;     /* ||b|| */
 } vfv_solve_info;
 
-/* Fills opts with the reference defaults: tol 1e-6, restart 50, max_outer 200, Jacobi, FP64. */
+/* Fills opts with the reference defaults: tol 1e-6, restart 50, max_outer 200, Jacobi, FP64 (graph engine). */
 void vfv_gmres_default_opts(vfv_gmres_opts* opts);
 
 /* ---- context */

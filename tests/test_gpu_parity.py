@@ -127,19 +127,34 @@ def test_ilu0_apply_matches_oracle(gpu_ctx, c1h_system, c1_hetero, order):
     assert _rel(zd.cpu().numpy(), zo) <= 1e-12
 
 
-@pytest.mark.parametrize("precond", [1, 2])
+@pytest.mark.parametrize("engine", [0, 1])
+@pytest.mark.parametrize("precond", [0, 1, 2])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_gmres_matches_lu(gpu_ctx, c1h_system, c1_hetero, precond, precision):
+def test_gmres_matches_lu(gpu_ctx, c1h_system, c1_hetero, precond, precision, engine):
     from vfvchem_vfvm3d_b200 import GmresOptions, Pattern
     (rp, ci, va), b, _ = c1h_system
     p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
     p.set_values(va)
     xl = lu_solve(rp, ci, va, b)
-    opts = GmresOptions(tol=1e-12, restart=30, max_outer=400, precond=precond, precision=precision,
-                        inner_rtol=1e-6 if precision == 1 else 0.0)
+    opts = GmresOptions(tol=1e-12, restart=30, max_outer=2000, precond=precond, precision=precision,
+                        inner_rtol=1e-6 if precision == 1 else 0.0, engine=engine)
     x, info = p.solve(b, c1_hetero.T0, opts)
     assert info.status == 0 and info.relres <= 1e-12
     assert _rel(x, xl) <= SOL_RTOL
+
+
+def test_engines_agree(gpu_ctx, c1h_system, c1_hetero):
+    """The persistent cycle kernel and the graph of per-phase kernels run the same arithmetic."""
+    from vfvchem_vfvm3d_b200 import GmresOptions, Pattern
+    (rp, ci, va), b, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    res = []
+    for engine in (0, 1):
+        x, info = p.solve(b, c1_hetero.T0, GmresOptions(tol=1e-11, restart=20, max_outer=500, precond=2, engine=engine))
+        res.append((x, info))
+    assert res[0][1].iters == res[1][1].iters
+    assert _rel(res[0][0], res[1][0]) <= 1e-12
 
 
 def test_config1_gmres30_jacobi(gpu_ctx, c1, c1_system):

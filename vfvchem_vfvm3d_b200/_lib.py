@@ -17,6 +17,7 @@ VFV_OK, VFV_NOT_CONVERGED, VFV_NONFINITE, VFV_BAD_INPUT, VFV_CUDA_ERROR, VFV_TIM
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
 FP64, MIXED = 0, 1
 ILU_MULTICOLOR, ILU_NATURAL = 0, 1
+ENGINE_PERSISTENT, ENGINE_GRAPH = 0, 1
 BC_TEMP, BC_FLUX = 0, 1
 
 
@@ -28,7 +29,7 @@ class GmresOpts(C.Structure):
         ("precond", C.c_int32),
         ("precision", C.c_int32),
         ("ilu_order", C.c_int32),
-        ("pad", C.c_int32),
+        ("engine", C.c_int32),
         ("inner_rtol", C.c_double),
     ]
 

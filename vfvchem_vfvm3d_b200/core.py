@@ -29,12 +29,14 @@ class GmresOptions:
     precision: int = L.FP64
     ilu_order: int = L.ILU_MULTICOLOR
     inner_rtol: float = 0.0
+    engine: int = L.ENGINE_GRAPH
 
     def to_c(self) -> L.GmresOpts:
         o = L.GmresOpts()
         o.tol, o.restart, o.max_outer = float(self.tol), int(self.restart), int(self.max_outer)
         o.precond, o.precision, o.ilu_order = int(self.precond), int(self.precision), int(self.ilu_order)
         o.inner_rtol = float(self.inner_rtol)
+        o.engine = int(self.engine)
         return o
 
 

@@ -10,10 +10,13 @@
 #include "host/mesh.hpp"
 #include "kernels/assemble.cuh"
 #include "kernels/ilu0.cuh"
+#include "kernels/gmres_cycle.cuh"
 #include "kernels/krylov.cuh"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -107,10 +110,12 @@ struct IluStruct {
     int order = -1;
     int nlev = 0;
     std::vector<int32_t> lev_ptr;  // [nlev+1] row ranges in the permuted numbering
+    DBuf<int32_t> d_lev_ptr;       // same, on the device (read by the cycle kernel)
     DBuf<int32_t> perm, rp, ci, dg, src;
     DBuf<double> lu64;
     DBuf<float> lu32;
     DBuf<int> bad;
+
     uint64_t version64 = ~0ull, version32 = ~0ull;
 };
 
@@ -129,7 +134,7 @@ struct vfv_pattern {
     DBuf<int64_t> slot_ptr, slot_trip;
     DBuf<double> trip_vals;
     std::map<int, std::unique_ptr<IluStruct>> ilu;
-    std::map<std::tuple<int, int, int, int>, std::unique_ptr<SolverBase>> solvers;
+    std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<SolverBase>> solvers;
     DBuf<double> tmp_b, tmp_x;  // staging for host-pointer solves
 };
 
@@ -201,12 +206,14 @@ int build_ilu_struct(vfv_ctx* ctx, vfv_pattern* p, int order, IluStruct& S) {
     }
     cudaStream_t s = ctx->stream;
     CK(S.perm.upload(perm.data(), n, s));
+    CK(S.d_lev_ptr.upload(S.lev_ptr.data(), S.lev_ptr.size(), s));
     CK(S.rp.upload(nrp.data(), n + 1, s));
     CK(S.ci.upload(nci.data(), p->nnz, s));
     CK(S.dg.upload(ndg.data(), n, s));
     CK(S.src.upload(nsrc.data(), p->nnz, s));
     CK(S.lu64.alloc(p->nnz));
     CK(S.bad.alloc(1));
+
     S.order = order;
     S.nlev = nlev;
     return VFV_OK;
@@ -239,25 +246,38 @@ int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
     return VFV_OK;
 }
 
+// z = (LU)^-1 r: one launch per level, lower levels then upper levels in reverse, chained with
+// programmatic dependent launch. `in` and `out` may alias; `t` must not alias either.
+template <typename T, bool LOWER>
+cudaError_t launch_level(cudaStream_t s, const IluStruct& S, int l, bool pdl, const T* lu, const T* in, T* t, T* out, const DevStatus* st) {
+    const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)std::max(1, (r1 - r0 + kLevBlock - 1) / kLevBlock));
+    cfg.blockDim = dim3(kLevBlock);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k_ilu0_level<T, LOWER>, r0, r1, (const int32_t*)S.rp.p, (const int32_t*)S.ci.p, (const int32_t*)S.dg.p, lu,
+                              (const int32_t*)S.perm.p, in, t, out, st);
+}
+
 template <typename T>
 void ilu_apply(cudaStream_t s, const IluStruct& S, const T* lu, const T* in, T* t, T* out, const DevStatus* st) {
-    constexpr int G = 8;
-    for (int l = 0; l < S.nlev; ++l) {
-        const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
-        k_ilu0_lower<T, G><<<grid_for((int64_t)(r1 - r0) * G), 256, 0, s>>>(r0, r1, S.rp.p, S.ci.p, S.dg.p, lu, S.perm.p, in, t, st);
-    }
-    for (int l = S.nlev - 1; l >= 0; --l) {
-        const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
-        k_ilu0_upper<T, G><<<grid_for((int64_t)(r1 - r0) * G), 256, 0, s>>>(r0, r1, S.rp.p, S.ci.p, S.dg.p, lu, S.perm.p, t, out, st);
-    }
+    for (int l = 0; l < S.nlev; ++l) launch_level<T, true>(s, S, l, l > 0, lu, in, t, out, st);
+    for (int l = S.nlev - 1; l >= 0; --l) launch_level<T, false>(s, S, l, true, lu, in, t, out, st);
 }
 
 template <typename T>
 struct Gmres : SolverBase {
     int64_t n = 0, ldv = 0;
-    int m = 0, precond = 0, ilu_order = 0;
-    int nblk = 0;
-    DBuf<T> V, z, z2, valK;
+    int m = 0, precond = 0, ilu_order = 0, engine = 0;
+    int nblk = 0, mega_grid = 0, mega_chunk = 0;
+    DBuf<T> V, z, z2, zc, valK;
+    DBuf<unsigned> bar;
+    DBuf<unsigned long long> trace;  // per-phase timestamps of the last cycle (VFV_TRACE_CYCLE=1)
     DBuf<double> part, hacc, coef, H, cs, sn, g, beta, inv_beta, y, dinv, scal, x, b;
     DBuf<unsigned> counter;
     DBuf<DevStatus> st;
@@ -269,21 +289,39 @@ struct Gmres : SolverBase {
         if (exec) cudaGraphExecDestroy(exec);
     }
 
-    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_) {
+    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_) {
         n = p->n;
         m = m_;
         precond = precond_;
         ilu_order = ilu_order_;
+        engine = engine_;
         ldv = (n + 63) / 64 * 64;
         nblk = (int)((n + kBlk * kRows - 1) / (kBlk * kRows));
-        const int64_t res_blocks = (n * 8 + kBlk - 1) / kBlk;
+        const int64_t res_blocks = (n * kSpG + kBlk - 1) / kBlk;
         CK(V.alloc((size_t)(m + 1) * ldv));
         CK(cudaMemset(V.p, 0, sizeof(T) * (size_t)(m + 1) * ldv));
         if (precond == VFV_PRECOND_ILU0) {
             CK(z.alloc(n));
             CK(z2.alloc(n));
+            CK(zc.alloc(n));
         }
-        CK(part.alloc(std::max<int64_t>((int64_t)kMaxBasis * nblk, res_blocks) + 16));
+        if (engine == VFV_ENGINE_PERSISTENT) {
+            int per_sm = 0, sms = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gmres_cycle<T>, kMegaThreads, 0));
+            CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+            if (per_sm < 1) return set_err(ctx, VFV_CUDA_ERROR, "cycle kernel cannot be resident");
+            mega_grid = (int)std::min<int64_t>((int64_t)per_sm * sms, std::max<int64_t>(1, (n + 255) / 256));
+            mega_chunk = (int)((n + mega_grid - 1) / mega_grid);
+            CK(bar.alloc(2 * kGenOffset));
+            CK(cudaMemset(bar.p, 0, 2 * kGenOffset * sizeof(unsigned)));
+            if (const char* e = getenv("VFV_TRACE_CYCLE")) {
+                if (e[0] == '1') {
+                    CK(trace.alloc((size_t)(m + 2) * 8));
+                    CK(cudaMemset(trace.p, 0, (size_t)(m + 2) * 8 * sizeof(unsigned long long)));
+                }
+            }
+        }
+        CK(part.alloc(std::max<int64_t>((int64_t)kMaxBasis * std::max(nblk, mega_grid), res_blocks) + 16));
         CK(hacc.alloc(kMaxBasis));
         CK(coef.alloc(kMaxBasis));
         CK(H.alloc((size_t)m * (m + 1)));
@@ -342,9 +380,78 @@ struct Gmres : SolverBase {
         else return ilu->lu32.p;
     }
 
+    // phase timestamps of the last cycle, averaged over its steps (diagnostics, VFV_TRACE_CYCLE=1)
+    void dump_trace(vfv_ctx* ctx, int cycles) {
+        std::vector<unsigned long long> h((size_t)(m + 2) * 8);
+        if (cudaMemcpy(h.data(), trace.p, h.size() * sizeof(h[0]), cudaMemcpyDeviceToHost) != cudaSuccess) return;
+        double ph[5] = {0, 0, 0, 0, 0};
+        int steps = 0;
+        for (int j = 0; j + 1 < m && h[(j + 1) * 8] != 0; ++j) {
+            const unsigned long long* t = &h[j * 8];
+            const unsigned long long nxt = h[(j + 1) * 8];
+            ph[0] += t[1] - t[0];
+            ph[1] += t[2] - t[1];
+            ph[2] += t[3] - t[2];
+            ph[3] += t[4] - t[3];
+            ph[4] += nxt - t[4];
+            ++steps;
+        }
+        if (steps == 0) return;
+        fprintf(stderr, "[vfv trace] cycles=%d steps/cycle=%d  per step (us): ilu %.1f spmv %.1f pass1 %.1f pass2 %.1f pass3 %.1f ; "
+                        "tail: lsq+update %.1f residual %.1f\n",
+                cycles, steps, ph[0] / steps / 1e3, ph[1] / steps / 1e3, ph[2] / steps / 1e3, ph[3] / steps / 1e3, ph[4] / steps / 1e3,
+                (h[(m + 0) * 8 + 1] - h[(m + 0) * 8 + 0]) / 1e3, (h[(m + 0) * 8 + 2] - h[(m + 0) * 8 + 1]) / 1e3);
+        (void)ctx;
+    }
+
+    CycleArgs cycle_args(vfv_pattern* p) const {
+        CycleArgs A{};
+        A.n = n;
+        A.ldv = ldv;
+        A.m = m;
+        A.chunk = mega_chunk;
+        A.precond = precond;
+        A.rp = p->rp.p;
+        A.ci = p->ci.p;
+        A.valK = krylov_vals(p);
+        A.val64 = p->val.p;
+        A.b = b.p;
+        A.x = x.p;
+        A.dinv = dinv.p;
+        if (ilu) {
+            A.nlev = ilu->nlev;
+            A.lev_ptr = ilu->d_lev_ptr.p;
+            A.lrp = ilu->rp.p;
+            A.lci = ilu->ci.p;
+            A.ldg = ilu->dg.p;
+            A.lu = lu_vals();
+            A.perm = ilu->perm.p;
+        }
+        A.V = V.p;
+        A.z = z.p;
+        A.t = z2.p;
+        A.zc = zc.p;
+        A.H = H.p;
+        A.cs = cs.p;
+        A.sn = sn.p;
+        A.g = g.p;
+        A.beta = beta.p;
+        A.inv_beta = inv_beta.p;
+        A.y = y.p;
+        A.hacc = hacc.p;
+        A.coef = coef.p;
+        A.part = part.p;
+        A.bar = bar.p;
+        A.trace = trace.p;
+        A.st = st.p;
+        A.scal = scal.p;
+        A.spin_limit = 20000000LL;
+        return A;
+    }
+
     // one restart cycle: m Arnoldi steps, least squares, update of x, new residual
     void enqueue_cycle(cudaStream_t s, vfv_pattern* p) {
-        constexpr int G = 8;
+        constexpr int G = kSpG;
         const T* vk = krylov_vals(p);
         const int sp_blocks = grid_for(n * G);
         for (int j = 0; j < m; ++j) {
@@ -377,7 +484,7 @@ struct Gmres : SolverBase {
     int solve(vfv_ctx* ctx, vfv_pattern* p, const double* d_b, const double* d_x0, double* d_x, const vfv_gmres_opts& o,
               vfv_solve_info* info) {
         cudaStream_t s = ctx->stream;
-        constexpr int G = 8;
+        constexpr int G = kSpG;
         const bool mixed = !std::is_same<T, double>::value;
         CK(cudaMemcpyAsync(b.p, d_b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaMemcpyAsync(x.p, d_x0, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -422,7 +529,7 @@ struct Gmres : SolverBase {
         CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
         k_residual<T, G><<<grid_for(n * G), kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
         ctx->launches += 1;
-        if (!exec) {
+        if (engine == VFV_ENGINE_GRAPH && !exec) {
             cudaGraph_t graph;
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             enqueue_cycle(s, p);
@@ -440,6 +547,12 @@ struct Gmres : SolverBase {
             CK(cudaMemcpyAsync(ctx->h_status, st.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
             hst = *ctx->h_status;
+            if (hst.timeout) {
+                rc = VFV_TIMEOUT;
+                CK(cudaMemsetAsync(bar.p, 0, 2 * kGenOffset * sizeof(unsigned), s));  // barrier state is undefined after a timeout
+                CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
+                break;
+            }
             if (hst.nonfinite) {
                 rc = VFV_NONFINITE;
                 break;
@@ -449,11 +562,20 @@ struct Gmres : SolverBase {
                 rc = VFV_NOT_CONVERGED;
                 break;
             }
-            CK(cudaGraphLaunch(exec, s));
-            ctx->launches += graph_nodes;
+            if (engine == VFV_ENGINE_GRAPH) {
+                CK(cudaGraphLaunch(exec, s));
+                ctx->launches += graph_nodes;
+            } else {
+                CycleArgs A = cycle_args(p);
+                void* args[] = {&A};
+                CK(cudaLaunchCooperativeKernel((const void*)k_gmres_cycle<T>, dim3(mega_grid), dim3(kMegaThreads), args, 0, s));
+                ctx->launches += 1;
+            }
             ++cycles;
         }
         CK(cudaGetLastError());
+        if (trace.p) dump_trace(ctx, cycles);
+
         CK(cudaMemcpyAsync(d_x, x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaStreamSynchronize(s));
         if (info) {
@@ -466,6 +588,7 @@ struct Gmres : SolverBase {
             return set_err(ctx, rc, "GMRES did not converge in " + std::to_string(o.max_outer) + " restart cycles (relres " +
                                         std::to_string(hst.beta0 / bnorm) + ")");
         if (rc == VFV_NONFINITE) return set_err(ctx, rc, "GMRES: non-finite residual");
+        if (rc == VFV_TIMEOUT) return set_err(ctx, rc, "GMRES cycle kernel: a grid barrier timed out");
         return VFV_OK;
     }
 };
@@ -478,22 +601,23 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
     if (o->precond < VFV_PRECOND_NONE || o->precond > VFV_PRECOND_ILU0) return set_err(ctx, VFV_BAD_INPUT, "unknown preconditioner");
     if (o->precision != VFV_FP64 && o->precision != VFV_MIXED) return set_err(ctx, VFV_BAD_INPUT, "unknown precision");
     if (o->ilu_order != VFV_ILU_MULTICOLOR && o->ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
+    if (o->engine != VFV_ENGINE_PERSISTENT && o->engine != VFV_ENGINE_GRAPH) return set_err(ctx, VFV_BAD_INPUT, "unknown engine");
     return VFV_OK;
 }
 
 int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info) {
-    const auto key = std::make_tuple(o->precision, o->precond, o->precond == VFV_PRECOND_ILU0 ? o->ilu_order : 0, o->restart);
+    const auto key = std::make_tuple(o->precision, o->precond, o->precond == VFV_PRECOND_ILU0 ? o->ilu_order : 0, o->restart, o->engine);
     auto it = p->solvers.find(key);
     if (it == p->solvers.end()) {
         std::unique_ptr<SolverBase> sb;
         int rc;
         if (o->precision == VFV_MIXED) {
             auto g = std::make_unique<Gmres<float>>();
-            rc = g->init(ctx, p, o->restart, o->precond, o->ilu_order);
+            rc = g->init(ctx, p, o->restart, o->precond, o->ilu_order, o->engine);
             sb = std::move(g);
         } else {
             auto g = std::make_unique<Gmres<double>>();
-            rc = g->init(ctx, p, o->restart, o->precond, o->ilu_order);
+            rc = g->init(ctx, p, o->restart, o->precond, o->ilu_order, o->engine);
             sb = std::move(g);
         }
         if (rc) return rc;
@@ -549,6 +673,7 @@ void vfv_gmres_default_opts(vfv_gmres_opts* o) {
     o->precond = VFV_PRECOND_JACOBI;
     o->precision = VFV_FP64;
     o->ilu_order = VFV_ILU_MULTICOLOR;
+    o->engine = VFV_ENGINE_GRAPH;
     o->inner_rtol = 0.0;
 }
 
@@ -737,7 +862,7 @@ int vfv_solve(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
 
 int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double* y) {
     if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    constexpr int G = 8;
+    constexpr int G = kSpG;
     k_spmv<double, double, double, double, G><<<grid_for(p->n * G), kBlk, 0, ctx->stream>>>(p->n, p->rp.p, p->ci.p, p->val.p, x, y, nullptr, nullptr);
     ctx->launches += 1;
     CK(cudaGetLastError());
@@ -746,7 +871,7 @@ int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double*
 
 int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y) {
     if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    constexpr int G = 8;
+    constexpr int G = kSpG;
     if (p->version32 != p->version) {
         if (!p->val32.p) CK(p->val32.alloc(p->nnz));
         k_cast<double, float><<<grid_for(p->nnz), 256, 0, ctx->stream>>>(p->nnz, p->val.p, p->val32.p);
@@ -774,6 +899,7 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
     DBuf<double> t;
     CK(t.alloc(p->n));
     ilu_apply<double>(ctx->stream, S, S.lu64.p, r, t.p, z, nullptr);
+    ctx->launches += 2 * S.nlev;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
     if (levels) *levels = S.nlev;

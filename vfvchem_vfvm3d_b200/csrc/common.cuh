@@ -40,7 +40,7 @@ struct DevStatus {
     int32_t nonfinite;   // a NaN/Inf was seen in a reduction
     int32_t converged;   // the last true residual met the tolerance
     int32_t total_steps; // Arnoldi steps over the whole solve
-    int32_t pad;
+    int32_t timeout;     // a bounded grid barrier gave up (the kernel left early)
     double resid_est;    // |g_{j+1}|, the residual-norm estimate after the last step
     double beta0;        // ||r_0|| of the current cycle
 };

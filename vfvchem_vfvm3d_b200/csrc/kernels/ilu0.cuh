@@ -61,45 +61,60 @@ __global__ void k_cast(int64_t n, const TS* __restrict__ in, TD* __restrict__ ou
     if (k < n) out[k] = (TD)in[k];
 }
 
-// Lower solve for one level: t[i] = rhs[perm[i]] - sum_{k<i} l_ik t[k]   (G lanes per row)
-template <typename T, int G>
-__global__ void __launch_bounds__(256) k_ilu0_lower(int32_t r0, int32_t r1, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                   const int32_t* __restrict__ dg, const T* __restrict__ lu, const int32_t* __restrict__ perm,
-                                                   const T* __restrict__ rhs, T* __restrict__ t, const DevStatus* __restrict__ st) {
-    if (st && st->done) return;
-    const int lane = threadIdx.x & (G - 1);
-    const int32_t i = r0 + (int32_t)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G);
-    T s = T(0);
-    if (i < r1) {
-        const int32_t e = dg[i];
-        for (int32_t k = rp[i] + lane; k < e; k += G) s += lu[k] * t[ci[k]];
-    }
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
-    if (lane == 0 && i < r1) t[i] = rhs[perm[i]] - s;
-}
+// ---------------------------------------------------------------- level sweeps
+// One launch per level, a thread per row. Each level is latency-bound (row range -> indices and
+// values -> gather of already solved rows -> store), so the launches are chained with programmatic
+// dependent launch: a level kernel first loads everything that does not depend on earlier levels
+// (its rows' column indices, factor values, right-hand side), then lets the next level's kernel
+// launch (griddepcontrol.launch_dependents) and only then waits for the previous level to finish
+// (griddepcontrol.wait) before gathering solved values. The next level's prologue therefore
+// overlaps this level's gathers instead of following them.
+constexpr int kLevBlock = 128;
+constexpr int kLevK = 16;  // entries of a row held in registers before the wait
 
-// Upper solve for one level: t[i] = (t[i] - sum_{j>i} u_ij t[j]) / u_ii ; out[perm[i]] = t[i]
-template <typename T, int G>
-__global__ void __launch_bounds__(256) k_ilu0_upper(int32_t r0, int32_t r1, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                   const int32_t* __restrict__ dg, const T* __restrict__ lu, const int32_t* __restrict__ perm,
-                                                   T* __restrict__ t, T* __restrict__ out, const DevStatus* __restrict__ st) {
-    if (st && st->done) return;
-    const int lane = threadIdx.x & (G - 1);
-    const int32_t i = r0 + (int32_t)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G);
-    T s = T(0);
-    int32_t d = 0;
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// LOWER: t[i] = in[perm[i]] - sum_{k < diag} lu[k] t[ci[k]]
+// UPPER: t[i] = (t[i] - sum_{k > diag} lu[k] t[ci[k]]) / lu[diag] ; out[perm[i]] = t[i]
+template <typename T, bool LOWER>
+__global__ void __launch_bounds__(kLevBlock) k_ilu0_level(int32_t r0, int32_t r1, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                         const int32_t* __restrict__ dg, const T* __restrict__ lu,
+                                                         const int32_t* __restrict__ perm, const T* __restrict__ in, T* t, T* out,
+                                                         const DevStatus* __restrict__ st) {
+    const int32_t i = r0 + (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    int32_t kb = 0, ke = 0, d = 0, pi = 0;
+    int32_t c[kLevK];
+    T v[kLevK];
+    T rhs = T(0), diag = T(1);
     if (i < r1) {
-        d = dg[i];
-        const int32_t e = rp[i + 1];
-        for (int32_t k = d + 1 + lane; k < e; k += G) s += lu[k] * t[ci[k]];
-    }
+        d = __ldg(dg + i);
+        kb = LOWER ? __ldg(rp + i) : d + 1;
+        ke = LOWER ? d : __ldg(rp + i + 1);
+        pi = __ldg(perm + i);
+        if (!LOWER) diag = __ldg(lu + d);
 #pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
-    if (lane == 0 && i < r1) {
-        const T v = (t[i] - s) / lu[d];
-        t[i] = v;
-        out[perm[i]] = v;
+        for (int q = 0; q < kLevK; ++q) {
+            c[q] = kb + q < ke ? __ldg(ci + kb + q) : -1;
+            v[q] = kb + q < ke ? __ldg(lu + kb + q) : T(0);
+        }
+    }
+    pdl_launch_dependents();
+    pdl_wait();
+    if (i >= r1 || (st && st->done)) return;
+    if (LOWER) rhs = in[pi];
+    else rhs = t[i];
+    T s = T(0);
+#pragma unroll
+    for (int q = 0; q < kLevK; ++q)
+        if (c[q] >= 0) s += v[q] * t[c[q]];
+    for (int32_t k = kb + kLevK; k < ke; ++k) s += __ldg(lu + k) * t[__ldg(ci + k)];
+    if (LOWER) {
+        t[i] = rhs - s;
+    } else {
+        const T x = (rhs - s) / diag;
+        t[i] = x;
+        out[pi] = x;
     }
 }
 

@@ -68,6 +68,35 @@ __device__ __forceinline__ double reduce_partials(const double* part, int nblk, 
 }
 
 // ---------------------------------------------------------------- SpMV (CSR, G lanes per row)
+constexpr int kSpG = 4;  // lanes per row: rows hold ~16 non-zeros, 4 lanes x 4 loads in flight each
+
+// This lane's share of row `row` of A x: loads of up to three strides are issued before the
+// multiply-adds so that every lane has several independent loads in flight.
+template <typename TV, typename TX, typename TA, int G>
+__device__ __forceinline__ TA row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const TV* __restrict__ val,
+                                      const TX* __restrict__ x, int64_t row, int lane) {
+    TA s = TA(0);
+    const int32_t b = __ldg(rp + row), e = __ldg(rp + row + 1);
+    int32_t k = b + lane;
+    for (; k + 2 * G < e; k += 3 * G) {
+        const int32_t c0 = __ldcs(ci + k), c1 = __ldcs(ci + k + G), c2 = __ldcs(ci + k + 2 * G);
+        const TV v0 = __ldcs(val + k), v1 = __ldcs(val + k + G), v2 = __ldcs(val + k + 2 * G);
+        s += (TA)v0 * (TA)__ldg(x + c0) + (TA)v1 * (TA)__ldg(x + c1) + (TA)v2 * (TA)__ldg(x + c2);
+    }
+    int32_t c[3];
+    TV v[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int32_t kk = k + q * G;
+        c[q] = kk < e ? __ldcs(ci + kk) : -1;
+        v[q] = kk < e ? __ldcs(val + kk) : TV(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        if (c[q] >= 0) s += (TA)v[q] * (TA)__ldg(x + c[q]);
+    return s;
+}
+
 // y = scale * (A x). Accumulation in TA. `scale` may be null (= 1).
 template <typename TV, typename TX, typename TY, typename TA, int G>
 __global__ void __launch_bounds__(kBlk) k_spmv(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
@@ -77,10 +106,7 @@ __global__ void __launch_bounds__(kBlk) k_spmv(int64_t n, const int32_t* __restr
     const int lane = threadIdx.x & (G - 1);
     const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     TA s = TA(0);
-    if (row < n) {
-        const int32_t b = __ldg(rp + row), e = __ldg(rp + row + 1);
-        for (int32_t k = b + lane; k < e; k += G) s += (TA)__ldcs(val + k) * (TA)__ldg(x + __ldcs(ci + k));
-    }
+    if (row < n) s = row_dot<TV, TX, TA, G>(rp, ci, val, x, row, lane);
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
     if (lane == 0 && row < n) {
@@ -100,10 +126,7 @@ __global__ void __launch_bounds__(kBlk) k_residual(KrylovDev K, const int32_t* _
     const int lane = threadIdx.x & (G - 1);
     const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     double s = 0.0;
-    if (row < K.n) {
-        const int32_t b0 = __ldg(rp + row), e = __ldg(rp + row + 1);
-        for (int32_t k = b0 + lane; k < e; k += G) s += __ldcs(val + k) * __ldg(x + __ldcs(ci + k));
-    }
+    if (row < K.n) s = row_dot<double, double, double, G>(rp, ci, val, x, row, lane);
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
     double r2 = 0.0;
