@@ -126,6 +126,9 @@ int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double*
 int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y);
 /* z = M^-1 r for the ILU(0) preconditioner of the pattern's current values (device arrays, double) */
 int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels);
+/* the symmetric permutation the ILU(0) factor lives on: perm[n] (new -> old) and the row ranges of
+ * its levels lev_ptr[nlev+1] (any pointer may be NULL; call once with NULLs to learn nlev) */
+int vfv_ilu0_ordering(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int32_t* perm, int32_t* lev_ptr, int32_t* nlev);
 
 /* ---- mesh (host, once per mesh): jittered unit cube, Delaunay, Voronoi dual */
 int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out);

@@ -109,8 +109,22 @@ def test_spmv_matches_oracle(gpu_ctx, c1h_system, c1_hetero):
     assert np.max(np.abs(yf.cpu().numpy() - yo)) <= 1e-5 * np.max(np.abs(yo))
 
 
+def _check_ordering(rp, ci, perm, lev_ptr):
+    """The permutation groups rows into levels no two coupled rows share, and every coupling
+    points from a later level to an earlier one in the lower factor (true of any ordering)."""
+    n = rp.size - 1
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    level = np.empty(n, np.int64)
+    for l in range(lev_ptr.size - 1):
+        level[perm[lev_ptr[l]:lev_ptr[l + 1]]] = l
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    off = rows != ci
+    assert np.all(level[rows[off]] != level[ci[off]])
+
+
 @pytest.mark.parametrize("order", [0, 1])
 def test_ilu0_apply_matches_oracle(gpu_ctx, c1h_system, c1_hetero, order):
+    """ILU(0) on the product's ordering, restated by the oracle on the same permutation."""
     import torch
     from vfvchem_vfvm3d_b200 import Pattern
     (rp, ci, va), _, _ = c1h_system
@@ -121,8 +135,15 @@ def test_ilu0_apply_matches_oracle(gpu_ctx, c1h_system, c1_hetero, order):
     zd = torch.empty_like(rd)
     torch.cuda.synchronize()
     nlev = p.ilu0_apply_device(rd.data_ptr(), zd.data_ptr(), order)
-    perm, lev = (ordering.multicolor if order == 0 else ordering.natural)(rp, ci)
-    assert nlev == int(lev.max()) + 1
+    perm, lev_ptr = p.ilu0_ordering(order)
+    assert lev_ptr.size == nlev + 1
+    _check_ordering(rp, ci, perm, lev_ptr)
+    if order == 1:  # the natural ordering is fully determined: level = longest lower chain
+        perm_o, lev_o = ordering.natural(rp, ci)
+        assert np.array_equal(perm, perm_o) and nlev == int(lev_o.max()) + 1
+    else:  # at most as many colours as plain greedy colouring
+        _, col = ordering.multicolor(rp, ci)
+        assert nlev <= int(col.max()) + 1
     zo = oracle.Ilu0(rp, ci, va, perm).apply(r)
     assert _rel(zd.cpu().numpy(), zo) <= 1e-12
 
@@ -212,7 +233,7 @@ def test_larger_mesh_properties(gpu_ctx):
     prob = steady_heat(40)
     h = SteadyHeatGpu(prob.mesh, prob.bnd_kind, ctx=gpu_ctx)
     b = h.assemble(prob.k, prob.q, prob.s, prob.T0, prob.bc_val)
-    x, info = h.pattern.solve(b, prob.T0, GmresOptions(tol=1e-11, restart=50, max_outer=400, precond=2))
+    x, info = h.pattern.solve(b, prob.T0, GmresOptions(tol=1e-12, restart=50, max_outer=400, precond=2))
     pos, _, _ = prob.mesh.export()
     assert np.max(np.abs(x - pos[:, 0])) < 1e-8
     rp, ci, va = h.pattern.export()

@@ -193,6 +193,16 @@ class Pattern:
                                                                C.c_void_p(z_ptr), C.byref(lev)))
         return lev.value
 
+    def ilu0_ordering(self, order: int = L.ILU_MULTICOLOR):
+        """(perm new->old, lev_ptr) of the ILU(0) factor's symmetric permutation (host only)."""
+        nlev = C.c_int32()
+        _check(self.ctx.handle, L.load().vfv_ilu0_ordering(self.ctx.handle, self._h, int(order), None, None, C.byref(nlev)))
+        perm = np.empty(self.n, np.int32)
+        lev = np.empty(nlev.value + 1, np.int32)
+        _check(self.ctx.handle, L.load().vfv_ilu0_ordering(self.ctx.handle, self._h, int(order), L.ptr(perm, C.c_int32),
+                                                          L.ptr(lev, C.c_int32), C.byref(nlev)))
+        return perm, lev
+
     def close(self) -> None:
         if self._owned and getattr(self, "_h", None):
             L.load().vfv_pattern_destroy(self._h)

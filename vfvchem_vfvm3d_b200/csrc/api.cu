@@ -110,11 +110,13 @@ struct IluStruct {
     int order = -1;
     int nlev = 0;
     std::vector<int32_t> lev_ptr;  // [nlev+1] row ranges in the permuted numbering
+    std::vector<int32_t> h_perm;   // new -> old
     DBuf<int32_t> d_lev_ptr;       // same, on the device (read by the cycle kernel)
     DBuf<int32_t> perm, rp, ci, dg, src;
     DBuf<double> lu64;
     DBuf<float> lu32;
     DBuf<int> bad;
+
 
     uint64_t version64 = ~0ull, version32 = ~0ull;
 };
@@ -141,6 +143,97 @@ struct vfv_pattern {
 // ================================================================ GMRES driver
 namespace {
 
+// Greedy colouring of the symmetrised pattern graph: colour(v) = smallest colour unused by the
+// already coloured neighbours, visiting vertices in `order`.
+int greedy_colour(int64_t n, const std::vector<std::vector<int32_t>>& adj, const std::vector<int32_t>& order, std::vector<int32_t>& col) {
+    std::fill(col.begin(), col.end(), -1);
+    std::vector<int64_t> mark(64, -1);
+    int nc = 0;
+    for (int64_t t = 0; t < n; ++t) {
+        const int32_t v = order[t];
+        for (int32_t u : adj[v])
+            if (col[u] >= 0) {
+                if (col[u] >= (int32_t)mark.size()) mark.resize(col[u] + 1, -1);
+                mark[col[u]] = t;
+            }
+        int32_t c = 0;
+        while (c < (int32_t)mark.size() && mark[c] == t) ++c;
+        col[v] = c;
+        nc = std::max(nc, c + 1);
+    }
+    return nc;
+}
+
+// Multicolour ordering with few colours (each colour is a level of both ILU sweeps): greedy in
+// index order, then iterated greedy (Culberson: re-running greedy with the vertices grouped by
+// colour class never needs more colours), then single-neighbour recolouring that tries to empty
+// the last class. Deterministic.
+int multicolor(int64_t n, const std::vector<std::vector<int32_t>>& lower, std::vector<int32_t>& col) {
+    std::vector<std::vector<int32_t>> adj(n);
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t j : lower[i]) {
+            adj[i].push_back(j);
+            adj[j].push_back((int32_t)i);
+        }
+    std::vector<int32_t> order(n);
+    for (int64_t i = 0; i < n; ++i) order[i] = (int32_t)i;
+    int nc = greedy_colour(n, adj, order, col);
+    std::vector<int32_t> c2(n);
+    for (int it = 0; it < 8; ++it) {
+        std::vector<int64_t> cnt(nc, 0);
+        for (int32_t c : col) cnt[c]++;
+        if (it % 2 == 0)
+            std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return col[a] > col[b]; });
+        else
+            std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+                return cnt[col[a]] != cnt[col[b]] ? cnt[col[a]] > cnt[col[b]] : col[a] < col[b];
+            });
+        const int nc2 = greedy_colour(n, adj, order, c2);
+        if (nc2 <= nc) {
+            nc = nc2;
+            col.swap(c2);
+        }
+    }
+    for (int round = 0; round < 2 && nc > 1; ++round) {
+        const int last = nc - 1;
+        int64_t left = 0;
+        for (int64_t v = 0; v < n; ++v) {
+            if (col[v] != last) continue;
+            bool done = false;
+            for (int c = 0; c < last && !done; ++c) {
+                int cntc = 0;
+                int32_t u = -1;
+                for (int32_t w : adj[v])
+                    if (col[w] == c) {
+                        ++cntc;
+                        u = w;
+                    }
+                if (cntc == 0) {
+                    col[v] = c;
+                    done = true;
+                } else if (cntc == 1) {
+                    std::vector<char> used(last, 0);
+                    for (int32_t w : adj[u])
+                        if (w != v && col[w] < last) used[col[w]] = 1;
+                    for (int cc = 0; cc < last; ++cc)
+                        if (cc != c && !used[cc]) {
+                            col[u] = cc;
+                            col[v] = c;
+                            done = true;
+                            break;
+                        }
+                }
+            }
+            if (!done) ++left;
+        }
+        if (left == 0) {
+            nc = last;
+            break;
+        }
+    }
+    return nc;
+}
+
 int build_ilu_struct(vfv_ctx* ctx, vfv_pattern* p, int order, IluStruct& S) {
     const int64_t n = p->n;
     const std::vector<int32_t>& rp = p->h_rp;
@@ -163,17 +256,7 @@ int build_ilu_struct(vfv_ctx* ctx, vfv_pattern* p, int order, IluStruct& S) {
             nlev = std::max(nlev, l + 1);
         }
     } else {
-        std::vector<int64_t> mark(256, -1);
-        for (int64_t i = 0; i < n; ++i) {
-            for (int32_t k : lower[i]) {
-                if (lev[k] >= (int32_t)mark.size()) mark.resize(lev[k] + 1, -1);
-                mark[lev[k]] = i;
-            }
-            int32_t c = 0;
-            while (c < (int32_t)mark.size() && mark[c] == i) ++c;
-            lev[i] = c;
-            nlev = std::max(nlev, c + 1);
-        }
+        nlev = multicolor(n, lower, lev);
     }
     std::vector<std::vector<int32_t>>().swap(lower);
     std::vector<int32_t> perm(n), iperm(n);
@@ -205,6 +288,7 @@ int build_ilu_struct(vfv_ctx* ctx, vfv_pattern* p, int order, IluStruct& S) {
         if (ndg[q] < 0) return set_err(ctx, VFV_BAD_INPUT, "ILU(0) needs a diagonal entry in every row of the pattern");
     }
     cudaStream_t s = ctx->stream;
+    S.h_perm = perm;
     CK(S.perm.upload(perm.data(), n, s));
     CK(S.d_lev_ptr.upload(S.lev_ptr.data(), S.lev_ptr.size(), s));
     CK(S.rp.upload(nrp.data(), n + 1, s));
@@ -213,6 +297,7 @@ int build_ilu_struct(vfv_ctx* ctx, vfv_pattern* p, int order, IluStruct& S) {
     CK(S.src.upload(nsrc.data(), p->nnz, s));
     CK(S.lu64.alloc(p->nnz));
     CK(S.bad.alloc(1));
+
 
     S.order = order;
     S.nlev = nlev;
@@ -404,6 +489,41 @@ struct Gmres : SolverBase {
         (void)ctx;
     }
 
+    // Diagnostics (VFV_PROFILE_STEP=1): time the kernels of one Arnoldi step (j = m/2, on the
+    // basis left by the last cycle) one group at a time with events, outside the graph.
+    void profile_step(vfv_ctx* ctx, vfv_pattern* p) {
+        cudaStream_t s = ctx->stream;
+        constexpr int G = kSpG;
+        const int j = m / 2;
+        const T* vk = krylov_vals(p);
+        const T* uj = V.p + (int64_t)j * ldv;
+        T* w = V.p + (int64_t)(j + 1) * ldv;
+        cudaEvent_t ev[6];
+        for (auto& e : ev) cudaEventCreate(&e);
+        cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s);
+        const T* in = uj;
+        cudaEventRecord(ev[0], s);
+        if (precond == VFV_PRECOND_ILU0) {
+            ilu_apply<T>(s, *ilu, lu_vals(), uj, z2.p, z.p, st.p);
+            in = z.p;
+        }
+        cudaEventRecord(ev[1], s);
+        k_spmv<T, T, T, T, G><<<grid_for(n * G), kBlk, 0, s>>>(n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
+        cudaEventRecord(ev[2], s);
+        k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
+        cudaEventRecord(ev[3], s);
+        k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+        cudaEventRecord(ev[4], s);
+        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+        cudaEventRecord(ev[5], s);
+        cudaEventSynchronize(ev[5]);
+        float t[5];
+        for (int q = 0; q < 5; ++q) cudaEventElapsedTime(&t[q], ev[q], ev[q + 1]);
+        fprintf(stderr, "[vfv step profile] %s j=%d (us): ilu %.1f spmv %.1f mdot %.1f update+dot %.1f update+norm %.1f\n",
+                sizeof(T) == 4 ? "fp32" : "fp64", j, t[0] * 1e3, t[1] * 1e3, t[2] * 1e3, t[3] * 1e3, t[4] * 1e3);
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
+
     CycleArgs cycle_args(vfv_pattern* p) const {
         CycleArgs A{};
         A.n = n;
@@ -575,6 +695,9 @@ struct Gmres : SolverBase {
         }
         CK(cudaGetLastError());
         if (trace.p) dump_trace(ctx, cycles);
+        if (const char* e = getenv("VFV_PROFILE_STEP")) {
+            if (e[0] == '1' && engine == VFV_ENGINE_GRAPH) profile_step(ctx, p);
+        }
 
         CK(cudaMemcpyAsync(d_x, x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaStreamSynchronize(s));
@@ -903,6 +1026,23 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
     if (levels) *levels = S.nlev;
+    return VFV_OK;
+}
+
+int vfv_ilu0_ordering(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int32_t* perm, int32_t* lev_ptr, int32_t* nlev) {
+    if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
+    auto it = p->ilu.find(ilu_order);
+    if (it == p->ilu.end()) {
+        auto S = std::make_unique<IluStruct>();
+        int rc = build_ilu_struct(ctx, p, ilu_order, *S);
+        if (rc) return rc;
+        it = p->ilu.emplace(ilu_order, std::move(S)).first;
+    }
+    const IluStruct& S = *it->second;
+    if (nlev) *nlev = S.nlev;
+    if (perm) std::memcpy(perm, S.h_perm.data(), S.h_perm.size() * sizeof(int32_t));
+    if (lev_ptr) std::memcpy(lev_ptr, S.lev_ptr.data(), S.lev_ptr.size() * sizeof(int32_t));
     return VFV_OK;
 }
 

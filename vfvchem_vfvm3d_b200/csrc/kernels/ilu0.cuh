@@ -70,7 +70,8 @@ __global__ void k_cast(int64_t n, const TS* __restrict__ in, TD* __restrict__ ou
 // (griddepcontrol.wait) before gathering solved values. The next level's prologue therefore
 // overlaps this level's gathers instead of following them.
 constexpr int kLevBlock = 128;
-constexpr int kLevK = 16;  // entries of a row held in registers before the wait
+constexpr int kLevMinBlocks = 12;  // <= 42 registers: a level leaves room on every SM for the next one
+constexpr int kLevK = 8;           // entries of a row held in registers before the wait
 
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
@@ -78,7 +79,7 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 // LOWER: t[i] = in[perm[i]] - sum_{k < diag} lu[k] t[ci[k]]
 // UPPER: t[i] = (t[i] - sum_{k > diag} lu[k] t[ci[k]]) / lu[diag] ; out[perm[i]] = t[i]
 template <typename T, bool LOWER>
-__global__ void __launch_bounds__(kLevBlock) k_ilu0_level(int32_t r0, int32_t r1, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+__global__ void __launch_bounds__(kLevBlock, kLevMinBlocks) k_ilu0_level(int32_t r0, int32_t r1, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                                          const int32_t* __restrict__ dg, const T* __restrict__ lu,
                                                          const int32_t* __restrict__ perm, const T* __restrict__ in, T* t, T* out,
                                                          const DevStatus* __restrict__ st) {

@@ -47,9 +47,11 @@ struct KrylovDev {
 };
 
 // ---------------------------------------------------------------- last-block helper
+// Threads that wrote partials fence their own writes before calling this (see publish_partial);
+// after the block-wide barrier thread 0 takes a ticket, and the block that takes the last ticket
+// reads every block's partials.
 __device__ __forceinline__ bool last_block_arrive(unsigned* counter) {
     __shared__ bool s_last;
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned t = atomicAdd(counter, 1u);
@@ -60,11 +62,39 @@ __device__ __forceinline__ bool last_block_arrive(unsigned* counter) {
     return s_last;
 }
 
+// store one partial and make it visible device-wide before the block arrives
+__device__ __forceinline__ void publish_partial(double* p, double v) {
+    *p = v;
+    __threadfence();
+}
+
 // Sum column c of part[c][0..nblk) with all threads of the block, in a fixed order; valid in thread 0.
 __device__ __forceinline__ double reduce_partials(const double* part, int nblk, double* red) {
     double s = 0.0;
     for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += __ldcg(part + b);
     return block_sum(s, red);
+}
+
+// Columns c < cnt of part[c][0..nblk): one warp per column, four independent accumulators per
+// lane, then a fixed shuffle tree; out(c, sum) is called by lane 0. Deterministic.
+template <typename F>
+__device__ __forceinline__ void reduce_cols_warp(const double* part, int nblk, int cnt, F out) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int c = wid; c < cnt; c += nw) {
+        const double* p = part + (int64_t)c * nblk;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int q = lane;
+        for (; q + 96 < nblk; q += 128) {
+            s0 += __ldcg(p + q);
+            s1 += __ldcg(p + q + 32);
+            s2 += __ldcg(p + q + 64);
+            s3 += __ldcg(p + q + 96);
+        }
+        for (; q < nblk; q += 32) s0 += __ldcg(p + q);
+        double s = (s0 + s1) + (s2 + s3);
+        s = warp_sum(s);
+        if (lane == 0) out(c, s);
+    }
 }
 
 // ---------------------------------------------------------------- SpMV (CSR, G lanes per row)
@@ -136,7 +166,7 @@ __global__ void __launch_bounds__(kBlk) k_residual(KrylovDev K, const int32_t* _
         r2 = r * r;
     }
     const double bs = block_sum(r2, red);
-    if (threadIdx.x == 0) K.part[blockIdx.x] = bs;
+    if (threadIdx.x == 0) publish_partial(K.part + blockIdx.x, bs);
     if (!last_block_arrive(K.counter)) return;
     const double tot = reduce_partials(K.part, gridDim.x, red);
     if (threadIdx.x == 0) {
@@ -187,16 +217,14 @@ __global__ void __launch_bounds__(kBlk) k_mdot(KrylovDev K, const T* __restrict_
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
         double s = 0.0;
         for (int q = 0; q < nw; ++q) s += red[i][q];
-        K.part[(int64_t)i * K.nblk + blockIdx.x] = s;
+        publish_partial(K.part + (int64_t)i * K.nblk + blockIdx.x, s);
     }
     if (!last_block_arrive(K.counter + 1)) return;
-    for (int i = 0; i < nvec; ++i) {
-        const double d = reduce_partials(K.part + (int64_t)i * K.nblk, gridDim.x, red2);
-        if (threadIdx.x == 0) {
-            K.hacc[i] = d * K.inv_beta[i];
-            K.coef[i] = d * K.inv_beta[i] * K.inv_beta[i];
-        }
-    }
+    reduce_cols_warp(K.part, K.nblk, nvec, [&](int i, double d) {
+        const double ib = K.inv_beta[i];
+        K.hacc[i] = d * ib;
+        K.coef[i] = d * ib * ib;
+    });
     if (threadIdx.x == 0) K.counter[1] = 0u;
 }
 
@@ -254,23 +282,21 @@ __global__ void __launch_bounds__(kBlk) k_update(KrylovDev K, const T* __restric
         for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
             double s = 0.0;
             for (int q = 0; q < nw; ++q) s += red[i][q];
-            K.part[(int64_t)i * K.nblk + blockIdx.x] = s;
+            publish_partial(K.part + (int64_t)i * K.nblk + blockIdx.x, s);
         }
         if (!last_block_arrive(K.counter + 2)) return;
-        for (int i = 0; i < nvec; ++i) {
-            const double d = reduce_partials(K.part + (int64_t)i * K.nblk, gridDim.x, red2);
-            if (threadIdx.x == 0) {
-                K.hacc[i] += d * K.inv_beta[i];
-                K.coef[i] = d * K.inv_beta[i] * K.inv_beta[i];
-            }
-        }
+        reduce_cols_warp(K.part, K.nblk, nvec, [&](int i, double d) {
+            const double ib = K.inv_beta[i];
+            K.hacc[i] += d * ib;
+            K.coef[i] = d * ib * ib;
+        });
         if (threadIdx.x == 0) K.counter[2] = 0u;
     } else {
         double s = 0.0;
 #pragma unroll
         for (int r = 0; r < kRows; ++r) s += wr[r] * wr[r];
         s = block_sum(s, red2);
-        if (threadIdx.x == 0) K.part[blockIdx.x] = s;
+        if (threadIdx.x == 0) publish_partial(K.part + blockIdx.x, s);
         if (!last_block_arrive(K.counter + 3)) return;
         const double tot = reduce_partials(K.part, gridDim.x, red2);
         if (threadIdx.x == 0) {
@@ -359,7 +385,7 @@ __global__ void __launch_bounds__(kBlk) k_norm2(int64_t n, const double* __restr
     double s = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += v[i] * v[i];
     s = block_sum(s, red);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (threadIdx.x == 0) publish_partial(part + blockIdx.x, s);
     if (!last_block_arrive(counter)) return;
     const double tot = reduce_partials(part, gridDim.x, red);
     if (threadIdx.x == 0) {
