@@ -126,6 +126,16 @@ int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double*
 int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y);
 /* z = M^-1 r for the ILU(0) preconditioner of the pattern's current values (device arrays, double) */
 int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels);
+/* Same result as vfv_ilu0_apply_device, allocating nothing. No counterpart in the reference: for
+ * callers that may not allocate device memory while they run (a time-step loop under a fixed
+ * memory budget, a host framework whose allocator owns the device memory, code that must not
+ * take the device-wide synchronisation of cudaMalloc/cudaFree mid-step). The work vector comes
+ * from a fixed 2 MiB device array inside the library, so n is limited to 262,144 rows (larger
+ * patterns are rejected with VFV_BAD_INPUT). The pattern's ILU(0) storage must already exist:
+ * call vfv_ilu0_apply_device (or an ILU(0) solve) on it once first. The first call on each device
+ * looks up the array's device address (make it before any stream capture). All calls share the
+ * array: calls that overlap on the GPU race. */
+int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels);
 /* the symmetric permutation the ILU(0) factor lives on: perm[n] (new -> old) and the row ranges of
  * its levels lev_ptr[nlev+1] (any pointer may be NULL; call once with NULLs to learn nlev) */
 int vfv_ilu0_ordering(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int32_t* perm, int32_t* lev_ptr, int32_t* nlev);

@@ -1029,6 +1029,60 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
     return VFV_OK;
 }
 
+// ---------------------------------------------------------------- ILU(0) apply without allocation
+// For callers that may not allocate device memory once they are running: code that drives the
+// solver from inside a time-step loop under a fixed memory budget, or from a host framework whose
+// allocator owns all device memory, or that must not hit the implicit device-wide synchronisation
+// of cudaMalloc/cudaFree in the middle of a step. vfv_ilu0_apply_device allocates its work vector
+// on every call; this variant takes it from one fixed device array compiled into the library.
+//
+// The array is a file-scope __device__ variable: every GPU that loads the library holds its
+// 2 MiB until the process exits. Host code cannot use the variable's name as a device address,
+// so the device address is looked up with cudaGetSymbolAddress once per device, with that device
+// current, by the first call on that device — make that first call before any stream capture.
+// Every call shares the array and it keeps the last call's contents; nothing in it has to start
+// at zero (the sweeps write every element before reading it). Calls that overlap on the GPU, from
+// any context or thread, race on the array.
+namespace {
+constexpr int64_t kNoAllocMaxRows = 1 << 18;  // 262,144 rows of doubles: 2 MiB
+__device__ __align__(256) double g_ilu_scratch[kNoAllocMaxRows];
+constexpr int kNoAllocMaxDevices = 64;
+double* g_ilu_scratch_ptr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels) {
+    if (!ctx || !p || !r || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
+    if (p->n > kNoAllocMaxRows)
+        return set_err(ctx, VFV_BAD_INPUT, "vfv_ilu0_apply_device_noalloc: " + std::to_string(p->n) +
+                                               " rows exceed its fixed work array of " + std::to_string(kNoAllocMaxRows) + " rows");
+    if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices) return set_err(ctx, VFV_BAD_INPUT, "device index out of range");
+    auto it = p->ilu.find(ilu_order);
+    if (it == p->ilu.end())
+        return set_err(ctx, VFV_BAD_INPUT,
+                       "vfv_ilu0_apply_device_noalloc: the pattern's ILU(0) storage is not set up; call vfv_ilu0_apply_device or an "
+                       "ILU(0) solve on it once first (that call allocates)");
+    IluStruct& S = *it->second;
+    double* scratch = g_ilu_scratch_ptr[ctx->device];
+    if (!scratch) {
+        int cur = -1;
+        CK(cudaGetDevice(&cur));
+        if (cur != ctx->device) CK(cudaSetDevice(ctx->device));
+        const cudaError_t e = cudaGetSymbolAddress((void**)&scratch, g_ilu_scratch);
+        if (cur != ctx->device) cudaSetDevice(cur);
+        if (e != cudaSuccess) return set_err(ctx, VFV_CUDA_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_ilu_scratch_ptr[ctx->device] = scratch;
+    }
+    int rc = ilu_refresh(ctx, p, S, false);  // numeric factor into the storage made at set-up
+    if (rc) return rc;
+    ilu_apply<double>(ctx->stream, S, S.lu64.p, r, scratch, z, nullptr);
+    ctx->launches += 2 * S.nlev;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    if (levels) *levels = S.nlev;
+    return VFV_OK;
+}
+
 int vfv_ilu0_ordering(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int32_t* perm, int32_t* lev_ptr, int32_t* nlev) {
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
