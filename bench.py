@@ -288,7 +288,7 @@ def main():
         "err_mixed": e_mx, "err_fp64": e_64, "ref_relres": info_ref.relres,
         "spmv_fp64_gbs": gbs64, "spmv_fp32_gbs": gbs32, "spmv_fp64_ms": sp64 * 1e3, "spmv_fp32_ms": sp32 * 1e3,
         "assembly_ms": asm_s * 1e3, "mesh_setup_s": t_mesh,
-        "roofline": {"bound": "hbm", "kernel": "k_spmv (FP64 CSR, 8 lanes/row)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "k_spmv<double> (CSR, 4 lanes/row)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
                      "frac": gbs64 / peak, "peak_kind": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_launch": bytes64},
         "cpu_baseline": cpu,

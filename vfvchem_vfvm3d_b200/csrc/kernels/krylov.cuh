@@ -100,30 +100,27 @@ __device__ __forceinline__ void reduce_cols_warp(const double* part, int nblk, i
 // ---------------------------------------------------------------- SpMV (CSR, G lanes per row)
 constexpr int kSpG = 4;  // lanes per row: rows hold ~16 non-zeros, 4 lanes x 4 loads in flight each
 
-// This lane's share of row `row` of A x: loads of up to three strides are issued before the
-// multiply-adds so that every lane has several independent loads in flight.
-template <typename TV, typename TX, typename TA, int G>
+// This lane's share of row `row` of A x. The row's first S*G column indices and values are loaded
+// before any x is gathered (S strides per lane, all independent), which keeps several loads in
+// flight per lane; rows longer than S*G finish in a tail loop.
+template <typename TV, typename TX, typename TA, int G, int S = 4>
 __device__ __forceinline__ TA row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const TV* __restrict__ val,
                                       const TX* __restrict__ x, int64_t row, int lane) {
-    TA s = TA(0);
     const int32_t b = __ldg(rp + row), e = __ldg(rp + row + 1);
-    int32_t k = b + lane;
-    for (; k + 2 * G < e; k += 3 * G) {
-        const int32_t c0 = __ldcs(ci + k), c1 = __ldcs(ci + k + G), c2 = __ldcs(ci + k + 2 * G);
-        const TV v0 = __ldcs(val + k), v1 = __ldcs(val + k + G), v2 = __ldcs(val + k + 2 * G);
-        s += (TA)v0 * (TA)__ldg(x + c0) + (TA)v1 * (TA)__ldg(x + c1) + (TA)v2 * (TA)__ldg(x + c2);
-    }
-    int32_t c[3];
-    TV v[3];
+    int32_t c[S];
+    TV v[S];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        const int32_t kk = k + q * G;
-        c[q] = kk < e ? __ldcs(ci + kk) : -1;
-        v[q] = kk < e ? __ldcs(val + kk) : TV(0);
+    for (int t = 0; t < S; ++t) {
+        const int32_t k = b + lane + t * G;
+        const bool ok = k < e;
+        c[t] = ok ? __ldcs(ci + k) : -1;
+        v[t] = ok ? __ldcs(val + k) : TV(0);
     }
+    TA s = TA(0);
 #pragma unroll
-    for (int q = 0; q < 3; ++q)
-        if (c[q] >= 0) s += (TA)v[q] * (TA)__ldg(x + c[q]);
+    for (int t = 0; t < S; ++t)
+        if (c[t] >= 0) s += (TA)v[t] * (TA)__ldg(x + c[t]);
+    for (int32_t k = b + lane + S * G; k < e; k += G) s += (TA)__ldcs(val + k) * (TA)__ldg(x + __ldcs(ci + k));
     return s;
 }
 
