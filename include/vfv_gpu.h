@@ -167,6 +167,13 @@ int vfv_heat_assemble(vfv_ctx* ctx, vfv_heat* h, const double* k, const double* 
                       const double* bc_val, int on_device, double* b_out);
 /* device pointer of the assembled right-hand side (n_tot doubles, owned by h) */
 const double* vfv_heat_rhs_device(vfv_heat* h);
+/* Adjoint gradient of an objective J(T) of the heat solution (zero production, s = 0), the
+ * backward() of the assembly + solve: solves A^T lambda = dJ/dT with GMRES (opts) and returns
+ * dJ/d(log k) and dJ/dq per vertex, for the k, q of the last vfv_heat_assemble. Host arrays of
+ * n_tot doubles; lambda, dJdlogk, dJdq may be NULL. No reference counterpart (the reference has no
+ * adjoint); its operators are the ones of SteadyHeat::assemble_matrix, steady_heat.rs:143-171. */
+int vfv_heat_adjoint(vfv_ctx* ctx, vfv_heat* h, const double* T, const double* dJdT, const vfv_gmres_opts* opts, double* lambda,
+                     double* dJdlogk, double* dJdq, vfv_solve_info* info);
 /* gradient of one field on the heat mesh: grad[3][n_tot] (host arrays) */
 int vfv_update_grad(vfv_ctx* ctx, vfv_heat* h, const double* f, double* grad);
 

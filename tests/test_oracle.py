@@ -181,3 +181,26 @@ def test_heat_slab_profile(lib_built):
     pos, _, _ = prob.mesh.export()
     exact = pos[:, 0] + pos[:, 0] * (1.0 - pos[:, 0]) / 2.0
     assert np.max(np.abs(x - exact)) < 5e-3
+
+
+def test_oracle_adjoint_matches_finite_differences(lib_built):
+    """Config 3 check at small size: the oracle's adjoint gradient against central differences
+    (step 1e-6) of the oracle's own forward model, on random unit directions in (log k, q)."""
+    from oracle import adjoint
+    from vfvchem_vfvm3d_b200.problems import steady_heat
+    prob = steady_heat(9, hetero=True)
+    rng = np.random.default_rng(11)
+    sensors = rng.choice(prob.n, size=40, replace=False)
+    target = rng.uniform(0.0, 1.0, sensors.size)
+    logk = np.log(prob.k)
+    J, gk, gq, _ = adjoint.gradient(prob, logk, prob.q, sensors, target)
+    worst = 0.0
+    for _ in range(6):
+        dk = rng.standard_normal(prob.n)
+        dq = rng.standard_normal(prob.n)
+        nrm = np.sqrt(dk @ dk + dq @ dq)
+        dk, dq = dk / nrm, dq / nrm
+        fd = adjoint.fd_directional(prob, logk, prob.q, sensors, target, dk, dq)
+        ad = gk @ dk + gq @ dq
+        worst = max(worst, abs(fd - ad) / max(abs(ad), 1e-30))
+    assert worst < 1e-6

@@ -87,6 +87,7 @@ SIGNATURES = [
     ("vfv_heat_assemble", C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_int, _DP]),
     ("vfv_heat_rhs_device", C.c_void_p, [_P]),
     ("vfv_update_grad", C.c_int, [_P, _P, _DP, _DP]),
+    ("vfv_heat_adjoint", C.c_int, [_P, _P, _DP, _DP, C.POINTER(GmresOpts), _DP, _DP, _DP, C.POINTER(SolveInfo)]),
 ]
 
 _lib = None

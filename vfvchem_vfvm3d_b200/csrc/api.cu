@@ -8,6 +8,7 @@
 #include "../../include/vfv_gpu.h"
 #include "common.cuh"
 #include "host/mesh.hpp"
+#include "kernels/adjoint.cuh"
 #include "kernels/assemble.cuh"
 #include "kernels/ilu0.cuh"
 #include "kernels/gmres_cycle.cuh"
@@ -781,7 +782,15 @@ struct vfv_heat {
     DBuf<double> area, dist, skew, gw, cvol, cskew, barea, bw;
     DBuf<double> f, grad, b;  // f: [5][n] = k, q, s, T, bc_val ; grad: [4][3][n]
     vfv_pattern* pat = nullptr;
-    ~vfv_heat() { delete pat; }
+    // adjoint (built on first use): transpose pattern, value map, reverse faces, work arrays
+    vfv_pattern* pat_t = nullptr;
+    DBuf<int32_t> tmap, rev;
+    DBuf<double> adj_work;  // pv, pn [n_dir]; sk [3 n_dir]; gkm [n]; psi [3 n]; T, g, lambda, zero, dlogk, dq [n]
+    std::vector<int32_t> h_rev;
+    ~vfv_heat() {
+        delete pat_t;
+        delete pat;
+    }
 };
 
 // ================================================================ C ABI
@@ -1246,7 +1255,98 @@ int vfv_heat_create(vfv_ctx* ctx, const vfv_mesh* mh, int32_t n_bnd, const int32
     CK(h->f.alloc(5 * n));
     CK(h->grad.alloc(12 * n));
     CK(h->b.alloc(n));
+    h->h_rev.resize(d.n_dir);
+    for (int64_t i = 0; i < d.n_dir; ++i) h->h_rev[i] = (int32_t)d.nbr_rev[i];
     *out = h.release();
+    return VFV_OK;
+}
+
+// Adjoint of the heat assembly (zero production): solve A^T lambda = dJ/dT with the GMRES of
+// vfv_solve, then dJ/d(log k) and dJ/dq by the gather kernels of kernels/adjoint.cu. Uses k, q
+// and their gradients from the last vfv_heat_assemble call.
+int vfv_heat_adjoint(vfv_ctx* ctx, vfv_heat* h, const double* T, const double* dJdT, const vfv_gmres_opts* opts, double* lambda,
+                     double* dJdlogk, double* dJdq, vfv_solve_info* info) {
+    if (!ctx || !h || !T || !dJdT) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    int rc = check_opts(ctx, opts);
+    if (rc) return rc;
+    if (info) std::memset(info, 0, sizeof(*info));
+    const int64_t n = h->n, E = h->n_dir;
+    cudaStream_t s = ctx->stream;
+    if (!h->pat_t) {
+        // transpose of the heat pattern: row j of A^T lists, in ascending order, the rows i of A
+        // with an entry in column j; tmap[k_t] = slot of that entry in A
+        const std::vector<int32_t>& rp = h->pat->h_rp;
+        const std::vector<int32_t>& ci = h->pat->h_ci;
+        const int64_t nnz = h->pat->nnz;
+        std::vector<int32_t> trp(n + 1, 0), tci(nnz), tmap(nnz);
+        for (int64_t k = 0; k < nnz; ++k) trp[ci[k] + 1]++;
+        for (int64_t j = 0; j < n; ++j) trp[j + 1] += trp[j];
+        std::vector<int32_t> cur(trp.begin(), trp.end() - 1);
+        for (int64_t i = 0; i < n; ++i)
+            for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+                const int32_t q = cur[ci[k]]++;
+                tci[q] = (int32_t)i;
+                tmap[q] = k;
+            }
+        vfv_pattern* pt = nullptr;
+        rc = vfv_pattern_from_csr(ctx, n, trp.data(), tci.data(), &pt);
+        if (rc) return rc;
+        h->pat_t = pt;
+        CK(h->tmap.upload(tmap.data(), nnz, s));
+        CK(h->rev.upload(h->h_rev.data(), E, s));
+        CK(h->adj_work.alloc((size_t)5 * E + (size_t)10 * n));
+    }
+    double* w = h->adj_work.p;
+    double* pv = w;
+    double* pn = w + E;
+    double* sk = w + 2 * E;
+    double* gkm = w + 5 * E;
+    double* psi = gkm + n;
+    double* dT = psi + 3 * n;
+    double* dg = dT + n;
+    double* dl = dg + n;
+    double* dzero = dl + n;
+    double* ddk = dzero + n;
+    double* ddq = ddk + n;
+    k_gather_vals<double><<<grid_for(h->pat->nnz), 256, 0, s>>>(h->pat->nnz, h->tmap.p, h->pat->val.p, h->pat_t->val.p);
+    ctx->launches += 1;
+    h->pat_t->version++;
+    CK(cudaMemcpyAsync(dT, T, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dg, dJdT, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(dzero, 0, n * sizeof(double), s));
+    rc = solve_dev(ctx, h->pat_t, dg, dzero, dl, opts, info);
+    if (rc) return rc;
+    AdjDev D{};
+    D.n = n;
+    D.n_dir = E;
+    D.np = h->np.p;
+    D.ni = h->ni.p;
+    D.rev = h->rev.p;
+    D.kind = h->kind.p;
+    D.area = h->area.p;
+    D.dist = h->dist.p;
+    D.skew = h->skew.p;
+    D.gw = h->gw.p;
+    D.cvol = h->cvol.p;
+    D.cskew = h->cskew.p;
+    D.k = h->f.p;
+    D.gk = h->grad.p;
+    D.T = dT;
+    D.lambda = dl;
+    D.pv = pv;
+    D.pn = pn;
+    D.sk = sk;
+    D.gkm = gkm;
+    D.psi = psi;
+    D.dlogk = ddk;
+    D.dq = ddq;
+    launch_adjoint_partials(s, D);
+    ctx->launches += 3;
+    CK(cudaGetLastError());
+    if (lambda) CK(cudaMemcpyAsync(lambda, dl, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (dJdlogk) CK(cudaMemcpyAsync(dJdlogk, ddk, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (dJdq) CK(cudaMemcpyAsync(dJdq, ddq, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     return VFV_OK;
 }
 

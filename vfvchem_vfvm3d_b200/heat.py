@@ -50,6 +50,19 @@ class SteadyHeatGpu:
     def rhs_device_ptr(self) -> int:
         return L.load().vfv_heat_rhs_device(self._h) or 0
 
+    def adjoint(self, T, dJdT, opts=None):
+        """backward(): (lambda, dJ/dlog k, dJ/dq) for an objective J(T) with gradient dJdT at the state T."""
+        from .core import GmresOptions, SolveInfo
+        opts = opts or GmresOptions(tol=1e-12, restart=50, max_outer=2000, precond=L.PRECOND_ILU0)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        g = np.ascontiguousarray(dJdT, dtype=np.float64)
+        lam, dk, dq = np.empty(self.n), np.empty(self.n), np.empty(self.n)
+        info = L.SolveInfo()
+        o = opts.to_c()
+        _check(self.ctx.handle, L.load().vfv_heat_adjoint(self.ctx.handle, self._h, L.dptr(T), L.dptr(g), C.byref(o), L.dptr(lam),
+                                                         L.dptr(dk), L.dptr(dq), C.byref(info)))
+        return lam, dk, dq, SolveInfo.from_c(info)
+
     def grad(self, f) -> np.ndarray:
         f = np.ascontiguousarray(f, dtype=np.float64)
         g = np.empty((3, self.n))
