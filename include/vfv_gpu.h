@@ -57,6 +57,7 @@ typedef struct vfv_ctx vfv_ctx;
 typedef struct vfv_pattern vfv_pattern;
 typedef struct vfv_mesh vfv_mesh;
 typedef struct vfv_heat vfv_heat;
+typedef struct vfv_transport vfv_transport;
 
 /* Options of LinearGmres::new_with_options(num_thread, tol, restart, max_outer)
  * (linear_gmres.rs:24; defaults tol 1e-6, restart 50, max_outer 200 at :20-22).
@@ -145,6 +146,8 @@ int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out);
 /* a mesh from given vertices (points first, then nodes with a boundary id each) */
 int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out);
 void vfv_mesh_destroy(vfv_mesh* m);
+/* count meshes at once (built in parallel on the host): out[i] = jitter cube of n[i]^3 points, seeds[i] */
+int vfv_mesh_jitter_cubes(int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out);
 /* counts: vertices split, tetrahedra, directed faces (2 x Voronoi faces), boundary sub-faces */
 int vfv_mesh_info(const vfv_mesh* m, int64_t* n_pts, int64_t* n_nds, int64_t* n_tet, int64_t* n_dir, int64_t* n_bsub);
 /* copy arrays out; any pointer may be NULL. Vector quantities are component-major [3][count]. */
@@ -176,6 +179,25 @@ int vfv_heat_adjoint(vfv_ctx* ctx, vfv_heat* h, const double* T, const double* d
                      double* dJdlogk, double* dJdq, vfv_solve_info* info);
 /* gradient of one field on the heat mesh: grad[3][n_tot] (host arrays) */
 int vfv_update_grad(vfv_ctx* ctx, vfv_heat* h, const double* f, double* grad);
+
+/* ---- batched transient transport (config 4): one species, implicit Euler, zero-flux walls.
+ * The meshes are concatenated into one block-diagonal system; every kernel runs over all of them.
+ * Per row, in push order: OpSclDomTimeUnity (opscl_dom_timeunity.rs:32-58), OpSclDomDiffusion
+ * (opscl_dom_diff.rs:40-91), OpSclDomAdvection (power law, opscl_dom_adv.rs:49-125) with the face mass
+ * flux of flow_helper::update_flux (flow_helper.rs:72-179) at zero pressure and body force; density
+ * and species weight 1. The reference has no solver that wires this composition (TransientMass has
+ * no advection). */
+int vfv_transport_create(vfv_ctx* ctx, int nmesh, vfv_mesh* const* meshes, double dt, vfv_transport** out);
+void vfv_transport_destroy(vfv_transport* t);
+vfv_pattern* vfv_transport_pattern(vfv_transport* t);
+/* row_ptr[nmesh+1] (may be NULL): row offsets of the meshes in the concatenated system */
+int vfv_transport_info(const vfv_transport* t, int64_t* n_tot, int64_t* nnz, int32_t* nmesh, int64_t* row_ptr);
+/* matrix from the diffusivity D[n_tot] and velocity vel[3][n_tot] (host or device arrays) */
+int vfv_transport_assemble(vfv_ctx* ctx, vfv_transport* t, const double* D, const double* vel, int on_device);
+/* nsteps implicit-Euler steps from c0 (host, n_tot) to c_out (host); one batched GMRES per step,
+ * converged when every mesh meets ||b_i - A_i c_i|| <= tol ||b_i||; iters[nsteps] may be NULL */
+int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, const vfv_gmres_opts* opts, double* c_out,
+                      int32_t* iters);
 
 #ifdef __cplusplus
 }

@@ -49,6 +49,7 @@ def lib():
             build()
         _lib = C.CDLL(_SO)
         _lib.orc_heat_triplets.restype = C.c_int64
+        _lib.orc_transport_triplets.restype = C.c_int64
         _lib.orc_csr_from_triplets.restype = C.c_int64
         _lib.orc_gmres.restype = C.c_int
         _lib.orc_ilu0_factor.restype = C.c_int
@@ -107,6 +108,27 @@ def heat_triplets(dual: dict, n_pts: int, node_bnd: np.ndarray, bnd_order, bnd_k
                                  _p(gk), _p(gq), _p(gs), _p(gT), _p(r), _p(c), _p(v), _p(b))
     del keep
     return r[:nt].copy(), c[:nt].copy(), v[:nt].copy(), b
+
+
+def transport_triplets(dual: dict, n_pts: int, node_bnd: np.ndarray, D, vel, dt: float):
+    """Triplets of the config-4 transport operator (time + diffusion + power-law advection) of one
+    mesh in push order. vel is [3][n]; gradients come from oracle.grad."""
+    n = dual["nbr_ptr"].size - 1
+    d, keep = _orc_dual(dual, n_pts)
+    D = _c(np.broadcast_to(D, (n,)), np.float64)
+    vel = _c(vel, np.float64).reshape(3, n)
+    gD = grad(dual, D)
+    gvel = _c(np.concatenate([grad(dual, vel[q]) for q in range(3)]), np.float64)
+    norm = _c(dual["norm"], np.float64)
+    nb = _c(node_bnd, np.int32)
+    cap = 4 * dual["nbr_idx"].size + 2 * n
+    r = np.empty(cap, np.uint64)
+    c = np.empty(cap, np.uint64)
+    v = np.empty(cap)
+    nt = lib().orc_transport_triplets(C.byref(d), _p(norm), _p(nb), C.c_int32(int(nb.max()) + 1 if nb.size else 0), _p(D), _p(gD),
+                                      _p(vel), _p(gvel), C.c_double(dt), _p(r), _p(c), _p(v))
+    del keep
+    return r[:nt].copy(), c[:nt].copy(), v[:nt].copy()
 
 
 def csr_from_triplets(n: int, rows, cols, vals):

@@ -169,6 +169,92 @@ int64_t orc_heat_triplets(const orc_dual* d, const int32_t* node_bnd, int32_t n_
 }
 
 /* ------------------------------------------------------------------------------------------ */
+/*
+ * Transient advection-diffusion (config 4) for one mesh, in push order per operator: time
+ * (OpSclDomTimeUnity::apply_time, opscl_dom_timeunity.rs:32-58) over points, diffusion
+ * (opscl_dom_diff.rs:55-87) over points, advection (OpSclDomAdvection, opscl_dom_adv.rs:49-125)
+ * over points, then the boundary twins (opscl_bnd_timeunity, opscl_bnd_diff, opscl_bnd_adv) for
+ * the nodes of each zero-flux boundary in boundary order. Face mass flux from
+ * flow_helper::update_flux (flow_helper.rs:72-179) with zero pressure and body force, density and
+ * species weight 1. gvel is [9][n] (du/dx, du/dy, du/dz, dv/dx, ...). Returns the triplet count.
+ */
+static int64_t transport_row_time(const orc_dual* d, int64_t v, double dt, uint64_t* r, uint64_t* c, double* val, int64_t t) {
+    return push(r, c, val, t, v, v, -d->cvol[v] / dt);
+}
+
+static double face_df(const orc_dual* d, int64_t v, int64_t i, const double* D, const double* gD) {
+    const int64_t N = d->n, E = d->n_dir;
+    const int64_t nb = d->ni[i];
+    const double dv = D[v], dn = D[nb];
+    const double sx = d->skew[i], sy = d->skew[E + i], sz = d->skew[2 * E + i];
+    const double dm = (dv + dn != 0.0) ? 2.0 * dv * dn / (dv + dn) : 0.0;
+    double df = dm + 0.5 * (sx * (gD[v] + gD[nb]) + sy * (gD[N + v] + gD[N + nb]) + sz * (gD[2 * N + v] + gD[2 * N + nb]));
+    return df > 0.0 ? df : dm;
+}
+
+static double face_flux(const orc_dual* d, const double* norm, int64_t v, int64_t i, const double* vel, const double* gvel) {
+    const int64_t N = d->n, E = d->n_dir;
+    const int64_t nb = d->ni[i];
+    const double sx = d->skew[i], sy = d->skew[E + i], sz = d->skew[2 * E + i];
+    const double nx = norm[i], ny = norm[E + i], nz = norm[2 * E + i];
+    const double den_f = 0.5 * (1.0 + 1.0) + 0.5 * (sx * (0.0 + 0.0) + sy * (0.0 + 0.0) + sz * (0.0 + 0.0));
+    double uf[3];
+    for (int q = 0; q < 3; ++q) {
+        const double* g = gvel + 3 * q * N;
+        uf[q] = 0.5 * (vel[q * N + v] + vel[q * N + nb]) + 0.5 * (sx * (g[v] + g[nb]) + sy * (g[N + v] + g[N + nb]) + sz * (g[2 * N + v] + g[2 * N + nb]));
+    }
+    return den_f * (uf[0] * nx + uf[1] * ny + uf[2] * nz + 0.0) * d->area[i];
+}
+
+static int64_t transport_row_diff(const orc_dual* d, int64_t v, const double* D, const double* gD, uint64_t* r, uint64_t* c, double* val,
+                                  int64_t t) {
+    for (int64_t i = d->np[v]; i < d->np[v + 1]; ++i) {
+        const double cond = face_df(d, v, i, D, gD) * d->area[i] / d->dist[i];
+        t = push(r, c, val, t, v, d->ni[i], cond);
+        t = push(r, c, val, t, v, v, -cond);
+    }
+    return t;
+}
+
+static int64_t transport_row_adv(const orc_dual* d, const double* norm, int64_t v, const double* D, const double* gD, const double* vel,
+                                 const double* gvel, uint64_t* r, uint64_t* c, double* val, int64_t t) {
+    for (int64_t i = d->np[v]; i < d->np[v + 1]; ++i) {
+        const int64_t E = d->n_dir;
+        const double sx = d->skew[i], sy = d->skew[E + i], sz = d->skew[2 * E + i];
+        const double wgt_f = 0.5 * (1.0 + 1.0) + 0.5 * (sx * (0.0 + 0.0) + sy * (0.0 + 0.0) + sz * (0.0 + 0.0));
+        const double den_f = wgt_f;
+        const double cond = face_df(d, v, i, D, gD) * d->area[i] / d->dist[i];
+        const double flux = den_f != 0.0 ? wgt_f / den_f * face_flux(d, norm, v, i, vel, gvel) : 0.0;
+        const double pe = cond != 0.0 ? flux / cond : 0.0;
+        double x = 1.0 - 0.1 * fabs(pe);
+        x = x > 0.0 ? x : 0.0;
+        const double x2 = x * x;
+        const double coeff = cond * (x2 * x2 * x - 1.0) + (-flux > 0.0 ? -flux : 0.0);
+        t = push(r, c, val, t, v, d->ni[i], coeff);
+        t = push(r, c, val, t, v, v, -coeff);
+    }
+    return t;
+}
+
+int64_t orc_transport_triplets(const orc_dual* d, const double* norm, const int32_t* node_bnd, int32_t n_bnd, const double* D,
+                               const double* gD, const double* vel, const double* gvel, double dt, uint64_t* r, uint64_t* c,
+                               double* val) {
+    int64_t t = 0;
+    for (int64_t v = 0; v < d->n_pts; ++v) t = transport_row_time(d, v, dt, r, c, val, t);
+    for (int64_t v = 0; v < d->n_pts; ++v) t = transport_row_diff(d, v, D, gD, r, c, val, t);
+    for (int64_t v = 0; v < d->n_pts; ++v) t = transport_row_adv(d, norm, v, D, gD, vel, gvel, r, c, val, t);
+    for (int32_t b = 0; b < n_bnd; ++b) {
+        for (int64_t v = d->n_pts; v < d->n; ++v)
+            if (node_bnd[v] == b) t = transport_row_time(d, v, dt, r, c, val, t);
+        for (int64_t v = d->n_pts; v < d->n; ++v)
+            if (node_bnd[v] == b) t = transport_row_diff(d, v, D, gD, r, c, val, t);
+        for (int64_t v = d->n_pts; v < d->n; ++v)
+            if (node_bnd[v] == b) t = transport_row_adv(d, norm, v, D, gD, vel, gvel, r, c, val, t);
+    }
+    return t;
+}
+
+/* ------------------------------------------------------------------------------------------ */
 /* stable sort of triplet indices by (row, col): counting sort on col, then on row */
 static void stable_order(int64_t n, int64_t nt, const uint64_t* r, const uint64_t* c, int64_t* ord) {
     int64_t* cnt = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));

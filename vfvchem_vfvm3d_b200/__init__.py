@@ -27,9 +27,10 @@ from .core import Context, Pattern, GmresOptions, SolveInfo, default_context  # 
 from .mesh import Mesh  # noqa: F401
 from .heat import SteadyHeatGpu  # noqa: F401
 from .linear import LinearGmres, Triplet, SparseMatrix  # noqa: F401
+from .transport import TransientTransportGpu  # noqa: F401
 from . import _lib  # noqa: F401
 
 __all__ = [
     "Context", "Pattern", "GmresOptions", "SolveInfo", "Mesh", "SteadyHeatGpu", "LinearGmres", "Triplet",
-    "SparseMatrix", "VFVChemError", "LinearGmresDidNotConverge", "default_context",
+    "SparseMatrix", "VFVChemError", "LinearGmresDidNotConverge", "default_context", "TransientTransportGpu",
 ]

@@ -78,6 +78,7 @@ SIGNATURES = [
     ("vfv_mesh_jitter_cube", C.c_int, [C.c_int, C.c_uint64, C.c_double, _PP]),
     ("vfv_mesh_from_vertices", C.c_int, [C.c_int64, C.c_int64, _DP, _I32P, _PP]),
     ("vfv_mesh_destroy", None, [_P]),
+    ("vfv_mesh_jitter_cubes", C.c_int, [C.c_int, _I32P, _U64P, C.c_double, C.POINTER(C.c_void_p)]),
     ("vfv_mesh_info", C.c_int, [_P, _I64P, _I64P, _I64P, _I64P, _I64P]),
     ("vfv_mesh_export", C.c_int, [_P, _DP, _I32P, _I32P]),
     ("vfv_mesh_export_dual", C.c_int, [_P, _I64P, _I32P, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _I64P, _I32P, _I32P, _DP, _DP, _DP]),
@@ -87,6 +88,12 @@ SIGNATURES = [
     ("vfv_heat_assemble", C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_int, _DP]),
     ("vfv_heat_rhs_device", C.c_void_p, [_P]),
     ("vfv_update_grad", C.c_int, [_P, _P, _DP, _DP]),
+    ("vfv_transport_create", C.c_int, [_P, C.c_int, C.POINTER(C.c_void_p), C.c_double, _PP]),
+    ("vfv_transport_destroy", None, [_P]),
+    ("vfv_transport_pattern", C.c_void_p, [_P]),
+    ("vfv_transport_info", C.c_int, [_P, _I64P, _I64P, _I32P, _I64P]),
+    ("vfv_transport_assemble", C.c_int, [_P, _P, _P, _P, C.c_int]),
+    ("vfv_transport_run", C.c_int, [_P, _P, _DP, C.c_int, C.POINTER(GmresOpts), _DP, _I32P]),
     ("vfv_heat_adjoint", C.c_int, [_P, _P, _DP, _DP, C.POINTER(GmresOpts), _DP, _DP, _DP, C.POINTER(SolveInfo)]),
 ]
 

@@ -363,6 +363,7 @@ struct Gmres : SolverBase {
     int nblk = 0, mega_grid = 0, mega_chunk = 0;
     DBuf<T> V, z, z2, zc, valK;
     DBuf<unsigned> bar;
+    DBuf<double> blk_buf;  // per-block residual / rhs norms of a batched solve
     DBuf<unsigned long long> trace;  // per-phase timestamps of the last cycle (VFV_TRACE_CYCLE=1)
     DBuf<double> part, hacc, coef, H, cs, sn, g, beta, inv_beta, y, dinv, scal, x, b;
     DBuf<unsigned> counter;
@@ -602,8 +603,11 @@ struct Gmres : SolverBase {
         k_residual<T, G><<<sp_blocks, kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
     }
 
+    // nblk > 0: block-diagonal system with block row ranges blk_d[0..nblk] (device); converged
+    // when every block meets ||b_i - A_i x_i|| <= tol ||b_i|| (the device stops a cycle early only on
+    // ||r|| <= tol min_i ||b_i||, which implies it for every block).
     int solve(vfv_ctx* ctx, vfv_pattern* p, const double* d_b, const double* d_x0, double* d_x, const vfv_gmres_opts& o,
-              vfv_solve_info* info) {
+              vfv_solve_info* info, int nblk = 0, const int64_t* blk_d = nullptr) {
         cudaStream_t s = ctx->stream;
         constexpr int G = kSpG;
         const bool mixed = !std::is_same<T, double>::value;
@@ -645,7 +649,22 @@ struct Gmres : SolverBase {
             }
             return VFV_OK;
         }
-        const double hs[2] = {o.tol * bnorm, mixed ? std::max(0.0, o.inner_rtol) : 0.0};
+        double tol_abs = o.tol * bnorm;
+        std::vector<double> blk_b2, blk_r2;
+        if (nblk > 0) {
+            if ((int64_t)blk_buf.n < 2 * (int64_t)nblk) CK(blk_buf.alloc(2 * (size_t)nblk));
+            k_block_resid2<<<nblk, kBlk, 0, s>>>(p->rp.p, p->ci.p, p->val.p, x.p, b.p, blk_d, blk_buf.p, blk_buf.p + nblk);
+            ctx->launches += 1;
+            blk_b2.resize(nblk);
+            blk_r2.resize(nblk);
+            CK(cudaMemcpyAsync(blk_b2.data(), blk_buf.p + nblk, nblk * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            double bmin = 1e300;
+            for (double v : blk_b2)
+                if (v > 0.0) bmin = std::min(bmin, std::sqrt(v));
+            tol_abs = o.tol * (bmin < 1e300 ? bmin : bnorm);
+        }
+        const double hs[2] = {tol_abs, mixed ? std::max(0.0, o.inner_rtol) : 0.0};
         CK(cudaMemcpyAsync(scal.p, hs, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
         CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
         k_residual<T, G><<<grid_for(n * G), kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
@@ -679,6 +698,15 @@ struct Gmres : SolverBase {
                 break;
             }
             if (hst.converged) break;
+            if (nblk > 0 && cycles > 0) {
+                k_block_resid2<<<nblk, kBlk, 0, s>>>(p->rp.p, p->ci.p, p->val.p, x.p, b.p, blk_d, blk_buf.p, nullptr);
+                ctx->launches += 1;
+                CK(cudaMemcpyAsync(blk_r2.data(), blk_buf.p, nblk * sizeof(double), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                bool all = true;
+                for (int i = 0; i < nblk && all; ++i) all = blk_r2[i] <= o.tol * o.tol * blk_b2[i];
+                if (all) break;
+            }
             if (cycles >= o.max_outer) {
                 rc = VFV_NOT_CONVERGED;
                 break;
@@ -729,7 +757,8 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
     return VFV_OK;
 }
 
-int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info) {
+int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info,
+              int nblk = 0, const int64_t* blk_d = nullptr) {
     const auto key = std::make_tuple(o->precision, o->precond, o->precond == VFV_PRECOND_ILU0 ? o->ilu_order : 0, o->restart, o->engine);
     auto it = p->solvers.find(key);
     if (it == p->solvers.end()) {
@@ -747,8 +776,8 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
         if (rc) return rc;
         it = p->solvers.emplace(key, std::move(sb)).first;
     }
-    if (o->precision == VFV_MIXED) return static_cast<Gmres<float>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info);
-    return static_cast<Gmres<double>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info);
+    if (o->precision == VFV_MIXED) return static_cast<Gmres<float>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info, nblk, blk_d);
+    return static_cast<Gmres<double>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info, nblk, blk_d);
 }
 
 int finish_pattern(vfv_ctx* ctx, vfv_pattern* p) {
@@ -791,6 +820,20 @@ struct vfv_heat {
         delete pat_t;
         delete pat;
     }
+};
+
+// Concatenation of several meshes into one block-diagonal transport system (config 4).
+struct vfv_transport {
+    vfv_ctx* ctx = nullptr;
+    int nmesh = 0;
+    int64_t n = 0, n_dir = 0;
+    double dt = 0.0;
+    std::vector<int64_t> row_ptr;  // [nmesh+1] vertex (row) offsets of the meshes
+    DBuf<int64_t> d_row_ptr;
+    DBuf<int32_t> np, ni, dloc;
+    DBuf<double> area, dist, skew, norm, gw, cvol, flux, fields, grads, b, c0, c1;
+    vfv_pattern* pat = nullptr;
+    ~vfv_transport() { delete pat; }
 };
 
 // ================================================================ C ABI
@@ -1145,6 +1188,43 @@ int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, cons
 
 void vfv_mesh_destroy(vfv_mesh* m) { delete m; }
 
+int vfv_mesh_jitter_cubes(int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out) {
+    if (count <= 0 || !n || !seeds || !out) return set_err(nullptr, VFV_BAD_INPUT, "invalid batch arguments");
+    for (int i = 0; i < count; ++i) {
+        out[i] = nullptr;
+        if (n[i] < 3 || n[i] > 400) return set_err(nullptr, VFV_BAD_INPUT, "grid size n must be in [3, 400]");
+    }
+    if (!(jitter >= 0.0 && jitter < 0.5)) return set_err(nullptr, VFV_BAD_INPUT, "jitter must be in [0, 0.5)");
+    std::vector<std::string> errs(count);
+    // meshes in parallel (largest first); the per-mesh OpenMP loops run serially inside
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int t = 0; t < count; ++t) {
+        const int i = order[t];
+        auto* mh = new vfv_mesh();
+        mh->m = make_jitter_cube(n[i], seeds[i], jitter);
+        std::string e = delaunay(mh->m);
+        if (e.empty()) e = build_dual(mh->m, mh->d);
+        if (!e.empty()) {
+            errs[i] = e;
+            delete mh;
+        } else {
+            out[i] = mh;
+        }
+    }
+    for (int i = 0; i < count; ++i)
+        if (!errs[i].empty()) {
+            for (int j = 0; j < count; ++j) {
+                delete out[j];
+                out[j] = nullptr;
+            }
+            return set_err(nullptr, VFV_BAD_INPUT, "mesh " + std::to_string(i) + ": " + errs[i]);
+        }
+    return VFV_OK;
+}
+
 int vfv_mesh_info(const vfv_mesh* m, int64_t* n_pts, int64_t* n_nds, int64_t* n_tet, int64_t* n_dir, int64_t* n_bsub) {
     if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
     if (n_pts) *n_pts = m->m.n_pts;
@@ -1424,6 +1504,163 @@ int vfv_update_grad(vfv_ctx* ctx, vfv_heat* h, const double* f, double* grad) {
     launch_grad(s, n, h->np.p, h->ni.p, h->gw.p, h->n_dir, 1, fl, gd.p);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(grad, gd.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return VFV_OK;
+}
+
+// ---------------------------------------------------------------- transient transport (config 4)
+int vfv_transport_create(vfv_ctx* ctx, int nmesh, vfv_mesh* const* meshes, double dt, vfv_transport** out) {
+    if (!ctx || nmesh <= 0 || !meshes || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (!(dt > 0.0)) return set_err(ctx, VFV_BAD_INPUT, "dt must be positive");
+    *out = nullptr;
+    auto t = std::make_unique<vfv_transport>();
+    t->ctx = ctx;
+    t->nmesh = nmesh;
+    t->dt = dt;
+    t->row_ptr.assign(nmesh + 1, 0);
+    int64_t ndir = 0;
+    for (int i = 0; i < nmesh; ++i) {
+        if (!meshes[i]) return set_err(ctx, VFV_BAD_INPUT, "NULL mesh");
+        t->row_ptr[i + 1] = t->row_ptr[i] + meshes[i]->d.n_tot;
+        ndir += meshes[i]->d.n_dir;
+    }
+    const int64_t n = t->row_ptr[nmesh];
+    if (n + ndir >= (int64_t)1 << 31) return set_err(ctx, VFV_BAD_INPUT, "batch too large for 32-bit indices");
+    t->n = n;
+    t->n_dir = ndir;
+    std::vector<int32_t> np(n + 1, 0), ni(ndir), dloc(n), rp(n + 1, 0), ci;
+    std::vector<double> area(ndir), dist(ndir), skew(3 * ndir), norm(3 * ndir), gw(3 * ndir), cvol(n);
+    ci.reserve(ndir + n);
+    int64_t e0 = 0;
+    for (int i = 0; i < nmesh; ++i) {
+        const Dual& d = meshes[i]->d;
+        const int64_t v0 = t->row_ptr[i], D = d.n_dir;
+        for (int64_t v = 0; v < d.n_tot; ++v) {
+            const int64_t gv = v0 + v;
+            np[gv] = (int32_t)(e0 + d.nbr_ptr[v]);
+            cvol[gv] = d.cvol[v];
+            const int64_t b = d.nbr_ptr[v], e = d.nbr_ptr[v + 1];
+            int32_t dl = 0;
+            while (b + dl < e && d.nbr_idx[b + dl] < v) ++dl;
+            dloc[gv] = dl;
+            for (int64_t k = b; k < b + dl; ++k) ci.push_back((int32_t)(v0 + d.nbr_idx[k]));
+            ci.push_back((int32_t)gv);
+            for (int64_t k = b + dl; k < e; ++k) ci.push_back((int32_t)(v0 + d.nbr_idx[k]));
+            rp[gv + 1] = (int32_t)ci.size();
+        }
+        for (int64_t k = 0; k < D; ++k) {
+            ni[e0 + k] = (int32_t)(v0 + d.nbr_idx[k]);
+            area[e0 + k] = d.area[k];
+            dist[e0 + k] = d.dist[k];
+            for (int c = 0; c < 3; ++c) {
+                skew[c * ndir + e0 + k] = d.skew[c * D + k];
+                norm[c * ndir + e0 + k] = d.norm[c * D + k];
+                gw[c * ndir + e0 + k] = d.gw[c * D + k];
+            }
+        }
+        e0 += D;
+    }
+    np[n] = (int32_t)ndir;
+    vfv_pattern* pat = nullptr;
+    int rc = vfv_pattern_from_csr(ctx, n, rp.data(), ci.data(), &pat);
+    if (rc) return rc;
+    t->pat = pat;
+    cudaStream_t s = ctx->stream;
+    CK(t->d_row_ptr.upload(t->row_ptr.data(), nmesh + 1, s));
+    CK(t->np.upload(np.data(), n + 1, s));
+    CK(t->ni.upload(ni.data(), ndir, s));
+    CK(t->dloc.upload(dloc.data(), n, s));
+    CK(t->area.upload(area.data(), ndir, s));
+    CK(t->dist.upload(dist.data(), ndir, s));
+    CK(t->skew.upload(skew.data(), 3 * ndir, s));
+    CK(t->norm.upload(norm.data(), 3 * ndir, s));
+    CK(t->gw.upload(gw.data(), 3 * ndir, s));
+    CK(t->cvol.upload(cvol.data(), n, s));
+    CK(t->flux.alloc(ndir));
+    CK(t->fields.alloc(4 * n));   // D, u, v, w
+    CK(t->grads.alloc(12 * n));   // grad D, grad u, grad v, grad w
+    CK(t->b.alloc(n));
+    CK(t->c0.alloc(n));
+    CK(t->c1.alloc(n));
+    *out = t.release();
+    return VFV_OK;
+}
+
+void vfv_transport_destroy(vfv_transport* t) {
+    if (!t) return;
+    if (t->ctx) cudaStreamSynchronize(t->ctx->stream);
+    delete t;
+}
+
+vfv_pattern* vfv_transport_pattern(vfv_transport* t) { return t ? t->pat : nullptr; }
+
+int vfv_transport_info(const vfv_transport* t, int64_t* n_tot, int64_t* nnz, int32_t* nmesh, int64_t* row_ptr) {
+    if (!t) return set_err(nullptr, VFV_BAD_INPUT, "transport is NULL");
+    if (n_tot) *n_tot = t->n;
+    if (nnz) *nnz = t->pat->nnz;
+    if (nmesh) *nmesh = t->nmesh;
+    if (row_ptr) std::memcpy(row_ptr, t->row_ptr.data(), (t->nmesh + 1) * sizeof(int64_t));
+    return VFV_OK;
+}
+
+int vfv_transport_assemble(vfv_ctx* ctx, vfv_transport* t, const double* D, const double* vel, int on_device) {
+    if (!ctx || !t || !D || !vel) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    const int64_t n = t->n;
+    cudaStream_t s = ctx->stream;
+    const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CK(cudaMemcpyAsync(t->fields.p, D, n * sizeof(double), kd, s));
+    CK(cudaMemcpyAsync(t->fields.p + n, vel, 3 * n * sizeof(double), kd, s));
+    const double* f4[4] = {t->fields.p, t->fields.p + n, t->fields.p + 2 * n, t->fields.p + 3 * n};
+    launch_grad(s, n, t->np.p, t->ni.p, t->gw.p, t->n_dir, 4, f4, t->grads.p);
+    TransportDev T{};
+    T.n = n;
+    T.n_dir = t->n_dir;
+    T.np = t->np.p;
+    T.ni = t->ni.p;
+    T.area = t->area.p;
+    T.dist = t->dist.p;
+    T.skew = t->skew.p;
+    T.norm = t->norm.p;
+    T.cvol = t->cvol.p;
+    T.rp = t->pat->rp.p;
+    T.dloc = t->dloc.p;
+    T.D = t->fields.p;
+    T.gD = t->grads.p;
+    T.vel = t->fields.p + n;
+    T.gvel = t->grads.p + 3 * n;
+    T.flux = t->flux.p;
+    T.dt = t->dt;
+    T.val = t->pat->val.p;
+    launch_face_flux(s, T);
+    launch_assemble_transport(s, T);
+    ctx->launches += 3;
+    CK(cudaGetLastError());
+    t->pat->version++;
+    return VFV_OK;
+}
+
+// nsteps of implicit Euler from c0 (host) with the current matrix: b = -vol c / dt, one batched GMRES
+// per step with the per-mesh stopping rule; the state stays on the device between steps.
+int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, const vfv_gmres_opts* opts, double* c_out,
+                      int32_t* iters) {
+    if (!ctx || !t || !c0 || !c_out || nsteps < 0) return set_err(ctx, VFV_BAD_INPUT, "invalid argument");
+    int rc = check_opts(ctx, opts);
+    if (rc) return rc;
+    const int64_t n = t->n;
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(t->c0.p, c0, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    double* cur = t->c0.p;
+    double* nxt = t->c1.p;
+    for (int k = 0; k < nsteps; ++k) {
+        launch_transport_rhs(s, n, t->cvol.p, t->dt, cur, t->b.p);
+        ctx->launches += 1;
+        vfv_solve_info info{};
+        rc = solve_dev(ctx, t->pat, t->b.p, cur, nxt, opts, &info, t->nmesh, t->d_row_ptr.p);
+        if (rc) return rc;
+        if (iters) iters[k] = info.iters;
+        std::swap(cur, nxt);
+    }
+    CK(cudaMemcpyAsync(c_out, cur, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return VFV_OK;
 }

@@ -146,6 +146,90 @@ __global__ void __launch_bounds__(256) k_assemble_heat(HeatDev H) {
     H.b[v] = bb;
 }
 
+// ---------------------------------------------------------------- transient transport (config 4)
+// Face mass flux with zero pressure and body force (flow_helper.rs:72-179 with vel_rc = 0):
+//   F = rho_f (u_f . n) A,  rho = 1,  u_f = skew-corrected arithmetic mean of the vertex velocities.
+__global__ void __launch_bounds__(256) k_face_flux(TransportDev T) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= T.n) return;
+    const int64_t N = T.n, D = T.n_dir;
+    const double uv = T.vel[v], vv = T.vel[N + v], wv = T.vel[2 * N + v];
+    double g[9];
+    for (int c = 0; c < 9; ++c) g[c] = T.gvel[c * N + v];
+    for (int32_t i = T.np[v]; i < T.np[v + 1]; ++i) {
+        const int32_t nb = T.ni[i];
+        const double sx = T.skew[i], sy = T.skew[D + i], sz = T.skew[2 * D + i];
+        const double nx = T.norm[i], ny = T.norm[D + i], nz = T.norm[2 * D + i];
+        const double den_f = 0.5 * (1.0 + 1.0) + 0.5 * (sx * (0.0 + 0.0) + sy * (0.0 + 0.0) + sz * (0.0 + 0.0));
+        const double u_f = 0.5 * (uv + T.vel[nb]) + 0.5 * (sx * (g[0] + T.gvel[nb]) + sy * (g[1] + T.gvel[N + nb]) + sz * (g[2] + T.gvel[2 * N + nb]));
+        const double v_f = 0.5 * (vv + T.vel[N + nb]) +
+                           0.5 * (sx * (g[3] + T.gvel[3 * N + nb]) + sy * (g[4] + T.gvel[4 * N + nb]) + sz * (g[5] + T.gvel[5 * N + nb]));
+        const double w_f = 0.5 * (wv + T.vel[2 * N + nb]) +
+                           0.5 * (sx * (g[6] + T.gvel[6 * N + nb]) + sy * (g[7] + T.gvel[7 * N + nb]) + sz * (g[8] + T.gvel[8 * N + nb]));
+        T.flux[i] = den_f * (u_f * nx + v_f * ny + w_f * nz + 0.0) * T.area[i];
+    }
+}
+
+// power-law factor A(|Pe|) = max(0, 1 - 0.1 |Pe|)^5, the fifth power as x^2 x^2 x
+__device__ __forceinline__ double power_law(double pe) {
+    const double x = fmax(1.0 - 0.1 * fabs(pe), 0.0);
+    const double x2 = x * x;
+    return x2 * x2 * x;
+}
+
+// Row v, push order: time (v,v), diffusion (v,n)/(v,v) per face, advection (v,n)/(v,v) per face.
+// Off-diagonal slot = c + coeff, diagonal = -vol/dt - sum c - sum coeff, each summed in that order.
+__global__ void __launch_bounds__(256) k_assemble_transport(TransportDev T) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= T.n) return;
+    const int64_t N = T.n, E = T.n_dir;
+    const int32_t b = T.np[v], e = T.np[v + 1];
+    const int32_t rb = T.rp[v], dl = T.dloc[v];
+    const double Dv = T.D[v];
+    const double gx = T.gD[v], gy = T.gD[N + v], gz = T.gD[2 * N + v];
+    double diag = -T.cvol[v] / T.dt;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int32_t i = b; i < e; ++i) {
+            const int32_t nb = T.ni[i];
+            const double Dn = T.D[nb];
+            const double sx = T.skew[i], sy = T.skew[E + i], sz = T.skew[2 * E + i];
+            const double dm = (Dv + Dn != 0.0) ? 2.0 * Dv * Dn / (Dv + Dn) : 0.0;
+            double df = dm + 0.5 * (sx * (gx + T.gD[nb]) + sy * (gy + T.gD[N + nb]) + sz * (gz + T.gD[2 * N + nb]));
+            df = df > 0.0 ? df : dm;
+            const double cond = df * T.area[i] / T.dist[i];
+            const int32_t loc = i - b;
+            const int32_t slot = rb + loc + (loc >= dl ? 1 : 0);
+            if (pass == 0) {
+                T.val[slot] = cond;
+                diag += -cond;
+            } else {
+                const double wgt_f = 0.5 * (1.0 + 1.0) + 0.5 * (sx * (0.0 + 0.0) + sy * (0.0 + 0.0) + sz * (0.0 + 0.0));
+                const double den_f = wgt_f;
+                const double flux = den_f != 0.0 ? wgt_f / den_f * T.flux[i] : 0.0;
+                const double pe = cond != 0.0 ? flux / cond : 0.0;
+                const double coeff = cond * (power_law(pe) - 1.0) + fmax(-flux, 0.0);
+                T.val[slot] += coeff;
+                diag += -coeff;
+            }
+        }
+    }
+    T.val[rb + dl] = diag;
+}
+
+// b = -c_prev vol / dt  (OpSclDomTimeUnity::apply_time right-hand side; zero-flux walls add nothing)
+__global__ void k_transport_rhs(int64_t n, const double* __restrict__ cvol, double dt, const double* __restrict__ c_prev, double* __restrict__ b) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) b[v] = 0.0 + -c_prev[v] * cvol[v] / dt;
+}
+
+void launch_face_flux(cudaStream_t s, const TransportDev& T) { k_face_flux<<<(unsigned)((T.n + 255) / 256), 256, 0, s>>>(T); }
+void launch_assemble_transport(cudaStream_t s, const TransportDev& T) {
+    k_assemble_transport<<<(unsigned)((T.n + 255) / 256), 256, 0, s>>>(T);
+}
+void launch_transport_rhs(cudaStream_t s, int64_t n, const double* cvol, double dt, const double* c_prev, double* b) {
+    k_transport_rhs<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, cvol, dt, c_prev, b);
+}
+
 // build_matrix from triplets: slot s receives the triplet values of its run, summed in push order.
 __global__ void k_values_from_triplets(int64_t nnz, const int64_t* __restrict__ sp, const int64_t* __restrict__ st,
                                        const double* __restrict__ tv, double* __restrict__ val) {

@@ -41,6 +41,33 @@ struct HeatDev {
     double* b;              // [n]
 };
 
+// Device data of the transient advection-diffusion operator (one species, implicit Euler):
+// OpSclDomTimeUnity (opscl_dom_timeunity.rs:32-58), OpSclDomDiffusion (opscl_dom_diff.rs:40-91) and
+// OpSclDomAdvection (opscl_dom_adv.rs:49-125) with their boundary twins on every node (zero-flux walls).
+struct TransportDev {
+    int64_t n, n_dir;
+    const int32_t* np;
+    const int32_t* ni;
+    const double* area;
+    const double* dist;
+    const double* skew;     // [3][n_dir]
+    const double* norm;     // [3][n_dir] unit normal out of the owning control volume
+    const double* cvol;     // [n]
+    const int32_t* rp;      // matrix CSR row pointer
+    const int32_t* dloc;    // [n] diagonal offset in the row
+    const double* D;        // [n] diffusivity
+    const double* gD;       // [3][n] its gradient
+    const double* vel;      // [3][n] velocity
+    const double* gvel;     // [9][n] its gradient (du/dx, du/dy, du/dz, dv/dx, ...)
+    double* flux;           // [n_dir] face mass flux (density 1)
+    double dt;
+    double* val;            // [nnz]
+};
+
+void launch_face_flux(cudaStream_t s, const TransportDev& T);
+void launch_assemble_transport(cudaStream_t s, const TransportDev& T);
+void launch_transport_rhs(cudaStream_t s, int64_t n, const double* cvol, double dt, const double* c_prev, double* b);
+
 void launch_grad(cudaStream_t s, int64_t n, const int32_t* np, const int32_t* ni, const double* gw, int64_t n_dir, int nf,
                  const double* const* f, double* out);
 void launch_assemble_heat(cudaStream_t s, const HeatDev& H);

@@ -40,6 +40,15 @@ class Mesh:
         return cls(h)
 
     @classmethod
+    def jitter_cubes(cls, ns, seeds, jitter: float = 0.25) -> list["Mesh"]:
+        """Many jittered cubes at once, built in parallel on the host."""
+        ns = np.ascontiguousarray(ns, dtype=np.int32)
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+        out = (C.c_void_p * ns.size)()
+        _check(L.load().vfv_mesh_jitter_cubes(int(ns.size), L.ptr(ns, C.c_int32), L.ptr(seeds, C.c_uint64), float(jitter), out))
+        return [cls(C.c_void_p(out[i])) for i in range(ns.size)]
+
+    @classmethod
     def from_vertices(cls, pos: np.ndarray, n_pts: int, node_bnd: np.ndarray) -> "Mesh":
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
         node_bnd = np.ascontiguousarray(node_bnd, dtype=np.int32)

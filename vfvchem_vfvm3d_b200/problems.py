@@ -58,3 +58,37 @@ def steady_heat(n: int, hetero: bool = False, mesh_seed: int = 42, field_seed: i
     T0 = np.zeros(N)
     T0[node_bnd == 1] = 1.0           # initial_dirichlet (steady_base.rs:53-57)
     return HeatProblem(mesh, k, q, s, T0, bc, node_bnd)
+
+
+@dataclass
+class TransportBatch:
+    meshes: list
+    n_grid: np.ndarray       # grid points per axis of every mesh
+    D: float
+    dt: float
+    steps: int
+
+
+def transport_batch(count: int = 256, nmin: int = 2000, nmax: int = 50000, seed: int = 4, D: float = 1e-3, dt: float = 1e-2,
+                    steps: int = 100) -> TransportBatch:
+    """Config 4: `count` jittered cubes with vertex counts N_i drawn log-uniform in [nmin, nmax]
+    (numpy PCG64, `seed`), n_i = round(N_i^(1/3)) grid points per axis, mesh seeds 1000 + i."""
+    rng = np.random.default_rng(seed)
+    N = np.exp(rng.uniform(np.log(nmin), np.log(nmax), count))
+    n = np.maximum(3, np.rint(np.cbrt(N))).astype(np.int32)
+    meshes = Mesh.jitter_cubes(n, 1000 + np.arange(count, dtype=np.uint64))
+    return TransportBatch(meshes, n, D, dt, steps)
+
+
+def transport_fields(meshes, phase_seed: int = 9):
+    """Velocity u = (sin pi y, sin pi z, sin pi x) ([3][n_tot]) and a seeded smooth initial field
+    c0 = 1 + 0.5 sin(pi x + a) sin(pi y + b) sin(pi z + c), phases per mesh from PCG64(phase_seed)."""
+    rng = np.random.default_rng(phase_seed)
+    vel, c0 = [], []
+    for m in meshes:
+        pos, _, _ = m.export()
+        x, y, z = pos[:, 0], pos[:, 1], pos[:, 2]
+        vel.append(np.stack([np.sin(np.pi * y), np.sin(np.pi * z), np.sin(np.pi * x)]))
+        a, b, c = rng.uniform(0, 2 * np.pi, 3)
+        c0.append(1.0 + 0.5 * np.sin(np.pi * x + a) * np.sin(np.pi * y + b) * np.sin(np.pi * z + c))
+    return np.concatenate(vel, axis=1), np.concatenate(c0)
