@@ -198,6 +198,11 @@ int vfv_transport_assemble(vfv_ctx* ctx, vfv_transport* t, const double* D, cons
  * converged when every mesh meets ||b_i - A_i c_i|| <= tol ||b_i||; iters[nsteps] may be NULL */
 int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, const vfv_gmres_opts* opts, double* c_out,
                       int32_t* iters);
+/* Transient adjoint (no reference counterpart): J = 0.5 ||c_nsteps - target||^2 and dJ/dD for the
+ * uniform diffusivity D of the last vfv_transport_assemble. Forward states are checkpointed every
+ * `every` steps and recomputed segment by segment during the backward sweep of transposed solves. */
+int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, int every, const double* target,
+                            const vfv_gmres_opts* opts, double* J, double* dJdD);
 
 #ifdef __cplusplus
 }

@@ -79,3 +79,39 @@ def test_uniform_field_is_preserved(gpu_ctx, batch):
     tr.assemble(1e-3, vel)
     c, _ = tr.run(np.full(tr.n, 2.5), 3, GmresOptions(tol=1e-12, restart=30, max_outer=500, precond=L.PRECOND_ILU0))
     assert np.max(np.abs(c - 2.5)) < 1e-9
+
+
+def _oracle_J(meshes, vel, c0, target, D, nsteps):
+    J, off = 0.0, 0
+    for m, (orp, oci, ova) in zip(meshes, _oracle_blocks(meshes, vel, D)):
+        lu = spla.splu(sp.csr_matrix((ova, oci, orp), shape=(m.n_tot, m.n_tot)).tocsc())
+        c = c0[off:off + m.n_tot].copy()
+        vol = m.dual()["cvol"]
+        for _ in range(nsteps):
+            c = lu.solve(-c * vol / DT)
+        r = c - target[off:off + m.n_tot]
+        J += 0.5 * float(r @ r)
+        off += m.n_tot
+    return J
+
+
+def test_transient_adjoint_dJdD_matches_finite_differences(gpu_ctx, batch):
+    """dJ/dD with checkpoints every 10 steps over 25 steps (a partial last segment) against central
+    differences of the oracle's LU time stepping."""
+    from vfvchem_vfvm3d_b200 import GmresOptions, TransientTransportGpu
+    from vfvchem_vfvm3d_b200 import _lib as L
+    meshes, vel, c0 = batch
+    D = 1e-3
+    target = 0.9 * c0 + 0.05
+    tr = TransientTransportGpu(meshes, DT, ctx=gpu_ctx)
+    tr.assemble(D, vel)
+    opts = GmresOptions(tol=1e-13, restart=30, max_outer=2000, precond=L.PRECOND_ILU0)
+    J, g = tr.adjoint_D(c0, 25, target, every=10, opts=opts)
+    Jo = _oracle_J(meshes, vel, c0, target, D, 25)
+    assert abs(J - Jo) <= 1e-10 * abs(Jo)
+    h = 1e-7
+    fd = (_oracle_J(meshes, vel, c0, target, D + h, 25) - _oracle_J(meshes, vel, c0, target, D - h, 25)) / (2 * h)
+    assert abs(fd - g) <= 1e-6 * abs(fd)
+    # the checkpoint interval changes only the schedule, not the result
+    _, g2 = tr.adjoint_D(c0, 25, target, every=7, opts=opts)
+    assert abs(g2 - g) <= 1e-9 * abs(g)

@@ -798,6 +798,30 @@ int finish_pattern(vfv_ctx* ctx, vfv_pattern* p) {
 
 }  // namespace
 
+// Transpose of a pattern: row j of A^T lists, in ascending order, the rows i of A with an entry in
+// column j; tmap[k_t] = slot of that entry in A (values of A^T are a gather of A's).
+int make_transpose(vfv_ctx* ctx, const vfv_pattern* p, vfv_pattern** out, DBuf<int32_t>& tmap_d) {
+    const int64_t n = p->n, nnz = p->nnz;
+    const std::vector<int32_t>& rp = p->h_rp;
+    const std::vector<int32_t>& ci = p->h_ci;
+    std::vector<int32_t> trp(n + 1, 0), tci(nnz), tmap(nnz);
+    for (int64_t k = 0; k < nnz; ++k) trp[ci[k] + 1]++;
+    for (int64_t j = 0; j < n; ++j) trp[j + 1] += trp[j];
+    std::vector<int32_t> cur(trp.begin(), trp.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const int32_t q = cur[ci[k]]++;
+            tci[q] = (int32_t)i;
+            tmap[q] = k;
+        }
+    vfv_pattern* pt = nullptr;
+    int rc = vfv_pattern_from_csr(ctx, n, trp.data(), tci.data(), &pt);
+    if (rc) return rc;
+    *out = pt;
+    CK(tmap_d.upload(tmap.data(), nnz, ctx->stream));
+    return VFV_OK;
+}
+
 // ================================================================ mesh / heat handles
 struct vfv_mesh {
     Mesh m;
@@ -833,7 +857,37 @@ struct vfv_transport {
     DBuf<int32_t> np, ni, dloc;
     DBuf<double> area, dist, skew, norm, gw, cvol, flux, fields, grads, b, c0, c1;
     vfv_pattern* pat = nullptr;
-    ~vfv_transport() { delete pat; }
+    // transient adjoint: transpose pattern and work space
+    vfv_pattern* pat_t = nullptr;
+    DBuf<int32_t> tmap;
+    DBuf<double> adj;        // checkpoints, one segment of states, two adjoint vectors, rhs, zero, partials, terms
+    DBuf<unsigned> adj_counter;
+    TransportDev dev() const {
+        TransportDev T{};
+        T.n = n;
+        T.n_dir = n_dir;
+        T.np = np.p;
+        T.ni = ni.p;
+        T.area = area.p;
+        T.dist = dist.p;
+        T.skew = skew.p;
+        T.norm = norm.p;
+        T.cvol = cvol.p;
+        T.rp = pat->rp.p;
+        T.dloc = dloc.p;
+        T.D = fields.p;
+        T.gD = grads.p;
+        T.vel = fields.p + n;
+        T.gvel = grads.p + 3 * n;
+        T.flux = flux.p;
+        T.dt = dt;
+        T.val = pat->val.p;
+        return T;
+    }
+    ~vfv_transport() {
+        delete pat_t;
+        delete pat;
+    }
 };
 
 // ================================================================ C ABI
@@ -1353,26 +1407,8 @@ int vfv_heat_adjoint(vfv_ctx* ctx, vfv_heat* h, const double* T, const double* d
     const int64_t n = h->n, E = h->n_dir;
     cudaStream_t s = ctx->stream;
     if (!h->pat_t) {
-        // transpose of the heat pattern: row j of A^T lists, in ascending order, the rows i of A
-        // with an entry in column j; tmap[k_t] = slot of that entry in A
-        const std::vector<int32_t>& rp = h->pat->h_rp;
-        const std::vector<int32_t>& ci = h->pat->h_ci;
-        const int64_t nnz = h->pat->nnz;
-        std::vector<int32_t> trp(n + 1, 0), tci(nnz), tmap(nnz);
-        for (int64_t k = 0; k < nnz; ++k) trp[ci[k] + 1]++;
-        for (int64_t j = 0; j < n; ++j) trp[j + 1] += trp[j];
-        std::vector<int32_t> cur(trp.begin(), trp.end() - 1);
-        for (int64_t i = 0; i < n; ++i)
-            for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
-                const int32_t q = cur[ci[k]]++;
-                tci[q] = (int32_t)i;
-                tmap[q] = k;
-            }
-        vfv_pattern* pt = nullptr;
-        rc = vfv_pattern_from_csr(ctx, n, trp.data(), tci.data(), &pt);
+        rc = make_transpose(ctx, h->pat, &h->pat_t, h->tmap);
         if (rc) return rc;
-        h->pat_t = pt;
-        CK(h->tmap.upload(tmap.data(), nnz, s));
         CK(h->rev.upload(h->h_rev.data(), E, s));
         CK(h->adj_work.alloc((size_t)5 * E + (size_t)10 * n));
     }
@@ -1612,25 +1648,7 @@ int vfv_transport_assemble(vfv_ctx* ctx, vfv_transport* t, const double* D, cons
     CK(cudaMemcpyAsync(t->fields.p + n, vel, 3 * n * sizeof(double), kd, s));
     const double* f4[4] = {t->fields.p, t->fields.p + n, t->fields.p + 2 * n, t->fields.p + 3 * n};
     launch_grad(s, n, t->np.p, t->ni.p, t->gw.p, t->n_dir, 4, f4, t->grads.p);
-    TransportDev T{};
-    T.n = n;
-    T.n_dir = t->n_dir;
-    T.np = t->np.p;
-    T.ni = t->ni.p;
-    T.area = t->area.p;
-    T.dist = t->dist.p;
-    T.skew = t->skew.p;
-    T.norm = t->norm.p;
-    T.cvol = t->cvol.p;
-    T.rp = t->pat->rp.p;
-    T.dloc = t->dloc.p;
-    T.D = t->fields.p;
-    T.gD = t->grads.p;
-    T.vel = t->fields.p + n;
-    T.gvel = t->grads.p + 3 * n;
-    T.flux = t->flux.p;
-    T.dt = t->dt;
-    T.val = t->pat->val.p;
+    const TransportDev T = t->dev();
     launch_face_flux(s, T);
     launch_assemble_transport(s, T);
     ctx->launches += 3;
@@ -1662,6 +1680,102 @@ int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nste
     }
     CK(cudaMemcpyAsync(c_out, cur, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    return VFV_OK;
+}
+
+// dJ/dD for J = 0.5 ||c_N - target||^2 after nsteps implicit-Euler steps from c0, for the uniform
+// diffusivity D of the last vfv_transport_assemble. Discrete adjoint: A^T lam_N = c_N - target,
+// A^T lam_k = M^T lam_{k+1} with M = diag(-vol/dt), dJ/dD = -sum_k lam_{k+1}^T (dA/dD) c_{k+1}.
+// The forward states are kept every `every` steps (checkpoints) and the states of one segment are
+// recomputed from its checkpoint while the backward sweep crosses it.
+int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, int every, const double* target,
+                            const vfv_gmres_opts* opts, double* J, double* dJdD) {
+    if (!ctx || !t || !c0 || !target || nsteps <= 0 || every <= 0) return set_err(ctx, VFV_BAD_INPUT, "invalid argument");
+    int rc = check_opts(ctx, opts);
+    if (rc) return rc;
+    const int64_t n = t->n;
+    cudaStream_t s = ctx->stream;
+    const int nck = (nsteps + every - 1) / every + 1;
+    const int blocks = (int)((n + 255) / 256);
+    if (!t->pat_t) {
+        rc = make_transpose(ctx, t->pat, &t->pat_t, t->tmap);
+        if (rc) return rc;
+    }
+    const size_t need = (size_t)n * (nck + every + 5) + (size_t)blocks + (size_t)nsteps + 8;
+    if (t->adj.n < need) CK(t->adj.alloc(need));
+    if (!t->adj_counter.p) {
+        CK(t->adj_counter.alloc(1));
+        CK(cudaMemset(t->adj_counter.p, 0, sizeof(unsigned)));
+    }
+    double* ck = t->adj.p;                       // [nck][n] checkpoints c_0, c_every, ...
+    double* seg = ck + (size_t)nck * n;          // [every][n] states of one segment
+    double* lam = seg + (size_t)every * n;       // adjoint vectors
+    double* lam2 = lam + n;
+    double* rhs = lam2 + n;
+    double* zero = rhs + n;
+    double* tmp = zero + n;
+    double* part = tmp + n;
+    double* terms = part + blocks;               // [nsteps]
+    k_gather_vals<double><<<grid_for(t->pat->nnz), 256, 0, s>>>(t->pat->nnz, t->tmap.p, t->pat->val.p, t->pat_t->val.p);
+    t->pat_t->version++;
+    CK(cudaMemsetAsync(zero, 0, n * sizeof(double), s));
+    CK(cudaMemcpyAsync(ck, c0, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    const TransportDev T = t->dev();
+    auto step = [&](const double* cin, double* cout) -> int {
+        launch_transport_rhs(s, n, t->cvol.p, t->dt, cin, t->b.p);
+        vfv_solve_info info{};
+        return solve_dev(ctx, t->pat, t->b.p, cin, cout, opts, &info, t->nmesh, t->d_row_ptr.p);
+    };
+    // forward sweep, keeping checkpoints
+    CK(cudaMemcpyAsync(t->c0.p, ck, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    double* cur = t->c0.p;
+    double* nxt = t->c1.p;
+    for (int k = 0; k < nsteps; ++k) {
+        if ((rc = step(cur, nxt))) return rc;
+        std::swap(cur, nxt);
+        if ((k + 1) % every == 0 && (k + 1) / every < nck) CK(cudaMemcpyAsync(ck + (size_t)((k + 1) / every) * n, cur, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    // J and lam_N
+    std::vector<double> hc(n), ht(target, target + n);
+    CK(cudaMemcpyAsync(hc.data(), cur, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double jsum = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double r = hc[i] - ht[i];
+        jsum += r * r;
+        hc[i] = r;
+    }
+    if (J) *J = 0.5 * jsum;
+    CK(cudaMemcpyAsync(rhs, hc.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    vfv_solve_info info{};
+    if ((rc = solve_dev(ctx, t->pat_t, rhs, zero, lam, opts, &info, t->nmesh, t->d_row_ptr.p))) return rc;
+    // backward sweep over the segments, last first
+    for (int k = nsteps - 1; k >= 0; --k) {
+        const int j = k / every;  // segment of state c_{k+1}: c_{j every + 1 .. j every + every}
+        if (k == nsteps - 1 || (k + 1) % every == 0) {
+            const int last = std::min(nsteps, j * every + every);
+            const double* from = ck + (size_t)j * n;
+            for (int q = j * every; q < last; ++q) {
+                double* to = seg + (size_t)(q - j * every) * n;
+                if ((rc = step(q == j * every ? from : seg + (size_t)(q - 1 - j * every) * n, to))) return rc;
+            }
+        }
+        const double* c_k1 = seg + (size_t)(k - j * every) * n;
+        launch_transport_dAdD_dot(s, T, lam, c_k1, part, t->adj_counter.p, terms + k);
+        if (k > 0) {
+            launch_transport_rhs(s, n, t->cvol.p, t->dt, lam, rhs);  // M^T lam = -vol lam / dt
+            if ((rc = solve_dev(ctx, t->pat_t, rhs, lam, lam2, opts, &info, t->nmesh, t->d_row_ptr.p))) return rc;
+            std::swap(lam, lam2);
+        }
+    }
+    std::vector<double> ht2(nsteps);
+    CK(cudaMemcpyAsync(ht2.data(), terms, nsteps * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaGetLastError());
+    double g = 0.0;
+    for (int k = 0; k < nsteps; ++k) g -= ht2[k];
+    if (dJdD) *dJdD = g;
+    (void)tmp;
     return VFV_OK;
 }
 

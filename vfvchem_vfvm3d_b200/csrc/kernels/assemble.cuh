@@ -68,6 +68,11 @@ void launch_face_flux(cudaStream_t s, const TransportDev& T);
 void launch_assemble_transport(cudaStream_t s, const TransportDev& T);
 void launch_transport_rhs(cudaStream_t s, int64_t n, const double* cvol, double dt, const double* c_prev, double* b);
 
+// part[blk] = sum over this block's rows v of lam_v sum_faces s_e (c_n - c_v), where
+// s_e = d(cond + coeff)/dD for a uniform diffusivity D (transient adjoint, config 4)
+void launch_transport_dAdD_dot(cudaStream_t s, const TransportDev& T, const double* lam, const double* c, double* part, unsigned* counter,
+                               double* out);
+
 void launch_grad(cudaStream_t s, int64_t n, const int32_t* np, const int32_t* ni, const double* gw, int64_t n_dir, int nf,
                  const double* const* f, double* out);
 void launch_assemble_heat(cudaStream_t s, const HeatDev& H);
