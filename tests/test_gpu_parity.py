@@ -109,6 +109,44 @@ def test_spmv_matches_oracle(gpu_ctx, c1h_system, c1_hetero):
     assert np.max(np.abs(yf.cpu().numpy() - yo)) <= 1e-5 * np.max(np.abs(yo))
 
 
+@pytest.mark.parametrize("lanes", [2, 4, 8])
+def test_spmv_lanes_variants_match_oracle(gpu_ctx, c1h_system, c1_hetero, lanes):
+    """Every lanes-per-row variant the autotuner may pick gives the oracle's product, and a solve
+    through it still converges to the LU solution."""
+    import torch
+    from vfvchem_vfvm3d_b200 import GmresOptions, Pattern, VFVChemError
+    from vfvchem_vfvm3d_b200 import _lib as L
+    (rp, ci, va), b, _ = c1h_system
+    xlu = lu_solve(rp, ci, va, b)
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    p.set_spmv_lanes(lanes, lanes)
+    x = np.random.default_rng(6).standard_normal(c1_hetero.n)
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.empty_like(xd)
+    torch.cuda.synchronize()
+    p.spmv_device(xd.data_ptr(), yd.data_ptr())
+    gpu_ctx.synchronize()
+    yo = oracle.spmv(rp, ci, va, x)
+    assert np.max(np.abs(yd.cpu().numpy() - yo)) <= 1e-13 * np.max(np.abs(yo))
+    xs, info = p.solve(b, opts=GmresOptions(tol=1e-12, restart=40, max_outer=100, precond=L.PRECOND_ILU0, precision=L.MIXED))
+    assert info.status == 0
+    assert np.max(np.abs(xs - xlu)) <= 1e-8 * np.max(np.abs(xlu))
+    with pytest.raises(VFVChemError):
+        p.set_spmv_lanes(3, 4)
+
+
+def test_autotune_picks_a_variant(gpu_ctx, c1h_system):
+    from vfvchem_vfvm3d_b200 import Pattern
+    (rp, ci, va), b, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    a, f = p.autotune()
+    assert a in (2, 4, 8) and f in (2, 4, 8)
+    x, info = p.solve(b)
+    assert info.status == 0
+
+
 def _check_ordering(rp, ci, perm, lev_ptr):
     """The permutation groups rows into levels no two coupled rows share, and every coupling
     points from a later level to an earlier one in the lower factor (true of any ordering)."""

@@ -193,6 +193,15 @@ class Pattern:
                                                                C.c_void_p(z_ptr), C.byref(lev)))
         return lev.value
 
+    def autotune(self):
+        """Pick the SpMV lanes per row (double, float) by measurement; call before the first solve."""
+        a, b = C.c_int32(), C.c_int32()
+        _check(self.ctx.handle, L.load().vfv_pattern_autotune(self.ctx.handle, self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_spmv_lanes(self, lanes64: int, lanes32: int) -> None:
+        _check(self.ctx.handle, L.load().vfv_pattern_set_spmv_lanes(self.ctx.handle, self._h, int(lanes64), int(lanes32)))
+
     def ilu0_ordering(self, order: int = L.ILU_MULTICOLOR):
         """(perm new->old, lev_ptr) of the ILU(0) factor's symmetric permutation (host only)."""
         nlev = C.c_int32()

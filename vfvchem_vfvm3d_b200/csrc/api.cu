@@ -129,6 +129,7 @@ struct SolverBase {
 struct vfv_pattern {
     vfv_ctx* ctx = nullptr;
     int64_t n = 0, nnz = 0, ntrip = 0;
+    int spmv_lanes[2] = {kSpG, kSpG};  // lanes per row of the SpMV for double / float values (autotuned)
     std::vector<int32_t> h_rp, h_ci;
     DBuf<int32_t> rp, ci, diag_pos;
     DBuf<double> val;
@@ -143,6 +144,22 @@ struct vfv_pattern {
 
 // ================================================================ GMRES driver
 namespace {
+
+// SpMV with the lanes-per-row the pattern was tuned for (2, 4 or 8)
+template <typename TV, typename TX, typename TY, typename TA>
+void launch_spmv(cudaStream_t s, int lanes, int64_t n, const int32_t* rp, const int32_t* ci, const TV* val, const TX* x, TY* y,
+                 const double* scale, const DevStatus* st) {
+    switch (lanes) {
+        case 2:
+            k_spmv<TV, TX, TY, TA, 2><<<grid_for(n * 2), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
+            break;
+        case 8:
+            k_spmv<TV, TX, TY, TA, 8><<<grid_for(n * 8), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
+            break;
+        default:
+            k_spmv<TV, TX, TY, TA, 4><<<grid_for(n * 4), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
+    }
+}
 
 // Greedy colouring of the symmetrised pattern graph: colour(v) = smallest colour unused by the
 // already coloured neighbours, visiting vertices in `order`.
@@ -584,7 +601,7 @@ struct Gmres : SolverBase {
                 ilu_apply<T>(s, *ilu, lu_vals(), uj, z2.p, z.p, st.p);
                 in = z.p;
             }
-            k_spmv<T, T, T, T, G><<<sp_blocks, kBlk, 0, s>>>(n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
+            launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
             k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
             k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
             k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
@@ -1091,8 +1108,7 @@ int vfv_solve(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
 
 int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double* y) {
     if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    constexpr int G = kSpG;
-    k_spmv<double, double, double, double, G><<<grid_for(p->n * G), kBlk, 0, ctx->stream>>>(p->n, p->rp.p, p->ci.p, p->val.p, x, y, nullptr, nullptr);
+    launch_spmv<double, double, double, double>(ctx->stream, p->spmv_lanes[0], p->n, p->rp.p, p->ci.p, p->val.p, x, y, nullptr, nullptr);
     ctx->launches += 1;
     CK(cudaGetLastError());
     return VFV_OK;
@@ -1100,13 +1116,12 @@ int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double*
 
 int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y) {
     if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    constexpr int G = kSpG;
     if (p->version32 != p->version) {
         if (!p->val32.p) CK(p->val32.alloc(p->nnz));
         k_cast<double, float><<<grid_for(p->nnz), 256, 0, ctx->stream>>>(p->nnz, p->val.p, p->val32.p);
         p->version32 = p->version;
     }
-    k_spmv<float, float, float, float, G><<<grid_for(p->n * G), kBlk, 0, ctx->stream>>>(p->n, p->rp.p, p->ci.p, p->val32.p, x, y, nullptr, nullptr);
+    launch_spmv<float, float, float, float>(ctx->stream, p->spmv_lanes[1], p->n, p->rp.p, p->ci.p, p->val32.p, x, y, nullptr, nullptr);
     ctx->launches += 1;
     CK(cudaGetLastError());
     return VFV_OK;
@@ -1186,6 +1201,67 @@ int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, c
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
     if (levels) *levels = S.nlev;
+    return VFV_OK;
+}
+
+// Autotuner: times the SpMV of this pattern (its current values) with 2, 4 and 8 lanes per row in
+// double and in float, keeps the fastest of each for every later SpMV and solver of the pattern.
+// Must run before the pattern's first solve (solvers capture their kernels once).
+int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t* lanes32) {
+    if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    cudaStream_t s = ctx->stream;
+    const int64_t n = p->n;
+    DBuf<double> x, y;
+    DBuf<float> v32, x32, y32;
+    CK(x.alloc(n));
+    CK(y.alloc(n));
+    CK(x32.alloc(n));
+    CK(y32.alloc(n));
+    CK(v32.alloc(p->nnz));
+    CK(cudaMemsetAsync(x.p, 0, n * sizeof(double), s));
+    CK(cudaMemsetAsync(x32.p, 0, n * sizeof(float), s));
+    k_cast<double, float><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, p->val.p, v32.p);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const int cand[3] = {2, 4, 8};
+    for (int prec = 0; prec < 2; ++prec) {
+        float best = 1e30f;
+        int best_g = kSpG;
+        for (int g : cand) {
+            auto run = [&] {
+                if (prec == 0) launch_spmv<double, double, double, double>(s, g, n, p->rp.p, p->ci.p, p->val.p, x.p, y.p, nullptr, nullptr);
+                else launch_spmv<float, float, float, float>(s, g, n, p->rp.p, p->ci.p, v32.p, x32.p, y32.p, nullptr, nullptr);
+            };
+            for (int w = 0; w < 3; ++w) run();
+            CK(cudaEventRecord(e0, s));
+            for (int r = 0; r < 10; ++r) run();
+            CK(cudaEventRecord(e1, s));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                best_g = g;
+            }
+        }
+        p->spmv_lanes[prec] = best_g;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->launches += 2 * 3 * 13 + 1;
+    CK(cudaGetLastError());
+    if (lanes64) *lanes64 = p->spmv_lanes[0];
+    if (lanes32) *lanes32 = p->spmv_lanes[1];
+    return VFV_OK;
+}
+
+int vfv_pattern_set_spmv_lanes(vfv_ctx* ctx, vfv_pattern* p, int32_t lanes64, int32_t lanes32) {
+    if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    auto ok = [](int32_t g) { return g == 2 || g == 4 || g == 8; };
+    if (!ok(lanes64) || !ok(lanes32)) return set_err(ctx, VFV_BAD_INPUT, "SpMV lanes per row must be 2, 4 or 8");
+    p->spmv_lanes[0] = lanes64;
+    p->spmv_lanes[1] = lanes32;
     return VFV_OK;
 }
 
