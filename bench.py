@@ -88,10 +88,10 @@ def extras_transport(ctx, count):
     target = np.full(tr.n, float(np.mean(c0)))
     aopts = GmresOptions(tol=1e-10, restart=30, max_outer=500, precond=L.PRECOND_ILU0, precision=L.MIXED, inner_rtol=1e-6)
     t0 = time.perf_counter()
-    J, dJdD = tr.adjoint_D(c0, tb.steps, target, every=10, opts=aopts)
+    J, dJdD, aits = tr.adjoint_D(c0, tb.steps, target, every=10, opts=aopts, return_iters=True)
     t_adj = time.perf_counter() - t0
     return {"meshes": count, "rows": tr.n, "nnz": tr.nnz, "steps": tb.steps, "run_s": t_run, "step_ms": t_run / tb.steps * 1e3,
-            "iters_per_step": float(np.mean(its)), "adjoint_dJdD_s": t_adj, "J": J, "dJdD": dJdD, "spmv_lanes_f64_f32": list(lanes),
+            "iters_per_step": float(np.mean(its)), "adjoint_dJdD_s": t_adj, "adjoint_iters_per_solve": float(np.mean(aits)), "J": J, "dJdD": dJdD, "spmv_lanes_f64_f32": list(lanes),
             "mesh_setup_s": t_mesh,
             "workload": f"{count} jittered cubes, N_i log-uniform in [2000, 50000], D=1e-3, u=(sin pi y, sin pi z, sin pi x), dt=1e-2; "
                         "GMRES(30)+ILU(0) mixed to 1e-10 relres per mesh and step; host arrays in/out"}

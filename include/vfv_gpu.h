@@ -206,9 +206,11 @@ int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nste
                       int32_t* iters);
 /* Transient adjoint (no reference counterpart): J = 0.5 ||c_nsteps - target||^2 and dJ/dD for the
  * uniform diffusivity D of the last vfv_transport_assemble. Forward states are checkpointed every
- * `every` steps and recomputed segment by segment during the backward sweep of transposed solves. */
+ * `every` steps and recomputed segment by segment during the backward sweep of transposed solves.
+ * adj_iters (may be NULL): nsteps entries, [k] = GMRES iterations of the transposed solve giving
+ * lambda_{k+1}. */
 int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, int every, const double* target,
-                            const vfv_gmres_opts* opts, double* J, double* dJdD);
+                            const vfv_gmres_opts* opts, double* J, double* dJdD, int32_t* adj_iters);
 
 #ifdef __cplusplus
 }

@@ -96,7 +96,7 @@ SIGNATURES = [
     ("vfv_transport_info", C.c_int, [_P, _I64P, _I64P, _I32P, _I64P]),
     ("vfv_transport_assemble", C.c_int, [_P, _P, _P, _P, C.c_int]),
     ("vfv_transport_run", C.c_int, [_P, _P, _DP, C.c_int, C.POINTER(GmresOpts), _DP, _I32P]),
-    ("vfv_transport_adjoint_D", C.c_int, [_P, _P, _DP, C.c_int, C.c_int, _DP, C.POINTER(GmresOpts), _DP, _DP]),
+    ("vfv_transport_adjoint_D", C.c_int, [_P, _P, _DP, C.c_int, C.c_int, _DP, C.POINTER(GmresOpts), _DP, _DP, _I32P]),
     ("vfv_heat_adjoint", C.c_int, [_P, _P, _DP, _DP, C.POINTER(GmresOpts), _DP, _DP, _DP, C.POINTER(SolveInfo)]),
 ]
 

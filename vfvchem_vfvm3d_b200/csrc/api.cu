@@ -137,6 +137,8 @@ struct vfv_pattern {
     uint64_t version = 0, version32 = ~0ull;
     DBuf<int64_t> slot_ptr, slot_trip;
     DBuf<double> trip_vals;
+    std::vector<int64_t> blocks;          // row ranges of the diagonal blocks of a block-diagonal system (may be empty)
+    const vfv_pattern* same_as = nullptr;  // a pattern with identical rows/columns (ILU orderings are shared)
     std::map<int, std::unique_ptr<IluStruct>> ilu;
     std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<SolverBase>> solvers;
     DBuf<double> tmp_b, tmp_x;  // staging for host-pointer solves
@@ -161,19 +163,62 @@ void launch_spmv(cudaStream_t s, int lanes, int64_t n, const int32_t* rp, const 
     }
 }
 
-// Greedy colouring of the symmetrised pattern graph: colour(v) = smallest colour unused by the
-// already coloured neighbours, visiting vertices in `order`.
-int greedy_colour(int64_t n, const std::vector<std::vector<int32_t>>& adj, const std::vector<int32_t>& order, std::vector<int32_t>& col) {
-    std::fill(col.begin(), col.end(), -1);
-    std::vector<int64_t> mark(64, -1);
-    int nc = 0;
-    for (int64_t t = 0; t < n; ++t) {
-        const int32_t v = order[t];
-        for (int32_t u : adj[v])
-            if (col[u] >= 0) {
-                if (col[u] >= (int32_t)mark.size()) mark.resize(col[u] + 1, -1);
-                mark[col[u]] = t;
+// Symmetrised, de-duplicated adjacency of the pattern graph (no self loops) as CSR.
+void sym_adjacency(const vfv_pattern* p, std::vector<int64_t>& xadj, std::vector<int32_t>& adj) {
+    const int64_t n = p->n;
+    const std::vector<int32_t>& rp = p->h_rp;
+    const std::vector<int32_t>& ci = p->h_ci;
+    xadj.assign(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] != i) {
+                xadj[i + 1]++;
+                xadj[ci[k] + 1]++;
             }
+    for (int64_t i = 0; i < n; ++i) xadj[i + 1] += xadj[i];
+    adj.resize(xadj[n]);
+    std::vector<int64_t> cur(xadj.begin(), xadj.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] != i) {
+                adj[cur[i]++] = ci[k];
+                adj[cur[ci[k]]++] = (int32_t)i;
+            }
+    // sort and drop duplicates row by row, compacting in place
+    std::vector<int64_t> len(n);
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t* a = adj.data() + xadj[i];
+        const int64_t m = xadj[i + 1] - xadj[i];
+        std::sort(a, a + m);
+        len[i] = std::unique(a, a + m) - a;
+    }
+    int64_t w = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t r0 = xadj[i];
+        for (int64_t k = 0; k < len[i]; ++k) adj[w + k] = adj[r0 + k];
+        xadj[i] = w;
+        w += len[i];
+    }
+    xadj[n] = w;
+    adj.resize(w);
+}
+
+// Greedy colouring: colour(v) = smallest colour unused by the already coloured neighbours,
+// visiting the vertices in `order` (which must list every vertex whose colour is reset to -1).
+int greedy_colour(const std::vector<int32_t>& order, const int64_t* xadj, const int32_t* adj, int32_t* col, std::vector<int64_t>& mark) {
+    for (int32_t v : order) col[v] = -1;
+    std::fill(mark.begin(), mark.end(), -1);
+    int nc = 0;
+    for (int64_t t = 0; t < (int64_t)order.size(); ++t) {
+        const int32_t v = order[t];
+        for (int64_t k = xadj[v]; k < xadj[v + 1]; ++k) {
+            const int32_t c = col[adj[k]];
+            if (c >= 0) {
+                if (c >= (int32_t)mark.size()) mark.resize(c + 1, -1);
+                mark[c] = t;
+            }
+        }
         int32_t c = 0;
         while (c < (int32_t)mark.size() && mark[c] == t) ++c;
         col[v] = c;
@@ -182,57 +227,73 @@ int greedy_colour(int64_t n, const std::vector<std::vector<int32_t>>& adj, const
     return nc;
 }
 
-// Multicolour ordering with few colours (each colour is a level of both ILU sweeps): greedy in
-// index order, then iterated greedy (Culberson: re-running greedy with the vertices grouped by
-// colour class never needs more colours), then single-neighbour recolouring that tries to empty
-// the last class. Deterministic.
-int multicolor(int64_t n, const std::vector<std::vector<int32_t>>& lower, std::vector<int32_t>& col) {
-    std::vector<std::vector<int32_t>> adj(n);
-    for (int64_t i = 0; i < n; ++i)
-        for (int32_t j : lower[i]) {
-            adj[i].push_back(j);
-            adj[j].push_back((int32_t)i);
-        }
-    std::vector<int32_t> order(n);
-    for (int64_t i = 0; i < n; ++i) order[i] = (int32_t)i;
-    int nc = greedy_colour(n, adj, order, col);
-    std::vector<int32_t> c2(n);
+// Stable counting sort of `order` by key[col[v]] (keys in [0, nkey)).
+void sort_by_class(std::vector<int32_t>& order, const int32_t* col, const std::vector<int32_t>& key, int nkey, std::vector<int32_t>& tmp) {
+    std::vector<int64_t> start(nkey + 1, 0);
+    for (int32_t v : order) start[key[col[v]] + 1]++;
+    for (int k = 0; k < nkey; ++k) start[k + 1] += start[k];
+    tmp.resize(order.size());
+    for (int32_t v : order) tmp[start[key[col[v]]]++] = v;
+    order.swap(tmp);
+}
+
+// Multicolour ordering with few colours (each colour is a level of both ILU sweeps) of the
+// vertices [r0, r1), which must have no edge leaving the range: greedy in index order, then
+// iterated greedy (Culberson: re-running greedy with the vertices grouped by colour class never
+// needs more colours), then single-neighbour recolouring that tries to empty the last class.
+// Deterministic.
+int multicolor_range(int64_t r0, int64_t r1, const int64_t* xadj, const int32_t* adj, int32_t* col) {
+    const int64_t n = r1 - r0;
+    if (n <= 0) return 0;
+    std::vector<int32_t> order(n), tmp;
+    for (int64_t i = 0; i < n; ++i) order[i] = (int32_t)(r0 + i);
+    std::vector<int64_t> mark(64, -1);
+    int nc = greedy_colour(order, xadj, adj, col, mark);
+    std::vector<int32_t> best(col + r0, col + r1);
     for (int it = 0; it < 8; ++it) {
-        std::vector<int64_t> cnt(nc, 0);
-        for (int32_t c : col) cnt[c]++;
-        if (it % 2 == 0)
-            std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return col[a] > col[b]; });
-        else
-            std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
-                return cnt[col[a]] != cnt[col[b]] ? cnt[col[a]] > cnt[col[b]] : col[a] < col[b];
-            });
-        const int nc2 = greedy_colour(n, adj, order, c2);
+        std::vector<int32_t> key(nc);
+        if (it % 2 == 0) {
+            for (int c = 0; c < nc; ++c) key[c] = nc - 1 - c;  // largest colour first
+        } else {
+            std::vector<int64_t> cnt(nc, 0);
+            for (int64_t i = r0; i < r1; ++i) cnt[col[i]]++;
+            std::vector<int32_t> cls(nc);
+            for (int c = 0; c < nc; ++c) cls[c] = c;
+            std::stable_sort(cls.begin(), cls.end(), [&](int32_t a, int32_t b) { return cnt[a] != cnt[b] ? cnt[a] > cnt[b] : a < b; });
+            for (int r = 0; r < nc; ++r) key[cls[r]] = r;  // most populated class first
+        }
+        sort_by_class(order, col, key, nc, tmp);
+        const int nc2 = greedy_colour(order, xadj, adj, col, mark);
         if (nc2 <= nc) {
             nc = nc2;
-            col.swap(c2);
+            std::copy(col + r0, col + r1, best.begin());
+        } else {
+            std::copy(best.begin(), best.end(), col + r0);
         }
     }
+    std::vector<char> used;
     for (int round = 0; round < 2 && nc > 1; ++round) {
         const int last = nc - 1;
         int64_t left = 0;
-        for (int64_t v = 0; v < n; ++v) {
+        used.assign(last, 0);
+        for (int64_t v = r0; v < r1; ++v) {
             if (col[v] != last) continue;
             bool done = false;
             for (int c = 0; c < last && !done; ++c) {
                 int cntc = 0;
                 int32_t u = -1;
-                for (int32_t w : adj[v])
-                    if (col[w] == c) {
+                for (int64_t k = xadj[v]; k < xadj[v + 1]; ++k)
+                    if (col[adj[k]] == c) {
                         ++cntc;
-                        u = w;
+                        u = adj[k];
                     }
                 if (cntc == 0) {
                     col[v] = c;
                     done = true;
                 } else if (cntc == 1) {
-                    std::vector<char> used(last, 0);
-                    for (int32_t w : adj[u])
-                        if (w != v && col[w] < last) used[col[w]] = 1;
+                    std::fill(used.begin(), used.end(), 0);
+                    for (int64_t k = xadj[u]; k < xadj[u + 1]; ++k)
+                        if (adj[k] != v && col[adj[k]] < last) used[col[adj[k]]] = 1;
                     for (int cc = 0; cc < last; ++cc)
                         if (cc != c && !used[cc]) {
                             col[u] = cc;
@@ -252,31 +313,48 @@ int multicolor(int64_t n, const std::vector<std::vector<int32_t>>& lower, std::v
     return nc;
 }
 
+// Multicolour ordering of the whole pattern; the diagonal blocks p->blocks (row ranges of a
+// block-diagonal system) are coloured independently in parallel when no edge couples two blocks.
+int multicolor(const vfv_pattern* p, const std::vector<int64_t>& xadj, const std::vector<int32_t>& adj, std::vector<int32_t>& col) {
+    const int64_t n = p->n;
+    std::vector<int64_t> blk = p->blocks;
+    bool ok = blk.size() >= 2 && blk.front() == 0 && blk.back() == n;
+    for (size_t b = 0; ok && b + 1 < blk.size(); ++b)
+        for (int64_t v = blk[b]; ok && v < blk[b + 1]; ++v)
+            for (int64_t k = xadj[v]; k < xadj[v + 1]; ++k)
+                if (adj[k] < blk[b] || adj[k] >= blk[b + 1]) {
+                    ok = false;
+                    break;
+                }
+    if (!ok) blk = {0, n};
+    const int64_t nb = (int64_t)blk.size() - 1;
+    int nc = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(max : nc)
+    for (int64_t b = 0; b < nb; ++b) nc = std::max(nc, multicolor_range(blk[b], blk[b + 1], xadj.data(), adj.data(), col.data()));
+    return nc;
+}
+
 int build_ilu_struct(vfv_ctx* ctx, vfv_pattern* p, int order, IluStruct& S) {
     const int64_t n = p->n;
     const std::vector<int32_t>& rp = p->h_rp;
     const std::vector<int32_t>& ci = p->h_ci;
-    // symmetrised adjacency (lower neighbours only are needed for levels / greedy colours)
-    std::vector<std::vector<int32_t>> lower(n);
-    for (int64_t i = 0; i < n; ++i)
-        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
-            const int32_t j = ci[k];
-            if (j < i) lower[i].push_back(j);
-            else if (j > i) lower[j].push_back((int32_t)i);
-        }
+    std::vector<int64_t> xadj;
+    std::vector<int32_t> adj;
+    sym_adjacency(p, xadj, adj);
     std::vector<int32_t> lev(n, 0);
     int nlev = 0;
-    if (order == VFV_ILU_NATURAL) {
+    if (order == VFV_ILU_NATURAL) {  // level = 1 + the deepest lower neighbour
         for (int64_t i = 0; i < n; ++i) {
             int32_t l = 0;
-            for (int32_t k : lower[i]) l = std::max(l, lev[k] + 1);
+            for (int64_t k = xadj[i]; k < xadj[i + 1] && adj[k] < i; ++k) l = std::max(l, lev[adj[k]] + 1);
             lev[i] = l;
             nlev = std::max(nlev, l + 1);
         }
     } else {
-        nlev = multicolor(n, lower, lev);
+        nlev = multicolor(p, xadj, adj, lev);
     }
-    std::vector<std::vector<int32_t>>().swap(lower);
+    std::vector<int64_t>().swap(xadj);
+    std::vector<int32_t>().swap(adj);
     std::vector<int32_t> perm(n), iperm(n);
     std::vector<int64_t> cnt(nlev + 1, 0);
     for (int64_t i = 0; i < n; ++i) cnt[lev[i] + 1]++;
@@ -319,6 +397,33 @@ int build_ilu_struct(vfv_ctx* ctx, vfv_pattern* p, int order, IluStruct& S) {
 
     S.order = order;
     S.nlev = nlev;
+    return VFV_OK;
+}
+
+// Copy of the ordering and permuted pattern of an ILU structure built for a pattern with the same
+// rows and columns (the numeric factor is recomputed from this pattern's values).
+template <typename T>
+cudaError_t copy_dbuf(DBuf<T>& to, const DBuf<T>& from, cudaStream_t s) {
+    cudaError_t e = to.alloc(from.n);
+    if (e != cudaSuccess || from.n == 0) return e;
+    return cudaMemcpyAsync(to.p, from.p, from.n * sizeof(T), cudaMemcpyDeviceToDevice, s);
+}
+
+int clone_ilu_struct(vfv_ctx* ctx, const IluStruct& F, int64_t nnz, IluStruct& S) {
+    cudaStream_t s = ctx->stream;
+    S.order = F.order;
+    S.nlev = F.nlev;
+    S.lev_ptr = F.lev_ptr;
+    S.h_perm = F.h_perm;
+    CK(copy_dbuf(S.d_lev_ptr, F.d_lev_ptr, s));
+    CK(copy_dbuf(S.perm, F.perm, s));
+    CK(copy_dbuf(S.rp, F.rp, s));
+    CK(copy_dbuf(S.ci, F.ci, s));
+    CK(copy_dbuf(S.dg, F.dg, s));
+    CK(copy_dbuf(S.src, F.src, s));
+    CK(S.lu64.alloc(nnz));
+    CK(S.bad.alloc(1));
+    CK(cudaStreamSynchronize(s));
     return VFV_OK;
 }
 
@@ -466,7 +571,12 @@ struct Gmres : SolverBase {
             auto it = p->ilu.find(ilu_order);
             if (it == p->ilu.end()) {
                 auto S = std::make_unique<IluStruct>();
-                int rc = build_ilu_struct(ctx, p, ilu_order, *S);
+                const IluStruct* twin = nullptr;
+                if (p->same_as) {
+                    auto jt = p->same_as->ilu.find(ilu_order);
+                    if (jt != p->same_as->ilu.end()) twin = jt->second.get();
+                }
+                int rc = twin ? clone_ilu_struct(ctx, *twin, p->nnz, *S) : build_ilu_struct(ctx, p, ilu_order, *S);
                 if (rc) return rc;
                 it = p->ilu.emplace(ilu_order, std::move(S)).first;
             }
@@ -747,6 +857,11 @@ struct Gmres : SolverBase {
 
         CK(cudaMemcpyAsync(d_x, x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaStreamSynchronize(s));
+        if (const char* e = getenv("VFV_TRACE_SOLVE")) {  // diagnostics: one line per solve
+            if (e[0] == '1')
+                fprintf(stderr, "[vfv solve] n=%lld %s cycles=%d iters=%d relres=%.3e bnorm=%.3e tol_abs=%.3e nblk=%d\n", (long long)n,
+                        mixed ? "mixed" : "fp64", cycles, hst.total_steps, hst.beta0 / bnorm, bnorm, tol_abs, nblk);
+        }
         if (info) {
             info->status = rc;
             info->iters = hst.total_steps;
@@ -834,6 +949,8 @@ int make_transpose(vfv_ctx* ctx, const vfv_pattern* p, vfv_pattern** out, DBuf<i
     vfv_pattern* pt = nullptr;
     int rc = vfv_pattern_from_csr(ctx, n, trp.data(), tci.data(), &pt);
     if (rc) return rc;
+    pt->blocks = p->blocks;
+    if (trp == rp && tci == ci) pt->same_as = p;  // structurally symmetric: share the ILU orderings
     *out = pt;
     CK(tmap_d.upload(tmap.data(), nnz, ctx->stream));
     return VFV_OK;
@@ -1677,6 +1794,7 @@ int vfv_transport_create(vfv_ctx* ctx, int nmesh, vfv_mesh* const* meshes, doubl
     int rc = vfv_pattern_from_csr(ctx, n, rp.data(), ci.data(), &pat);
     if (rc) return rc;
     t->pat = pat;
+    pat->blocks.assign(t->row_ptr.begin(), t->row_ptr.end());
     cudaStream_t s = ctx->stream;
     CK(t->d_row_ptr.upload(t->row_ptr.data(), nmesh + 1, s));
     CK(t->np.upload(np.data(), n + 1, s));
@@ -1765,7 +1883,7 @@ int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nste
 // The forward states are kept every `every` steps (checkpoints) and the states of one segment are
 // recomputed from its checkpoint while the backward sweep crosses it.
 int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, int every, const double* target,
-                            const vfv_gmres_opts* opts, double* J, double* dJdD) {
+                            const vfv_gmres_opts* opts, double* J, double* dJdD, int32_t* adj_iters) {
     if (!ctx || !t || !c0 || !target || nsteps <= 0 || every <= 0) return set_err(ctx, VFV_BAD_INPUT, "invalid argument");
     int rc = check_opts(ctx, opts);
     if (rc) return rc;
@@ -1825,6 +1943,7 @@ int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, in
     CK(cudaMemcpyAsync(rhs, hc.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
     vfv_solve_info info{};
     if ((rc = solve_dev(ctx, t->pat_t, rhs, zero, lam, opts, &info, t->nmesh, t->d_row_ptr.p))) return rc;
+    if (adj_iters) adj_iters[nsteps - 1] = info.iters;
     // backward sweep over the segments, last first
     for (int k = nsteps - 1; k >= 0; --k) {
         const int j = k / every;  // segment of state c_{k+1}: c_{j every + 1 .. j every + every}
@@ -1841,6 +1960,7 @@ int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, in
         if (k > 0) {
             launch_transport_rhs(s, n, t->cvol.p, t->dt, lam, rhs);  // M^T lam = -vol lam / dt
             if ((rc = solve_dev(ctx, t->pat_t, rhs, lam, lam2, opts, &info, t->nmesh, t->d_row_ptr.p))) return rc;
+            if (adj_iters) adj_iters[k - 1] = info.iters;
             std::swap(lam, lam2);
         }
     }

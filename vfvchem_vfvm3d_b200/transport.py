@@ -51,16 +51,19 @@ class TransientTransportGpu:
                                                           L.ptr(its, C.c_int32)))
         return out, its[:nsteps]
 
-    def adjoint_D(self, c0, nsteps: int, target, every: int = 10, opts: GmresOptions | None = None):
-        """(J, dJ/dD) for J = 0.5 ||c_nsteps - target||^2, checkpointing every `every` steps."""
+    def adjoint_D(self, c0, nsteps: int, target, every: int = 10, opts: GmresOptions | None = None, return_iters: bool = False):
+        """(J, dJ/dD) for J = 0.5 ||c_nsteps - target||^2, checkpointing every `every` steps; with
+        return_iters also the GMRES iterations of each transposed solve ([k] gives lambda_{k+1})."""
         opts = opts or GmresOptions(tol=1e-12, restart=30, max_outer=500, precond=L.PRECOND_ILU0)
         c0 = np.ascontiguousarray(c0, dtype=np.float64)
         target = np.ascontiguousarray(target, dtype=np.float64)
         J, g = C.c_double(), C.c_double()
+        its = np.zeros(max(nsteps, 1), np.int32)
         o = opts.to_c()
         _check(self.ctx.handle, L.load().vfv_transport_adjoint_D(self.ctx.handle, self._h, L.dptr(c0), int(nsteps), int(every),
-                                                                L.dptr(target), C.byref(o), C.byref(J), C.byref(g)))
-        return J.value, g.value
+                                                                L.dptr(target), C.byref(o), C.byref(J), C.byref(g),
+                                                                L.ptr(its, C.c_int32)))
+        return (J.value, g.value, its[:nsteps]) if return_iters else (J.value, g.value)
 
     def close(self) -> None:
         if getattr(self, "_h", None):
