@@ -42,6 +42,8 @@ extern "C" {
 #define VFV_PRECOND_NONE 0
 #define VFV_PRECOND_JACOBI 1 /* the reference's JacobiPreconLinOp (linear_gmres.rs:79) */
 #define VFV_PRECOND_ILU0 2   /* added: ILU(0) on A's pattern */
+#define VFV_PRECOND_BJ4 3    /* added: 4x4 block-Jacobi over rows {v, N+v, 2N+v, 3N+v} of a field-major
+                                [u | v | w | p] system (n = 4N); graph engine only */
 #define VFV_FP64 0           /* all Krylov vectors, SpMV and preconditioner in double */
 #define VFV_MIXED 1          /* float inner GMRES cycles inside double iterative refinement */
 #define VFV_ILU_MULTICOLOR 0 /* ILU(0) of the greedy-multicolour permutation (few levels) */
@@ -211,6 +213,39 @@ int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nste
  * lambda_{k+1}. */
 int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, int every, const double* target,
                             const vfv_gmres_opts* opts, double* J, double* dJdD, int32_t* adj_iters);
+
+/* ---------------------------------------------------------------- coupled Navier-Stokes (SteadyFlow)
+ * The field-major [u | v | w | p] system (n = 4 N unknowns) of SteadyFlow::assemble_matrix
+ * (src/steady/core/steady_flow.rs:255-303) for one domain whose six faces are velocity boundaries
+ * (OpVecBndDirichlet + OpSclBndDivergence + OpSclBndPressureStabilizer per boundary) and whose
+ * pressure is fixed at one vertex (OpSclDomPressureReference, opscl_dom_pref.rs:40-64), with the
+ * Rhie-Chow flow data of flow_helper::update_flow (src/operator/core/flow_helper.rs:3-179). Pattern:
+ * bit-exact to the reference's triplet build; values: the row's triplets summed in push order. */
+typedef struct vfv_flow vfv_flow;
+
+/* Symbolic setup only, on the host (no device): nnz and triplet count of the system, and its CSR
+ * pattern when rowptr [4N+1] / colind [nnz] are given. Replaces update_sparse for this system. */
+int vfv_flow_pattern_host(const vfv_mesh* mesh, int64_t pref_vid, int64_t* nnz, int64_t* ntrip, int32_t* rowptr, int32_t* colind);
+/* rho, mu [N]; fce, bc_vel [3][N] (body force rho g; boundary velocity at node vertices);
+ * pref_vid: vertex whose pressure row becomes p = pref. Every node must lie on a boundary. */
+int vfv_flow_create(vfv_ctx* ctx, const vfv_mesh* mesh, const double* rho, const double* mu, const double* fce, const double* bc_vel,
+                    int64_t pref_vid, double pref, vfv_flow** out);
+void vfv_flow_destroy(vfv_flow* f);
+vfv_pattern* vfv_flow_pattern(vfv_flow* f); /* owned by the flow handle */
+int vfv_flow_info(const vfv_flow* f, int64_t* n_unknowns, int64_t* nnz, int64_t* ntrip);
+/* A(x), b(x) at the state x = [u | v | w | p] (update_grad, update_flow, assemble_matrix,
+ * build_matrix of steady_base.rs:60-66 / :86-91); b may be NULL. Host or device pointers. */
+int vfv_flow_assemble(vfv_ctx* ctx, vfv_flow* f, const double* x, double* b);
+int vfv_flow_assemble_device(vfv_ctx* ctx, vfv_flow* f, const double* x_dev, double* b_dev);
+/* Damped Picard iteration of SteadyBase::solve (src/steady/steady_base.rs:70-112): per iteration
+ * assemble at x, solve A x_u = b with x as the initial guess, x = (1 - damp) x + damp x_u, and the
+ * scaled change of scaled_residual (src/base/scaling.rs:113-136); stops below tol. x (host, [4N])
+ * holds the initial state (boundary velocities loaded) and receives the result. res, lin_iters
+ * (max_iter entries) may be NULL. solve_seconds: device time of the linear solves. Errors as the
+ * reference: SolverNonPositiveMaxIter / SolverNonPositiveTolerance / SolverInvalidDamping ->
+ * VFV_BAD_INPUT, SteadyNonFiniteResidual -> VFV_NONFINITE, SteadyDidNotConverge -> VFV_NOT_CONVERGED. */
+int vfv_flow_picard(vfv_ctx* ctx, vfv_flow* f, double* x, int max_iter, double tol, double damp, const vfv_gmres_opts* opts,
+                    double* res, int32_t* lin_iters, int32_t* iters_done, double* solve_seconds);
 
 #ifdef __cplusplus
 }

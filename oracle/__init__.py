@@ -10,6 +10,8 @@ Modules:
   geom_tet.py   the Voronoi dual of a tetrahedralisation (numpy)
   lu.py         FP64 sparse LU solve (scipy SuperLU), the reference's LinearLu role
   ordering.py   ILU(0) orderings (natural dependency levels, greedy multicolour)
+  ns_oracle.c   coupled Navier-Stokes assembly: pressure-gradient coefficients, Rhie-Chow flow
+                data, triplets of SteadyFlow::assemble_matrix in push order  (C, ctypes)
 """
 from __future__ import annotations
 
@@ -53,6 +55,8 @@ def lib():
         _lib.orc_csr_from_triplets.restype = C.c_int64
         _lib.orc_gmres.restype = C.c_int
         _lib.orc_ilu0_factor.restype = C.c_int
+        _lib.orc_grad_coeff.restype = C.c_int64
+        _lib.orc_ns_triplets.restype = C.c_int64
     return _lib
 
 
@@ -199,3 +203,76 @@ def gmres(rp, ci, va, b, x0=None, tol=1e-6, restart=50, max_outer=200, precond=1
     rc = lib().orc_gmres(C.c_int64(n), _p(rp), _p(ci), _p(va), _p(b), _p(x), C.c_double(tol), C.c_int(restart), C.c_int(max_outer),
                          C.c_int(precond), C.byref(s) if s is not None else None, C.c_int64(max_steps), C.byref(its), C.byref(rel))
     return x, rc == 0, its.value, rel.value
+
+
+# ---------------------------------------------------------------- coupled Navier-Stokes (ns_oracle.c)
+class OrcNsGeom(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64), ("n_pts", C.c_int64), ("n_dir", C.c_int64), ("n_bsub", C.c_int64),
+        ("np", C.c_void_p), ("ni", C.c_void_p), ("dist", C.c_void_p), ("area", C.c_void_p), ("norm", C.c_void_p),
+        ("skew", C.c_void_p), ("gw", C.c_void_p), ("cvol", C.c_void_p), ("cskew", C.c_void_p), ("bp", C.c_void_p),
+        ("bj", C.c_void_p), ("bk", C.c_void_p), ("barea", C.c_void_p), ("bnorm", C.c_void_p), ("bw", C.c_void_p),
+        ("gcp", C.c_void_p), ("gcv", C.c_void_p), ("gcc", C.c_void_p), ("n_gc", C.c_int64),
+    ]
+
+
+class NsGeom:
+    """The dual plus its pressure-gradient coefficients (Tetrahedron::grad_coeff) for the NS oracle."""
+
+    def __init__(self, dual: dict, n_pts: int):
+        self.keep = {k: np.ascontiguousarray(v) for k, v in dual.items()}
+        self.n = self.keep["nbr_ptr"].size - 1
+        self.n_pts = n_pts
+        g = OrcNsGeom()
+        g.n, g.n_pts, g.n_dir, g.n_bsub = self.n, n_pts, self.keep["nbr_idx"].size, self.keep["bnd_j"].size
+        for f, k in [("np", "nbr_ptr"), ("ni", "nbr_idx"), ("dist", "dist"), ("area", "area"), ("norm", "norm"), ("skew", "skew"),
+                     ("gw", "grad_wgt"), ("cvol", "cvol"), ("cskew", "cskew"), ("bp", "bnd_ptr"), ("bj", "bnd_j"), ("bk", "bnd_k"),
+                     ("barea", "bnd_area"), ("bnorm", "bnd_norm"), ("bw", "bnd_wgt")]:
+            setattr(g, f, self.keep[k].ctypes.data)
+        self.gcp = np.zeros(self.n + 1, np.int64)
+        tot = lib().orc_grad_coeff(C.byref(g), _p(self.gcp), None, None, C.c_int64(0))
+        self.gcv = np.empty(max(tot, 1), np.int32)
+        self.gcc = np.empty((3, max(tot, 1)))
+        lib().orc_grad_coeff(C.byref(g), _p(self.gcp), _p(self.gcv), _p(self.gcc), C.c_int64(max(tot, 1)))
+        self.n_gc = tot
+        g.gcp, g.gcv, g.gcc, g.n_gc = self.gcp.ctypes.data, self.gcv.ctypes.data, self.gcc.ctypes.data, max(tot, 1)
+        self.g = g
+        self.dual = dual
+
+    def vec_grad(self, vec):
+        """[9][n] LSQ gradients of the three components (u_x u_y u_z v_x ... w_z)."""
+        vec = np.asarray(vec, np.float64).reshape(3, self.n)
+        return np.ascontiguousarray(np.concatenate([grad(self.dual, vec[q]) for q in range(3)]))
+
+    def flow(self, vel, p, den, visc, fce):
+        """(rc, flux): Rhie-Chow coefficient V/a_P per vertex and face mass flux per directed face."""
+        vel = _c(vel, np.float64).reshape(3, self.n)
+        fce = _c(fce, np.float64).reshape(3, self.n)
+        den, visc, p = (_c(np.broadcast_to(a, (self.n,)), np.float64) for a in (den, visc, p))
+        gvel, gfce = self.vec_grad(vel), self.vec_grad(fce)
+        gden, gvisc = grad(self.dual, den), grad(self.dual, visc)
+        rc = np.empty(self.n)
+        flux = np.empty(self.keep["nbr_idx"].size)
+        lib().orc_ns_flow(C.byref(self.g), _p(vel), _p(gvel), _p(p), _p(den), _p(gden), _p(visc), _p(gvisc), _p(fce), _p(gfce), _p(rc),
+                          _p(flux))
+        return rc, flux
+
+    def triplets(self, node_bnd, bnd_order, bc_vel, pref_vid, pref, vel, p, den, visc, fce):
+        """Triplets (rows, cols, vals) and b [4n] of SteadyFlow::assemble_matrix at the state (vel, p)."""
+        vel = _c(vel, np.float64).reshape(3, self.n)
+        fce = _c(fce, np.float64).reshape(3, self.n)
+        den, visc, p = (_c(np.broadcast_to(a, (self.n,)), np.float64) for a in (den, visc, p))
+        rc, flux = self.flow(vel, p, den, visc, fce)
+        gvel, gfce = self.vec_grad(vel), self.vec_grad(fce)
+        gden, gvisc = grad(self.dual, den), grad(self.dual, visc)
+        nb, order = _c(node_bnd, np.int32), _c(bnd_order, np.int32)
+        bcv = _c(bc_vel, np.float64).reshape(3, self.n)
+        args = [_p(nb), C.c_int32(order.size), _p(order), _p(bcv), C.c_int64(pref_vid), C.c_double(pref), _p(vel), _p(gvel), _p(den),
+                _p(gden), _p(visc), _p(gvisc), _p(fce), _p(gfce), _p(rc), _p(flux)]
+        cap = lib().orc_ns_triplets(C.byref(self.g), *args, None, None, None, None)
+        r = np.empty(cap, np.uint64)
+        c = np.empty(cap, np.uint64)
+        v = np.empty(cap)
+        b = np.empty(4 * self.n)
+        nt = lib().orc_ns_triplets(C.byref(self.g), *args, _p(r), _p(c), _p(v), _p(b))
+        return r[:nt].copy(), c[:nt].copy(), v[:nt].copy(), b

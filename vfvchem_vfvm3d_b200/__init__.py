@@ -7,6 +7,9 @@ Python face of libvfvgpu (C ABI in include/vfv_gpu.h). The names mirror the refe
 * :class:`SteadyHeatGpu` — the device assembly of ``SteadyHeat::assemble_matrix``
   (src/steady/core/steady_heat.rs:143-171) over a :class:`Mesh` (the Voronoi dual of
   ``Tetrahedron::update_tet``, src/base/geom_tet.rs:58-350).
+* :class:`TransientTransportGpu` — batched transient advection-diffusion over many meshes.
+* :class:`SteadyFlowGpu` — the coupled Navier-Stokes system of ``SteadyFlow``
+  (src/steady/core/steady_flow.rs) and its damped Picard loop.
 * :class:`Context`, :class:`Pattern` — the device context and a CSR pattern with its values.
 
 Everything runs on the GPU through the compiled library; importing works without a GPU, but any
@@ -28,9 +31,10 @@ from .mesh import Mesh  # noqa: F401
 from .heat import SteadyHeatGpu  # noqa: F401
 from .linear import LinearGmres, Triplet, SparseMatrix  # noqa: F401
 from .transport import TransientTransportGpu  # noqa: F401
+from .flow import SteadyFlowGpu  # noqa: F401
 from . import _lib  # noqa: F401
 
 __all__ = [
     "Context", "Pattern", "GmresOptions", "SolveInfo", "Mesh", "SteadyHeatGpu", "LinearGmres", "Triplet",
-    "SparseMatrix", "VFVChemError", "LinearGmresDidNotConverge", "default_context", "TransientTransportGpu",
+    "SparseMatrix", "VFVChemError", "LinearGmresDidNotConverge", "default_context", "TransientTransportGpu", "SteadyFlowGpu",
 ]

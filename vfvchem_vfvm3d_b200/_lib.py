@@ -14,7 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvfvgpu.so")
 
 VFV_OK, VFV_NOT_CONVERGED, VFV_NONFINITE, VFV_BAD_INPUT, VFV_CUDA_ERROR, VFV_TIMEOUT = range(6)
-PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_BJ4 = 0, 1, 2, 3
 FP64, MIXED = 0, 1
 ILU_MULTICOLOR, ILU_NATURAL = 0, 1
 ENGINE_PERSISTENT, ENGINE_GRAPH = 0, 1
@@ -97,6 +97,14 @@ SIGNATURES = [
     ("vfv_transport_assemble", C.c_int, [_P, _P, _P, _P, C.c_int]),
     ("vfv_transport_run", C.c_int, [_P, _P, _DP, C.c_int, C.POINTER(GmresOpts), _DP, _I32P]),
     ("vfv_transport_adjoint_D", C.c_int, [_P, _P, _DP, C.c_int, C.c_int, _DP, C.POINTER(GmresOpts), _DP, _DP, _I32P]),
+    ("vfv_flow_pattern_host", C.c_int, [_P, C.c_int64, _I64P, _I64P, _I32P, _I32P]),
+    ("vfv_flow_create", C.c_int, [_P, _P, _DP, _DP, _DP, _DP, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]),
+    ("vfv_flow_destroy", None, [_P]),
+    ("vfv_flow_pattern", _P, [_P]),
+    ("vfv_flow_info", C.c_int, [_P, _I64P, _I64P, _I64P]),
+    ("vfv_flow_assemble", C.c_int, [_P, _P, _DP, _DP]),
+    ("vfv_flow_assemble_device", C.c_int, [_P, _P, C.c_void_p, C.c_void_p]),
+    ("vfv_flow_picard", C.c_int, [_P, _P, _DP, C.c_int, C.c_double, C.c_double, C.POINTER(GmresOpts), _DP, _I32P, _I32P, _DP]),
     ("vfv_heat_adjoint", C.c_int, [_P, _P, _DP, _DP, C.POINTER(GmresOpts), _DP, _DP, _DP, C.POINTER(SolveInfo)]),
 ]
 

@@ -428,6 +428,26 @@ __global__ void k_jacobi_inv(int64_t n, const int32_t* __restrict__ diag_pos, co
     dinv[i] = d != 0.0 ? 1.0 / d : 1.0;
 }
 
+// z = M^-1 r for the 4x4 block-Jacobi preconditioner of a field-major 4-field system: block v
+// couples rows {v, nb+v, 2nb+v, 3nb+v}; binv is [16][nb] (row-major 4x4 per block). `in` and `out`
+// may alias (each thread reads its four entries before writing them).
+template <typename T>
+__global__ void __launch_bounds__(256) k_bj4_apply(int64_t nb, const T* __restrict__ binv, const T* in, T* out, const DevStatus* st) {
+    if (st && st->done) return;
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nb) return;
+    T r[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) r[c] = in[c * nb + v];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        T acc = binv[(4 * a) * nb + v] * r[0];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) acc += binv[(4 * a + c) * nb + v] * r[c];
+        out[a * nb + v] = acc;
+    }
+}
+
 // out[k] = (T)(val[k] * dinv[col[k]])  (right Jacobi scaling folded into the Krylov matrix)
 template <typename T>
 __global__ void k_scale_cols(int64_t nnz, const int32_t* __restrict__ ci, const double* __restrict__ val,

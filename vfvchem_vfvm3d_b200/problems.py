@@ -92,3 +92,46 @@ def transport_fields(meshes, phase_seed: int = 9):
         a, b, c = rng.uniform(0, 2 * np.pi, 3)
         c0.append(1.0 + 0.5 * np.sin(np.pi * x + a) * np.sin(np.pi * y + b) * np.sin(np.pi * z + c))
     return np.concatenate(vel, axis=1), np.concatenate(c0)
+
+
+@dataclass
+class FlowProblem:
+    """Steady incompressible flow in the unit cube with velocity boundaries on all six faces and
+    the pressure fixed at one node (the layout of the reference's examples/flow/flow_lid.rs)."""
+    mesh: Mesh
+    rho: np.ndarray       # density per vertex
+    mu: np.ndarray        # viscosity per vertex
+    fce: np.ndarray       # body force [3][n] (rho g, not g)
+    bc_vel: np.ndarray    # boundary velocity [3][n] at nodes, 0 at points
+    node_bnd: np.ndarray  # boundary id per vertex, -1 for points
+    pref_vid: int         # vertex whose pressure is fixed (node 0 = first node)
+    pref: float = 0.0
+    bnd_order: np.ndarray = field(default_factory=lambda: HEAT_BND_ORDER.copy())
+
+    @property
+    def n(self) -> int:
+        return self.mesh.n_tot
+
+    def initial_state(self) -> np.ndarray:
+        """x0 = [u | v | w | p] with the boundary velocities loaded (initial_dirichlet)."""
+        x = np.zeros(4 * self.n)
+        x[:3 * self.n] = self.bc_vel.reshape(-1)
+        return x
+
+
+def lid_cavity(n: int, mesh_seed: int = 42, rho: float = 1.0, mu: float = 0.01, lid=(1.0, 0.0, 0.0), gravity: float = 0.0) -> FlowProblem:
+    """Lid-driven cavity: u = lid on bnd_t (z = 1), no-slip on the other faces, p = 0 at node 0;
+    rho = 1, mu = 0.01 (Re = 100 with U = L = 1) by default. ``gravity`` adds the body force
+    (0, 0, -rho g)."""
+    mesh = Mesh.jitter_cube(n, mesh_seed, 0.25)
+    N = mesh.n_tot
+    _, nb, _ = mesh.export()
+    node_bnd = np.full(N, -1, np.int32)
+    node_bnd[mesh.n_pts:] = nb
+    bc = np.zeros((3, N))
+    top = node_bnd == 5
+    for q in range(3):
+        bc[q, top] = lid[q]
+    fce = np.zeros((3, N))
+    fce[2, :] = -rho * gravity
+    return FlowProblem(mesh, np.full(N, float(rho)), np.full(N, float(mu)), fce, bc, node_bnd, mesh.n_pts)
