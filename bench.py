@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--engine", type=int, default=1, help="0 persistent cycle kernel, 1 CUDA graph of per-phase kernels")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched-transport timings")
     ap.add_argument("--batch", type=int, default=256, help="meshes in the batched transport timing")
+    ap.add_argument("--flow-n", type=int, default=64, help="grid points per axis of the cavity flow timing")
     return ap.parse_args()
 
 
@@ -65,6 +66,50 @@ def extras_adjoint(heat, prob, x_ref_h, ctx):
         ts.append(time.perf_counter() - t0)
     return {"adjoint_s": min(ts), "adjoint_iters": info.iters, "sensors": 1000, "grad_norm_logk": float(np.linalg.norm(dk)),
             "grad_norm_q": float(np.linalg.norm(dq)), "workload": "dJ/dlog k and dJ/dq on the same 1M-vertex system, host arrays in/out"}
+
+
+def extras_flow(ctx, n):
+    """Lid-driven cavity (rho = 1, mu = 0.01, lid u = (1, 0, 0)) on an n^3 jittered cube, 4 n^3
+    unknowns: up to 20 damped Picard iterations (damping 0.8), each solved by GMRES(100) + 4x4
+    block-Jacobi to 1e-8 relative residual, FP64 and FP32-inner / FP64-refinement."""
+    from vfvchem_vfvm3d_b200 import SteadyFlowGpu
+    from vfvchem_vfvm3d_b200 import _lib as L
+    from vfvchem_vfvm3d_b200.flow import flow_options
+    from vfvchem_vfvm3d_b200.problems import lid_cavity
+    import torch
+    t0 = time.perf_counter()
+    prob = lid_cavity(n)
+    t_mesh = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    fl = SteadyFlowGpu(prob, ctx=ctx)
+    t_setup = time.perf_counter() - t0
+    x0 = torch.tensor(prob.initial_state(), device="cuda")
+    bd = torch.empty_like(x0)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+    fl.assemble_device(x0.data_ptr(), bd.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(5):
+        fl.assemble_device(x0.data_ptr(), bd.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    asm_ms = e0.elapsed_time(e1) / 5
+    out = {"workload": f"lid-driven cavity {n}^3 ({4 * prob.n} unknowns, {fl.nnz} nnz, {fl.ntrip} triplets), Re 100; "
+                       "20 Picard iterations max, damping 0.8, GMRES(100)+BJ4 to 1e-8 relres",
+           "unknowns": 4 * prob.n, "nnz": fl.nnz, "triplets": fl.ntrip, "mesh_s": t_mesh, "setup_s": t_setup, "assembly_ms": asm_ms}
+    finals = {}
+    for prec, name in [(L.FP64, "fp64"), (L.MIXED, "mixed")]:
+        t0 = time.perf_counter()
+        r = fl.picard(max_iter=20, tol=1e-300, damp=0.8, opts=flow_options(prec, tol=1e-8, max_outer=100), raise_on_error=False)
+        out[name] = {"picard_s": time.perf_counter() - t0, "solve_s": r.solve_seconds, "picard_iters": r.iterations,
+                     "gmres_iters": int(np.sum(r.lin_iters)), "last_residual": float(r.residuals[-1]) if r.iterations else None,
+                     "status": r.status}
+        finals[name] = r.x
+    out["speedup_mixed_vs_fp64_solve"] = out["fp64"]["solve_s"] / max(out["mixed"]["solve_s"], 1e-12)
+    out["rel_diff_mixed_vs_fp64"] = float(np.linalg.norm(finals["mixed"] - finals["fp64"]) / np.linalg.norm(finals["fp64"]))
+    fl.close()
+    return out
 
 
 def extras_transport(ctx, count):
@@ -320,7 +365,8 @@ def main():
     extras = None
     if not args.no_extras and world == 1:
         extras = {"steady_adjoint": extras_adjoint(heat, prob, x_ref.cpu().numpy(), ctx),
-                  "batched_transport": extras_transport(ctx, args.batch)}
+                  "batched_transport": extras_transport(ctx, args.batch),
+                  "cavity_flow": extras_flow(ctx, args.flow_n)}
 
     clocks = clk.summary()
     out = {
