@@ -36,7 +36,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vfv", choices=["vfv", "reference"])
-    ap.add_argument("--n", type=int, default=100, help="grid points per axis (100 -> 1,000,000 vertices)")
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=100, help="grid points per axis (100 -> 1,000,000 vertices)")
     ap.add_argument("--restart", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -216,19 +216,13 @@ def cpu_baseline_jacobi(rp, ci, va, b, x0, restart, budget_s, steps_needed=None)
 
 def main():
     args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from vfvchem_vfvm3d_b200 import replicas
+    R = replicas.init_from_env()
+    rank, world, local = R.rank, R.world, R.local
     import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     if args.impl == "reference":
-        return run_reference(args, rank, world, dist)
+        return run_reference(args, R)
 
     from vfvchem_vfvm3d_b200 import Context, GmresOptions, SteadyHeatGpu
     from vfvchem_vfvm3d_b200 import _lib as L
@@ -289,8 +283,7 @@ def main():
             ts.append(e0.elapsed_time(e1) / 1e3)
         return ts, infos, err(x_d)
 
-    if dist:
-        dist.barrier()
+    replicas.barrier(R)
     torch.cuda.synchronize()
     launches0 = ctx.launch_count
     with ClockSampler(local) as clk:
@@ -300,10 +293,8 @@ def main():
     torch.cuda.synchronize()
     mx_s = sum(t_mx) / len(t_mx)
     f64_s = sum(t_64) / len(t_64)
-    if dist:
-        t = torch.tensor([mx_s, f64_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        mx_s, f64_s = float(t[0]), float(t[1])
+    replicas.barrier(R)
+    mx_s, f64_s = replicas.max_over_ranks(R, [mx_s, f64_s])
 
     # SpMV (FP64 and FP32) timed alone: the kernel the metric names
     xs = torch.randn(n, dtype=torch.float64, device=dev)
@@ -404,17 +395,16 @@ def main():
     }
     if rank == 0:
         print(json.dumps(out))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finalize(R)
 
 
-def run_reference(args, rank, world, dist):
-    """Reference arm: Jacobi GMRES on the host cores (the reference's LinearGmres algorithm)."""
-    if rank != 0:
-        if dist:
-            dist.barrier()
-            dist.destroy_process_group()
+def run_reference(args, R):
+    """Reference arm: Jacobi GMRES on the host cores (the reference's LinearGmres algorithm);
+    rank 0 alone runs it, the other ranks only join the final barrier."""
+    from vfvchem_vfvm3d_b200 import replicas
+    world = R.world
+    if R.rank != 0:
+        replicas.finalize(R)
         return
     import oracle  # the reference arm runs the CPU port of the reference's algorithm
     from vfvchem_vfvm3d_b200.problems import steady_heat
@@ -448,9 +438,7 @@ def run_reference(args, rank, world, dist):
                                            f"{its} steps run to relres {rel:.2e} ({'converged' if ok else 'extrapolated'})"},
                 "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     print(json.dumps(out))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finalize(R)
 
 
 if __name__ == "__main__":
