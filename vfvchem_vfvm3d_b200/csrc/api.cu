@@ -149,7 +149,7 @@ struct vfv_pattern {
 // ================================================================ GMRES driver
 namespace {
 
-// SpMV with the lanes-per-row the pattern was tuned for (2, 4 or 8)
+// SpMV with the lanes-per-row the pattern was tuned for (2, 4, 8, 16 or 32)
 template <typename TV, typename TX, typename TY, typename TA>
 void launch_spmv(cudaStream_t s, int lanes, int64_t n, const int32_t* rp, const int32_t* ci, const TV* val, const TX* x, TY* y,
                  const double* scale, const DevStatus* st) {
@@ -159,6 +159,12 @@ void launch_spmv(cudaStream_t s, int lanes, int64_t n, const int32_t* rp, const 
             break;
         case 8:
             k_spmv<TV, TX, TY, TA, 8><<<grid_for(n * 8), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
+            break;
+        case 16:
+            k_spmv<TV, TX, TY, TA, 16><<<grid_for(n * 16), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
+            break;
+        case 32:
+            k_spmv<TV, TX, TY, TA, 32><<<grid_for(n * 32), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
             break;
         default:
             k_spmv<TV, TX, TY, TA, 4><<<grid_for(n * 4), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
@@ -1358,8 +1364,9 @@ int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, c
     return VFV_OK;
 }
 
-// Autotuner: times the SpMV of this pattern (its current values) with 2, 4 and 8 lanes per row in
-// double and in float, keeps the fastest of each for every later SpMV and solver of the pattern.
+// Autotuner: times the SpMV of this pattern (its current values) with 2, 4, 8, 16 and 32 lanes per
+// row in double and in float (short rows of a scalar problem favour few lanes, the 2-ring rows of
+// the coupled flow system a warp per row), keeps the fastest of each for every later SpMV and solver of the pattern.
 // Must run before the pattern's first solve (solvers capture their kernels once).
 int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t* lanes32) {
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
@@ -1378,7 +1385,7 @@ int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    const int cand[3] = {2, 4, 8};
+    const int cand[5] = {2, 4, 8, 16, 32};
     for (int prec = 0; prec < 2; ++prec) {
         float best = 1e30f;
         int best_g = kSpG;
@@ -1403,7 +1410,7 @@ int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->launches += 2 * 3 * 13 + 1;
+    ctx->launches += 2 * 5 * 13 + 1;
     CK(cudaGetLastError());
     if (lanes64) *lanes64 = p->spmv_lanes[0];
     if (lanes32) *lanes32 = p->spmv_lanes[1];
@@ -1412,8 +1419,8 @@ int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t
 
 int vfv_pattern_set_spmv_lanes(vfv_ctx* ctx, vfv_pattern* p, int32_t lanes64, int32_t lanes32) {
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    auto ok = [](int32_t g) { return g == 2 || g == 4 || g == 8; };
-    if (!ok(lanes64) || !ok(lanes32)) return set_err(ctx, VFV_BAD_INPUT, "SpMV lanes per row must be 2, 4 or 8");
+    auto ok = [](int32_t g) { return g == 2 || g == 4 || g == 8 || g == 16 || g == 32; };
+    if (!ok(lanes64) || !ok(lanes32)) return set_err(ctx, VFV_BAD_INPUT, "SpMV lanes per row must be 2, 4, 8, 16 or 32");
     p->spmv_lanes[0] = lanes64;
     p->spmv_lanes[1] = lanes32;
     return VFV_OK;
@@ -2185,6 +2192,8 @@ int vfv_flow_create(vfv_ctx* ctx, const vfv_mesh* mh, const double* rho, const d
     int rc = vfv_pattern_from_csr(ctx, 4 * n, L.rp.data(), L.ci.data(), &pat);
     if (rc) return rc;
     f->pat = pat;
+    rc = vfv_pattern_autotune(ctx, pat, nullptr, nullptr);  // rows of 16 to 400 entries: measure the SpMV shape
+    if (rc) return rc;
     cudaStream_t s = ctx->stream;
     std::vector<int32_t> np(n + 1), bp(n + 1);
     for (int64_t v = 0; v <= n; ++v) {
