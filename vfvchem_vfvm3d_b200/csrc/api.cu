@@ -660,11 +660,13 @@ struct Gmres : SolverBase {
             in = z.p;
         }
         cudaEventRecord(ev[1], s);
-        k_spmv<T, T, T, T, G><<<grid_for(n * G), kBlk, 0, s>>>(n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
+        launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
         cudaEventRecord(ev[2], s);
         k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
+        k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
         cudaEventRecord(ev[3], s);
         k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+        k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
         cudaEventRecord(ev[4], s);
         k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
         cudaEventRecord(ev[5], s);
@@ -739,7 +741,9 @@ struct Gmres : SolverBase {
             }
             launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
             k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
+            k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
             k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+            k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
             k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
         }
         k_backsolve<<<1, 32, 0, s>>>(K);

@@ -22,6 +22,8 @@ namespace vfv {
 
 constexpr int kBlk = 256;        // threads per block of the vector kernels
 constexpr int kRows = 4;         // rows per thread in the multi-vector kernels
+constexpr int kVecMinBlocks = 8; // <= 32 registers: 8 x 256 threads per SM, so the 977 blocks of a
+                                 // 10^6-row vector fit in one wave of 148 SMs (no tail wave)
 constexpr int kMaxBasis = 128;   // m + 1 <= kMaxBasis
 
 // Per-solve device workspace pointers used by the Krylov kernels.
@@ -75,23 +77,29 @@ __device__ __forceinline__ double reduce_partials(const double* part, int nblk, 
     return block_sum(s, red);
 }
 
-// Columns c < cnt of part[c][0..nblk): one warp per column, four independent accumulators per
-// lane, then a fixed shuffle tree; out(c, sum) is called by lane 0. Deterministic.
+// Columns c < cnt of part[c][0..nblk): one warp per column; each lane loads 16 partials at once
+// (the last block's reduction is latency-bound, so the loads of a batch must all be in flight),
+// sums them pairwise, then a fixed shuffle tree; out(c, sum) is called by lane 0. Deterministic.
 template <typename F>
 __device__ __forceinline__ void reduce_cols_warp(const double* part, int nblk, int cnt, F out) {
+    constexpr int kB = 16;  // partials per lane in flight: one L2 round trip per 512 partials
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int c = wid; c < cnt; c += nw) {
         const double* p = part + (int64_t)c * nblk;
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int q = lane;
-        for (; q + 96 < nblk; q += 128) {
-            s0 += __ldcg(p + q);
-            s1 += __ldcg(p + q + 32);
-            s2 += __ldcg(p + q + 64);
-            s3 += __ldcg(p + q + 96);
+        double s = 0.0;
+        for (int q0 = 0; q0 < nblk; q0 += 32 * kB) {
+            double v[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                const int q = q0 + lane + 32 * k;
+                v[k] = q < nblk ? __ldcg(p + q) : 0.0;
+            }
+#pragma unroll
+            for (int h = kB / 2; h > 0; h >>= 1)
+#pragma unroll
+                for (int k = 0; k < h; ++k) v[k] += v[k + h];
+            s += v[0];
         }
-        for (; q < nblk; q += 32) s0 += __ldcg(p + q);
-        double s = (s0 + s1) + (s2 + s3);
         s = warp_sum(s);
         if (lane == 0) out(c, s);
     }
@@ -185,9 +193,9 @@ __global__ void __launch_bounds__(kBlk) k_residual(KrylovDev K, const int32_t* _
 }
 
 // ---------------------------------------------------------------- multi-dot (first CGS pass)
-// d_i = <u_i, w> for i < nvec. Last block: hacc[i] = d_i / beta_i, coef[i] = d_i / beta_i^2.
+// Per-block partials of d_i = <u_i, w> for i < nvec (k_dots_finish<true> completes them).
 template <typename T>
-__global__ void __launch_bounds__(kBlk) k_mdot(KrylovDev K, const T* __restrict__ V, const T* __restrict__ w, int nvec) {
+__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_mdot(KrylovDev K, const T* __restrict__ V, const T* __restrict__ w, int nvec) {
     if (K.st->done) return;
     __shared__ double red[kMaxBasis][kBlk / 32];
     __shared__ double red2[kBlk / 32];
@@ -214,23 +222,52 @@ __global__ void __launch_bounds__(kBlk) k_mdot(KrylovDev K, const T* __restrict_
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
         double s = 0.0;
         for (int q = 0; q < nw; ++q) s += red[i][q];
-        publish_partial(K.part + (int64_t)i * K.nblk + blockIdx.x, s);
+        K.part[(int64_t)i * K.nblk + blockIdx.x] = s;  // summed by k_dots_finish (the next launch)
     }
-    if (!last_block_arrive(K.counter + 1)) return;
-    reduce_cols_warp(K.part, K.nblk, nvec, [&](int i, double d) {
-        const double ib = K.inv_beta[i];
-        K.hacc[i] = d * ib;
-        K.coef[i] = d * ib * ib;
-    });
-    if (threadIdx.x == 0) K.counter[1] = 0u;
+}
+
+// Cross-block sums of the multi-dot partials, one warp per basis vector spread over the GPU (a
+// last-block reduction here would leave the GPU idle for ~15 µs while one block walks
+// nvec x nblk partials). FIRST: hacc_i = d_i / beta_i; else hacc_i += d_i / beta_i; both set
+// coef_i = d_i / beta_i^2 for the update that follows.
+template <bool FIRST>
+__global__ void __launch_bounds__(256) k_dots_finish(KrylovDev K, int nvec) {
+    if (K.st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (c >= nvec) return;
+    const double* p = K.part + (int64_t)c * K.nblk;
+    constexpr int kB = 16;
+    double s = 0.0;
+    for (int q0 = 0; q0 < K.nblk; q0 += 32 * kB) {
+        double v[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) {
+            const int q = q0 + lane + 32 * k;
+            v[k] = q < K.nblk ? p[q] : 0.0;
+        }
+#pragma unroll
+        for (int h = kB / 2; h > 0; h >>= 1)
+#pragma unroll
+            for (int k = 0; k < h; ++k) v[k] += v[k + h];
+        s += v[0];
+    }
+    s = warp_sum(s);
+    if (lane == 0) {
+        const double ib = K.inv_beta[c];
+        if (FIRST) K.hacc[c] = s * ib;
+        else K.hacc[c] += s * ib;
+        K.coef[c] = s * ib * ib;
+    }
 }
 
 // ---------------------------------------------------------------- update + second pass
-// w <- w - sum_i coef_i u_i. Then, with FINAL == false, the second CGS pass d'_i = <u_i, w>
-// (last block adds d'_i/beta_i into hacc and sets coef); with FINAL == true, ||w||^2 and the
-// last block finishes the Hessenberg column j, the Givens rotation and the convergence test.
+// w <- w - sum_i coef_i u_i. Then, with FINAL == false, the partials of the second CGS pass
+// d'_i = <u_i, w> (k_dots_finish<false> adds d'_i/beta_i into hacc and sets coef); with
+// FINAL == true, ||w||^2 and the last block finishes the Hessenberg column j, the Givens rotation
+// and the convergence test.
 template <typename T, bool FINAL>
-__global__ void __launch_bounds__(kBlk) k_update(KrylovDev K, const T* __restrict__ V, T* __restrict__ w, int nvec, int j) {
+__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, const T* __restrict__ V, T* __restrict__ w, int nvec, int j) {
     if (K.st->done) return;
     __shared__ double red[kMaxBasis][kBlk / 32];
     __shared__ double red2[kBlk / 32];
@@ -242,6 +279,9 @@ __global__ void __launch_bounds__(kBlk) k_update(KrylovDev K, const T* __restric
     double acc[kRows];
 #pragma unroll
     for (int r = 0; r < kRows; ++r) acc[r] = 0.0;
+    // the second CGS pass (FINAL == false) keeps four basis vectors' loads in flight per thread;
+    // the last pass does better without (its occupancy is the limit)
+#pragma unroll(FINAL ? 1 : 4)
     for (int i = 0; i < nvec; ++i) {
         const T* u = V + (int64_t)i * K.ldv;
         const double c = s_coef[i];
@@ -279,15 +319,8 @@ __global__ void __launch_bounds__(kBlk) k_update(KrylovDev K, const T* __restric
         for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
             double s = 0.0;
             for (int q = 0; q < nw; ++q) s += red[i][q];
-            publish_partial(K.part + (int64_t)i * K.nblk + blockIdx.x, s);
+            K.part[(int64_t)i * K.nblk + blockIdx.x] = s;  // summed by k_dots_finish<false>
         }
-        if (!last_block_arrive(K.counter + 2)) return;
-        reduce_cols_warp(K.part, K.nblk, nvec, [&](int i, double d) {
-            const double ib = K.inv_beta[i];
-            K.hacc[i] += d * ib;
-            K.coef[i] = d * ib * ib;
-        });
-        if (threadIdx.x == 0) K.counter[2] = 0u;
     } else {
         double s = 0.0;
 #pragma unroll
