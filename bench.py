@@ -40,7 +40,8 @@ def parse():
     ap.add_argument("--restart", type=int, default=50)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--engine", type=int, default=1, help="0 persistent cycle kernel, 1 CUDA graph of per-phase kernels")
+    ap.add_argument("--engine", type=int, default=2,
+                    help="0 persistent cycle kernel, 1 CUDA graph of per-phase kernels, 2 graph with the ILU(0) sweeps overlapped (flexible GMRES)")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched-transport timings")
     ap.add_argument("--batch", type=int, default=256, help="meshes in the batched transport timing")
     ap.add_argument("--flow-n", type=int, default=64, help="grid points per axis of the cavity flow timing")
@@ -376,7 +377,7 @@ def main():
         "data": "synthetic (seeded jittered-cube Delaunay mesh, seeded fields)",
         "config": {"workload": f"steady heat, {args.n}^3 jittered cube ({n} vertices, {nnz} nnz), log k~N(0,1), q~U[0,1]; "
                                f"GMRES({args.restart})+ILU(0) multicolour to 1e-8 rel. error",
-                   "n": n, "nnz": nnz, "restart": args.restart, "tol_relres": tol, "l2": "inputs larger than L2 (no flush)",
+                   "n": n, "nnz": nnz, "restart": args.restart, "tol_relres": tol, "engine": args.engine, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "fp64_solve_s": f64_s,
         "speedup_mixed_vs_fp64": f64_s / mx_s,

@@ -50,6 +50,8 @@ extern "C" {
 #define VFV_ILU_NATURAL 1    /* ILU(0) in the given order, level scheduled */
 #define VFV_ENGINE_PERSISTENT 0 /* one cooperative kernel per restart cycle, grid barriers between phases */
 #define VFV_ENGINE_GRAPH 1      /* a CUDA graph of one kernel per phase, replayed per restart cycle (default) */
+#define VFV_ENGINE_OVERLAP 2    /* graph engine as flexible GMRES whose ILU(0) sweeps run on a second stream,
+                                   overlapped with the orthogonalisation (ILU(0) only) */
 
 /* ---- boundary-condition kinds of the heat operator (SteadyHeat::add_temp_bnd / add_hflx_bnd) */
 #define VFV_BC_TEMP 0 /* Dirichlet: OpSclBndDirichlet */

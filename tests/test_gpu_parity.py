@@ -202,6 +202,27 @@ def test_gmres_matches_lu(gpu_ctx, c1h_system, c1_hetero, precond, precision, en
     assert _rel(x, xl) <= SOL_RTOL
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("order", [0, 1])
+def test_overlap_engine_matches_lu(gpu_ctx, c1h_system, c1_hetero, precision, order):
+    """Flexible GMRES with the ILU(0) sweeps overlapped with the orthogonalisation: same bars,
+    and within a few iterations of the plain right-preconditioned GMRES."""
+    from vfvchem_vfvm3d_b200 import GmresOptions, Pattern, VFVChemError
+    (rp, ci, va), b, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    xl = lu_solve(rp, ci, va, b)
+    kw = dict(tol=1e-12, restart=30, max_outer=2000, precond=2, precision=precision, ilu_order=order,
+              inner_rtol=1e-6 if precision == 1 else 0.0)
+    x, info = p.solve(b, c1_hetero.T0, GmresOptions(engine=2, **kw))
+    assert info.status == 0 and info.relres <= 1e-12
+    assert _rel(x, xl) <= SOL_RTOL
+    _, ref = p.solve(b, c1_hetero.T0, GmresOptions(engine=1, **kw))
+    assert abs(info.iters - ref.iters) <= max(3, ref.iters // 10)
+    with pytest.raises(VFVChemError):
+        p.solve(b, None, GmresOptions(engine=2, precond=1))
+
+
 def test_engines_agree(gpu_ctx, c1h_system, c1_hetero):
     """The persistent cycle kernel and the graph of per-phase kernels run the same arithmetic."""
     from vfvchem_vfvm3d_b200 import GmresOptions, Pattern

@@ -17,7 +17,7 @@ VFV_OK, VFV_NOT_CONVERGED, VFV_NONFINITE, VFV_BAD_INPUT, VFV_CUDA_ERROR, VFV_TIM
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_BJ4 = 0, 1, 2, 3
 FP64, MIXED = 0, 1
 ILU_MULTICOLOR, ILU_NATURAL = 0, 1
-ENGINE_PERSISTENT, ENGINE_GRAPH = 0, 1
+ENGINE_PERSISTENT, ENGINE_GRAPH, ENGINE_OVERLAP = 0, 1, 2
 BC_TEMP, BC_FLUX = 0, 1
 
 

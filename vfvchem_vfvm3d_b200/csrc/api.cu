@@ -465,25 +465,36 @@ int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
 // z = (LU)^-1 r: one launch per level, lower levels then upper levels in reverse, chained with
 // programmatic dependent launch. `in` and `out` may alias; `t` must not alias either.
 template <typename T, bool LOWER>
-cudaError_t launch_level(cudaStream_t s, const IluStruct& S, int l, bool pdl, const T* lu, const T* in, T* t, T* out, const DevStatus* st) {
+cudaError_t launch_level(cudaStream_t s, const IluStruct& S, int l, bool pdl, const T* lu, const T* in, T* t, T* out, const DevStatus* st,
+                         int prio = 0, bool use_prio = false) {
     const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)std::max(1, (r1 - r0 + kLevBlock - 1) / kLevBlock));
     cfg.blockDim = dim3(kLevBlock);
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = pdl ? attr : nullptr;
-    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchAttribute attr[2];
+    int na = 0;
+    if (pdl) {
+        attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    if (use_prio) {  // scheduled ahead of concurrently queued blocks of lower priority
+        attr[na].id = cudaLaunchAttributePriority;
+        attr[na].val.priority = prio;
+        ++na;
+    }
+    cfg.attrs = na ? attr : nullptr;
+    cfg.numAttrs = na;
     return cudaLaunchKernelEx(&cfg, k_ilu0_level<T, LOWER>, r0, r1, (const int32_t*)S.rp.p, (const int32_t*)S.ci.p, (const int32_t*)S.dg.p, lu,
                               (const int32_t*)S.perm.p, in, t, out, st);
 }
 
 template <typename T>
-void ilu_apply(cudaStream_t s, const IluStruct& S, const T* lu, const T* in, T* t, T* out, const DevStatus* st) {
-    for (int l = 0; l < S.nlev; ++l) launch_level<T, true>(s, S, l, l > 0, lu, in, t, out, st);
-    for (int l = S.nlev - 1; l >= 0; --l) launch_level<T, false>(s, S, l, true, lu, in, t, out, st);
+void ilu_apply(cudaStream_t s, const IluStruct& S, const T* lu, const T* in, T* t, T* out, const DevStatus* st, int prio = 0,
+               bool use_prio = false) {
+    for (int l = 0; l < S.nlev; ++l) launch_level<T, true>(s, S, l, l > 0, lu, in, t, out, st, prio, use_prio);
+    for (int l = S.nlev - 1; l >= 0; --l) launch_level<T, false>(s, S, l, true, lu, in, t, out, st, prio, use_prio);
 }
 
 template <typename T>
@@ -506,8 +517,17 @@ struct Gmres : SolverBase {
     int64_t graph_nodes = 0;
     IluStruct* ilu = nullptr;
     uint64_t bj_version = ~0ull;
+    // overlapped engine: preconditioned basis Z, SpMV output a, q = M^-1 a, the second stream
+    DBuf<T> Zb, abuf, qbuf;
+    DBuf<double> coefz;
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int ilu_prio = 0;  // greatest stream priority: the sweeps' blocks go first when SM slots free up
     ~Gmres() override {
         if (exec) cudaGraphExecDestroy(exec);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (s2) cudaStreamDestroy(s2);
     }
 
     int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_) {
@@ -525,6 +545,18 @@ struct Gmres : SolverBase {
             CK(z.alloc(n));
             CK(z2.alloc(n));
             CK(zc.alloc(n));
+        }
+        if (engine == VFV_ENGINE_OVERLAP) {
+            CK(Zb.alloc((size_t)(m + 1) * ldv));
+            CK(abuf.alloc(n));
+            CK(qbuf.alloc(n));
+            CK(coefz.alloc(kMaxBasis));
+            int lo = 0, hi = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            ilu_prio = hi;
+            CK(cudaStreamCreateWithPriority(&s2, cudaStreamNonBlocking, hi));
+            CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         }
         if (precond == VFV_PRECOND_BJ4) {
             if (n % 4 != 0) return set_err(ctx, VFV_BAD_INPUT, "block-Jacobi(4) needs a system of 4 fields of equal length");
@@ -586,6 +618,7 @@ struct Gmres : SolverBase {
         K.y = y.p;
         K.st = st.p;
         K.scal = scal.p;
+        K.coefz = coefz.p;
         if (precond == VFV_PRECOND_ILU0) {
             auto it = p->ilu.find(ilu_order);
             if (it == p->ilu.end()) {
@@ -665,10 +698,10 @@ struct Gmres : SolverBase {
         k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
         k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
         cudaEventRecord(ev[3], s);
-        k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+        k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
         k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
         cudaEventRecord(ev[4], s);
-        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
         cudaEventRecord(ev[5], s);
         cudaEventSynchronize(ev[5]);
         float t[5];
@@ -723,8 +756,38 @@ struct Gmres : SolverBase {
         return A;
     }
 
+    // Overlapped engine (ILU(0) only): flexible GMRES whose preconditioned vectors come by linearity,
+    // z_{j+1} = M^-1 w - sum_i c_i z_i, so the latency-bound ILU(0) sweeps of M^-1 w run on a second
+    // stream while the bandwidth-bound CGS2 passes orthogonalise w; the correction of x is Z y.
+    void enqueue_cycle_overlap(cudaStream_t s, vfv_pattern* p) {
+        constexpr int G = kSpG;
+        const T* vk = krylov_vals(p);
+        const int sp_blocks = grid_for(n * G);
+        ilu_apply<T>(s, *ilu, lu_vals(), V.p, z2.p, Zb.p, st.p);  // z_0 = M^-1 u_0
+        for (int j = 0; j < m; ++j) {
+            T* w = V.p + (int64_t)(j + 1) * ldv;
+            launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, Zb.p + (int64_t)j * ldv, abuf.p,
+                                    inv_beta.p + j, st.p);
+            cudaEventRecord(ev_fork, s);
+            cudaStreamWaitEvent(s2, ev_fork, 0);
+            ilu_apply<T>(s2, *ilu, lu_vals(), abuf.p, z2.p, qbuf.p, st.p, ilu_prio, true);
+            cudaEventRecord(ev_join, s2);
+            k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, abuf.p, j + 1);
+            k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
+            k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, abuf.p, w, j + 1, j);
+            k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
+            k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
+            cudaStreamWaitEvent(s, ev_join, 0);
+            k_zupdate<T><<<nblk, kBlk, 0, s>>>(K, Zb.p, qbuf.p, j + 1, j);
+        }
+        k_backsolve<<<1, 32, 0, s>>>(K);
+        k_combine<T, 0><<<grid_for(n), kBlk, 0, s>>>(K, Zb.p, x.p, nullptr, nullptr);
+        k_residual<T, G><<<sp_blocks, kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+    }
+
     // one restart cycle: m Arnoldi steps, least squares, update of x, new residual
     void enqueue_cycle(cudaStream_t s, vfv_pattern* p) {
+        if (engine == VFV_ENGINE_OVERLAP) return enqueue_cycle_overlap(s, p);
         constexpr int G = kSpG;
         const T* vk = krylov_vals(p);
         const int sp_blocks = grid_for(n * G);
@@ -742,9 +805,9 @@ struct Gmres : SolverBase {
             launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
             k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
             k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-            k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+            k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
             k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-            k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1, j);
+            k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
         }
         k_backsolve<<<1, 32, 0, s>>>(K);
         const int vb = grid_for(n);
@@ -841,7 +904,7 @@ struct Gmres : SolverBase {
         CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
         k_residual<T, G><<<grid_for(n * G), kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
         ctx->launches += 1;
-        if (engine == VFV_ENGINE_GRAPH && !exec) {
+        if (engine != VFV_ENGINE_PERSISTENT && !exec) {
             cudaGraph_t graph;
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             enqueue_cycle(s, p);
@@ -883,7 +946,7 @@ struct Gmres : SolverBase {
                 rc = VFV_NOT_CONVERGED;
                 break;
             }
-            if (engine == VFV_ENGINE_GRAPH) {
+            if (engine != VFV_ENGINE_PERSISTENT) {
                 CK(cudaGraphLaunch(exec, s));
                 ctx->launches += graph_nodes;
             } else {
@@ -932,7 +995,10 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
         return set_err(ctx, VFV_BAD_INPUT, "block-Jacobi(4) runs on the graph engine only");
     if (o->precision != VFV_FP64 && o->precision != VFV_MIXED) return set_err(ctx, VFV_BAD_INPUT, "unknown precision");
     if (o->ilu_order != VFV_ILU_MULTICOLOR && o->ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
-    if (o->engine != VFV_ENGINE_PERSISTENT && o->engine != VFV_ENGINE_GRAPH) return set_err(ctx, VFV_BAD_INPUT, "unknown engine");
+    if (o->engine != VFV_ENGINE_PERSISTENT && o->engine != VFV_ENGINE_GRAPH && o->engine != VFV_ENGINE_OVERLAP)
+        return set_err(ctx, VFV_BAD_INPUT, "unknown engine");
+    if (o->engine == VFV_ENGINE_OVERLAP && o->precond != VFV_PRECOND_ILU0)
+        return set_err(ctx, VFV_BAD_INPUT, "the overlapped engine needs the ILU(0) preconditioner");
     return VFV_OK;
 }
 

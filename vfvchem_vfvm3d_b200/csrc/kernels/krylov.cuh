@@ -36,6 +36,7 @@ struct KrylovDev {
     unsigned* counter;  // [4] last-block counters
     double* hacc;       // [kMaxBasis] current Hessenberg column (accumulated over the CGS passes)
     double* coef;       // [kMaxBasis] update coefficients d_i / beta_i^2
+    double* coefz;      // [kMaxBasis] both CGS passes' coefficients summed (overlapped engine), or null
     double* H;          // [m][m+1] column-major Hessenberg (rotated in place)
     double* cs;         // [m]
     double* sn;         // [m]
@@ -257,17 +258,19 @@ __global__ void __launch_bounds__(256) k_dots_finish(KrylovDev K, int nvec) {
         const double ib = K.inv_beta[c];
         if (FIRST) K.hacc[c] = s * ib;
         else K.hacc[c] += s * ib;
-        K.coef[c] = s * ib * ib;
+        const double cf = s * ib * ib;
+        K.coef[c] = cf;
+        if (K.coefz) K.coefz[c] = FIRST ? cf : K.coefz[c] + cf;
     }
 }
 
 // ---------------------------------------------------------------- update + second pass
-// w <- w - sum_i coef_i u_i. Then, with FINAL == false, the partials of the second CGS pass
+// w <- win - sum_i coef_i u_i (win == w except in the overlapped engine). Then, with FINAL == false, the partials of the second CGS pass
 // d'_i = <u_i, w> (k_dots_finish<false> adds d'_i/beta_i into hacc and sets coef); with
 // FINAL == true, ||w||^2 and the last block finishes the Hessenberg column j, the Givens rotation
 // and the convergence test.
 template <typename T, bool FINAL>
-__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, const T* __restrict__ V, T* __restrict__ w, int nvec, int j) {
+__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, const T* __restrict__ V, const T* win, T* w, int nvec, int j) {
     if (K.st->done) return;
     __shared__ double red[kMaxBasis][kBlk / 32];
     __shared__ double red2[kBlk / 32];
@@ -296,7 +299,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, con
     for (int r = 0; r < kRows; ++r) {
         const int64_t row = base + r * kBlk;
         if (row < K.n) {
-            const T nv = (T)((double)w[row] - acc[r]);
+            const T nv = (T)((double)win[row] - acc[r]);
             w[row] = nv;
             wr[r] = (double)nv;
         } else {
@@ -373,6 +376,37 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, con
 
 // ---------------------------------------------------------------- end of cycle
 // Back substitution R y = g on the rotated Hessenberg (k = steps), y_i scaled by 1/beta_i.
+// Overlapped engine: the preconditioned image of the new basis vector by linearity,
+// z_{j+1} = M^-1 (w - sum_i c_i u_i) = q - sum_i c_i z_i with q = M^-1 w computed concurrently
+// with the orthogonalisation and c_i the sum of both CGS passes' coefficients.
+template <typename T>
+__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_zupdate(KrylovDev K, T* Z, const T* __restrict__ q, int nvec, int j) {
+    if (K.st->done) return;
+    __shared__ double s_c[kMaxBasis];
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) s_c[i] = K.coefz[i];
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * (kBlk * kRows) + threadIdx.x;
+    double acc[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) acc[r] = 0.0;
+#pragma unroll 4
+    for (int i = 0; i < nvec; ++i) {
+        const T* z = Z + (int64_t)i * K.ldv;
+        const double c = s_c[i];
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+            const int64_t row = base + r * kBlk;
+            if (row < K.n) acc[r] += c * (double)z[row];
+        }
+    }
+    T* out = Z + (int64_t)(j + 1) * K.ldv;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+        const int64_t row = base + r * kBlk;
+        if (row < K.n) out[row] = (T)((double)q[row] - acc[r]);
+    }
+}
+
 __global__ void k_backsolve(KrylovDev K) {
     if (threadIdx.x != 0) return;
     const int k = K.st->steps;
