@@ -497,6 +497,11 @@ void ilu_apply(cudaStream_t s, const IluStruct& S, const T* lu, const T* in, T* 
     for (int l = S.nlev - 1; l >= 0; --l) launch_level<T, false>(s, S, l, true, lu, in, t, out, st, prio, use_prio);
 }
 
+constexpr int kStepsPerIf = 4;  // Arnoldi steps per IF node of a cycle graph
+
+// Sets the IF condition of the next group of Arnoldi steps of a cycle graph: run it unless the solve stopped.
+__global__ void k_step_condition(cudaGraphConditionalHandle h, const DevStatus* st) { cudaGraphSetConditional(h, st->done ? 0u : 1u); }
+
 template <typename T>
 struct Gmres : SolverBase {
     int64_t n = 0, ldv = 0;
@@ -514,7 +519,9 @@ struct Gmres : SolverBase {
     DBuf<DevStatus> st;
     KrylovDev K{};
     cudaGraphExec_t exec = nullptr;
-    int64_t graph_nodes = 0;
+    int64_t graph_nodes = 0, step_nodes = 0;
+    bool pending_steps = false;
+    int steps_seen = 0;
     IluStruct* ilu = nullptr;
     uint64_t bj_version = ~0ull;
     // overlapped engine: preconditioned basis Z, SpMV output a, q = M^-1 a, the second stream
@@ -756,18 +763,21 @@ struct Gmres : SolverBase {
         return A;
     }
 
+    // One restart cycle = prologue, m Arnoldi steps, epilogue (least squares, update of x, new residual).
+    //
     // Overlapped engine (ILU(0) only): flexible GMRES whose preconditioned vectors come by linearity,
     // z_{j+1} = M^-1 w - sum_i c_i z_i, so the latency-bound ILU(0) sweeps of M^-1 w run on a second
     // stream while the bandwidth-bound CGS2 passes orthogonalise w; the correction of x is Z y.
-    void enqueue_cycle_overlap(cudaStream_t s, vfv_pattern* p) {
-        constexpr int G = kSpG;
+    void enqueue_prologue(cudaStream_t s) {
+        if (engine == VFV_ENGINE_OVERLAP) ilu_apply<T>(s, *ilu, lu_vals(), V.p, z2.p, Zb.p, st.p);  // z_0 = M^-1 u_0
+    }
+
+    void enqueue_step(cudaStream_t s, vfv_pattern* p, int j) {
         const T* vk = krylov_vals(p);
-        const int sp_blocks = grid_for(n * G);
-        ilu_apply<T>(s, *ilu, lu_vals(), V.p, z2.p, Zb.p, st.p);  // z_0 = M^-1 u_0
-        for (int j = 0; j < m; ++j) {
-            T* w = V.p + (int64_t)(j + 1) * ldv;
-            launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, Zb.p + (int64_t)j * ldv, abuf.p,
-                                    inv_beta.p + j, st.p);
+        const int lanes = p->spmv_lanes[sizeof(T) == 8 ? 0 : 1];
+        T* w = V.p + (int64_t)(j + 1) * ldv;
+        if (engine == VFV_ENGINE_OVERLAP) {
+            launch_spmv<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, Zb.p + (int64_t)j * ldv, abuf.p, inv_beta.p + j, st.p);
             cudaEventRecord(ev_fork, s);
             cudaStreamWaitEvent(s2, ev_fork, 0);
             ilu_apply<T>(s2, *ilu, lu_vals(), abuf.p, z2.p, qbuf.p, st.p, ilu_prio, true);
@@ -779,39 +789,33 @@ struct Gmres : SolverBase {
             k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
             cudaStreamWaitEvent(s, ev_join, 0);
             k_zupdate<T><<<nblk, kBlk, 0, s>>>(K, Zb.p, qbuf.p, j + 1, j);
+            return;
         }
-        k_backsolve<<<1, 32, 0, s>>>(K);
-        k_combine<T, 0><<<grid_for(n), kBlk, 0, s>>>(K, Zb.p, x.p, nullptr, nullptr);
-        k_residual<T, G><<<sp_blocks, kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+        const T* uj = V.p + (int64_t)j * ldv;
+        const T* in = uj;
+        if (precond == VFV_PRECOND_ILU0) {
+            ilu_apply<T>(s, *ilu, lu_vals(), uj, z2.p, z.p, st.p);
+            in = z.p;
+        } else if (precond == VFV_PRECOND_BJ4) {
+            k_bj4_apply<T><<<grid_for(n / 4), 256, 0, s>>>(n / 4, bj_vals(), uj, z.p, st.p);
+            in = z.p;
+        }
+        launch_spmv<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
+        k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
+        k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
+        k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
+        k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
+        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
     }
 
-    // one restart cycle: m Arnoldi steps, least squares, update of x, new residual
-    void enqueue_cycle(cudaStream_t s, vfv_pattern* p) {
-        if (engine == VFV_ENGINE_OVERLAP) return enqueue_cycle_overlap(s, p);
+    void enqueue_epilogue(cudaStream_t s, vfv_pattern* p) {
         constexpr int G = kSpG;
-        const T* vk = krylov_vals(p);
         const int sp_blocks = grid_for(n * G);
-        for (int j = 0; j < m; ++j) {
-            const T* uj = V.p + (int64_t)j * ldv;
-            T* w = V.p + (int64_t)(j + 1) * ldv;
-            const T* in = uj;
-            if (precond == VFV_PRECOND_ILU0) {
-                ilu_apply<T>(s, *ilu, lu_vals(), uj, z2.p, z.p, st.p);
-                in = z.p;
-            } else if (precond == VFV_PRECOND_BJ4) {
-                k_bj4_apply<T><<<grid_for(n / 4), 256, 0, s>>>(n / 4, bj_vals(), uj, z.p, st.p);
-                in = z.p;
-            }
-            launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
-            k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
-            k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-            k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
-            k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-            k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
-        }
         k_backsolve<<<1, 32, 0, s>>>(K);
         const int vb = grid_for(n);
-        if (precond == VFV_PRECOND_ILU0) {
+        if (engine == VFV_ENGINE_OVERLAP) {
+            k_combine<T, 0><<<vb, kBlk, 0, s>>>(K, Zb.p, x.p, nullptr, nullptr);
+        } else if (precond == VFV_PRECOND_ILU0) {
             k_combine<T, 2><<<vb, kBlk, 0, s>>>(K, V.p, x.p, nullptr, z.p);
             ilu_apply<T>(s, *ilu, lu_vals(), z.p, z2.p, z.p, nullptr);  // out may alias in: the upper sweep starts after the lower one
             k_add_to_x<T><<<vb, 256, 0, s>>>(n, x.p, z.p);
@@ -825,6 +829,104 @@ struct Gmres : SolverBase {
             k_combine<T, 0><<<vb, kBlk, 0, s>>>(K, V.p, x.p, nullptr, nullptr);
         }
         k_residual<T, G><<<sp_blocks, kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+    }
+
+    // The whole cycle, captured as one straight graph (every step's kernels return at once once the
+    // device `done` flag is set).
+    void enqueue_cycle(cudaStream_t s, vfv_pattern* p) {
+        enqueue_prologue(s);
+        for (int j = 0; j < m; ++j) enqueue_step(s, p, j);
+        enqueue_epilogue(s, p);
+    }
+
+    // Appends what `fn` enqueues on s to graph g after the nodes `deps`; returns the new frontier.
+    template <typename F>
+    cudaError_t capture_into(cudaStream_t s, cudaGraph_t g, std::vector<cudaGraphNode_t>& deps, F fn) {
+        cudaError_t e = cudaStreamBeginCaptureToGraph(s, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                                      cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            if (const char* t = getenv("VFV_TRACE_SOLVE"))
+                if (t[0] == '1') fprintf(stderr, "[vfv] begin capture to graph: %s (deps %zu)\n", cudaGetErrorString(e), deps.size());
+            return e;
+        }
+        fn();
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t* nd = nullptr;
+        size_t nn = 0;
+        cudaError_t e2 = cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &nd, &nn);
+        if (e2 != cudaSuccess)
+            if (const char* t = getenv("VFV_TRACE_SOLVE"))
+                if (t[0] == '1') fprintf(stderr, "[vfv] capture info: %s\n", cudaGetErrorString(e2));
+        std::vector<cudaGraphNode_t> front(nd, nd + (e2 == cudaSuccess ? nn : 0));
+        cudaGraph_t out = nullptr;
+        e = cudaStreamEndCapture(s, &out);
+        if (e2 != cudaSuccess) return e2;
+        if (e != cudaSuccess) return e;
+        deps.swap(front);
+        return cudaSuccess;
+    }
+
+    // The cycle as a graph whose Arnoldi steps sit in IF nodes, kStepsPerIf steps per node: a
+    // one-thread kernel before each node sets the condition from the device `done` flag, so the
+    // groups after convergence cost one tiny launch each instead of ~25 kernels per step (a step of
+    // a running group that finds the solve done still returns at once, as in the straight graph). Returns an error (and leaves no graph) where the
+    // driver cannot build it; the caller then captures the straight graph.
+    cudaError_t build_conditional_graph(cudaStream_t s, vfv_pattern* p, cudaGraph_t* out, int64_t* top_nodes, int64_t* step_nodes) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaGraphCreate(&g, 0);
+        if (e != cudaSuccess) return e;
+        std::vector<cudaGraphNode_t> deps;
+        int64_t body_nodes = 0;
+        const char* stage = "prologue";
+        e = capture_into(s, g, deps, [&] { enqueue_prologue(s); });
+        for (int j0 = 0; j0 < m && e == cudaSuccess; j0 += kStepsPerIf) {
+            const int j1 = std::min(m, j0 + kStepsPerIf);
+            stage = "handle";  // one handle per conditional node
+            cudaGraphConditionalHandle h;
+            e = cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault);
+            if (e != cudaSuccess) break;
+            stage = "condition kernel";
+            e = capture_into(s, g, deps, [&] { k_step_condition<<<1, 1, 0, s>>>(h, st.p); });
+            if (e != cudaSuccess) break;
+            stage = "conditional node";
+            cudaGraphNodeParams np{};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h;
+            np.conditional.type = cudaGraphCondTypeIf;
+            np.conditional.size = 1;
+            cudaGraphNode_t cn;
+            e = cudaGraphAddNode(&cn, g, deps.empty() ? nullptr : deps.data(), deps.size(), &np);
+            if (e != cudaSuccess) break;
+            cudaGraph_t body = np.conditional.phGraph_out[0];
+            std::vector<cudaGraphNode_t> none;
+            stage = "step body";
+            e = capture_into(s, body, none, [&] {
+                for (int j = j0; j < j1; ++j) enqueue_step(s, p, j);
+            });
+            if (e == cudaSuccess && j0 == 0) {
+                size_t bn = 0;
+                e = cudaGraphGetNodes(body, nullptr, &bn);
+                body_nodes = (int64_t)bn / (j1 - j0);
+            }
+            deps.assign(1, cn);
+        }
+        if (e == cudaSuccess) {
+            stage = "epilogue";
+            e = capture_into(s, g, deps, [&] { enqueue_epilogue(s, p); });
+        }
+        if (e != cudaSuccess) {
+            if (const char* t = getenv("VFV_TRACE_SOLVE"))
+                if (t[0] == '1') fprintf(stderr, "[vfv] conditional cycle graph not built (%s, %zu dependencies): %s\n", stage, deps.size(), cudaGetErrorString(e));
+            cudaGraphDestroy(g);
+            cudaGetLastError();
+            return e;
+        }
+        size_t tn = 0;
+        cudaGraphGetNodes(g, nullptr, &tn);
+        *out = g;
+        *top_nodes = (int64_t)tn;
+        *step_nodes = body_nodes;
+        return cudaSuccess;
     }
 
     // nblk > 0: block-diagonal system with block row ranges blk_d[0..nblk] (device); converged
@@ -905,23 +1007,47 @@ struct Gmres : SolverBase {
         k_residual<T, G><<<grid_for(n * G), kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
         ctx->launches += 1;
         if (engine != VFV_ENGINE_PERSISTENT && !exec) {
-            cudaGraph_t graph;
-            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            enqueue_cycle(s, p);
-            CK(cudaStreamEndCapture(s, &graph));
-            size_t nodes = 0;
-            CK(cudaGraphGetNodes(graph, nullptr, &nodes));
-            graph_nodes = (int64_t)nodes;
-            cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-            cudaGraphDestroy(graph);
-            CK(e);
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaErrorUnknown;
+            if (!getenv("VFV_STRAIGHT_GRAPH")) {  // conditional steps unless asked for the straight graph
+                e = build_conditional_graph(s, p, &graph, &graph_nodes, &step_nodes);
+                if (e == cudaSuccess) {
+                    e = cudaGraphInstantiate(&exec, graph, 0);
+                    cudaGraphDestroy(graph);
+                    if (e != cudaSuccess) {
+                        if (const char* t = getenv("VFV_TRACE_SOLVE"))
+                            if (t[0] == '1') fprintf(stderr, "[vfv] conditional cycle graph not instantiated: %s\n", cudaGetErrorString(e));
+                        exec = nullptr;
+                        cudaGetLastError();
+                    }
+                }
+            }
+            if (e != cudaSuccess) {
+                step_nodes = 0;
+                CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                enqueue_cycle(s, p);
+                CK(cudaStreamEndCapture(s, &graph));
+                size_t nodes = 0;
+                CK(cudaGraphGetNodes(graph, nullptr, &nodes));
+                graph_nodes = (int64_t)nodes;
+                e = cudaGraphInstantiate(&exec, graph, 0);
+                cudaGraphDestroy(graph);
+                CK(e);
+            }
         }
         int cycles = 0, rc = VFV_OK;
+        steps_seen = 0;
+        pending_steps = false;
         DevStatus hst{};
         for (;;) {
             CK(cudaMemcpyAsync(ctx->h_status, st.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
             hst = *ctx->h_status;
+            if (pending_steps) {
+                ctx->launches += step_nodes * (int64_t)(hst.total_steps - steps_seen);
+                pending_steps = false;
+            }
+            steps_seen = hst.total_steps;
             if (hst.timeout) {
                 rc = VFV_TIMEOUT;
                 CK(cudaMemsetAsync(bar.p, 0, 2 * kGenOffset * sizeof(unsigned), s));  // barrier state is undefined after a timeout
@@ -948,7 +1074,10 @@ struct Gmres : SolverBase {
             }
             if (engine != VFV_ENGINE_PERSISTENT) {
                 CK(cudaGraphLaunch(exec, s));
+                // straight graph: every node launches; conditional graph: the top-level nodes, plus
+                // the bodies of the steps run (counted when the cycle's status comes back)
                 ctx->launches += graph_nodes;
+                pending_steps = step_nodes > 0;
             } else {
                 CycleArgs A = cycle_args(p);
                 void* args[] = {&A};
