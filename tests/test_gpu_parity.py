@@ -223,6 +223,26 @@ def test_overlap_engine_matches_lu(gpu_ctx, c1h_system, c1_hetero, precision, or
         p.solve(b, None, GmresOptions(engine=2, precond=1))
 
 
+@pytest.mark.parametrize("engine", [1, 2])
+def test_conditional_and_straight_cycle_graphs_agree(gpu_ctx, c1h_system, c1_hetero, engine, monkeypatch):
+    """The cycle graph with IF nodes over groups of steps and the straight graph (VFV_STRAIGHT_GRAPH)
+    run the same kernels in the same order: identical iterates."""
+    from vfvchem_vfvm3d_b200 import GmresOptions, Pattern
+    (rp, ci, va), b, _ = c1h_system
+    out = []
+    for straight in (False, True):
+        if straight:
+            monkeypatch.setenv("VFV_STRAIGHT_GRAPH", "1")
+        else:
+            monkeypatch.delenv("VFV_STRAIGHT_GRAPH", raising=False)
+        p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)  # a new pattern builds its own graph
+        p.set_values(va)
+        out.append(p.solve(b, c1_hetero.T0, GmresOptions(tol=1e-11, restart=30, max_outer=500, precond=2, engine=engine)))
+    monkeypatch.delenv("VFV_STRAIGHT_GRAPH", raising=False)
+    assert out[0][1].iters == out[1][1].iters
+    assert np.array_equal(out[0][0], out[1][0])
+
+
 def test_engines_agree(gpu_ctx, c1h_system, c1_hetero):
     """The persistent cycle kernel and the graph of per-phase kernels run the same arithmetic."""
     from vfvchem_vfvm3d_b200 import GmresOptions, Pattern
