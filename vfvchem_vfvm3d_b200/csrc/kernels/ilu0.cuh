@@ -70,8 +70,10 @@ __global__ void k_cast(int64_t n, const TS* __restrict__ in, TD* __restrict__ ou
 // (griddepcontrol.wait) before gathering solved values. The next level's prologue therefore
 // overlaps this level's gathers instead of following them.
 constexpr int kLevBlock = 128;
-constexpr int kLevMinBlocks = 12;  // <= 42 registers: a level leaves room on every SM for the next one
-constexpr int kLevK = 8;           // entries of a row held in registers before the wait
+constexpr int kLevMinBlocks = 8;   // <= 64 registers: a ~100k-row level (~780 blocks) is one wave
+constexpr int kLevK = 16;          // entries of a row held in registers before the wait: rows of the
+                                   // late colours hold up to ~15 lower (early colours: upper) entries,
+                                   // and every entry left to the loop costs a dependent round trip
 
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
