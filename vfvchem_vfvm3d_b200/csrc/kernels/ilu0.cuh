@@ -96,6 +96,9 @@ __global__ void __launch_bounds__(kLevBlock, kLevMinBlocks) k_ilu0_level(int32_t
         ke = LOWER ? d : __ldg(rp + i + 1);
         pi = __ldg(perm + i);
         if (!LOWER) diag = __ldg(lu + d);
+        // the lower sweep's right-hand side is complete before the sweep's first (non-PDL) launch,
+        // so it is read before the wait; the upper sweep's comes from the lower sweep (after it)
+        if (LOWER) rhs = in[pi];
 #pragma unroll
         for (int q = 0; q < kLevK; ++q) {
             c[q] = kb + q < ke ? __ldg(ci + kb + q) : -1;
@@ -105,8 +108,7 @@ __global__ void __launch_bounds__(kLevBlock, kLevMinBlocks) k_ilu0_level(int32_t
     pdl_launch_dependents();
     pdl_wait();
     if (i >= r1 || (st && st->done)) return;
-    if (LOWER) rhs = in[pi];
-    else rhs = t[i];
+    if (!LOWER) rhs = t[i];
     T s = T(0);
 #pragma unroll
     for (int q = 0; q < kLevK; ++q)
