@@ -1,13 +1,12 @@
-// C ABI of libvfvgpu: contexts, sparse patterns, the graph-captured GMRES driver, mesh and heat
-// operator handles. Host orchestration only; the kernels live in kernels/*.
+// C ABI of libvfvgpu: contexts, sparse patterns, ILU(0) orderings and the graph-captured GMRES
+// driver. The operator handles live in heat_api.cu, transport_api.cu, flow_api.cu and mesh_api.cu;
+// host orchestration only, the kernels live in kernels/*.
 //
 // Reference interfaces mirrored (src/linear/linear_base.rs:5-10, src/linear/linear_gmres.rs:8-85):
 //   update_sparse -> vfv_pattern_from_triplets (sorted de-duplicated pattern + slot map, once)
 //   build_matrix  -> vfv_values_from_triplets  (device scatter summing duplicates in push order)
 //   solve_matrix  -> vfv_solve                 (restarted right-preconditioned GMRES, warm start)
-#include "../../include/vfv_gpu.h"
-#include "common.cuh"
-#include "host/mesh.hpp"
+#include "internal.cuh"
 #include "kernels/adjoint.cuh"
 #include "kernels/assemble.cuh"
 #include "kernels/ilu0.cuh"
@@ -29,63 +28,13 @@
 #include <type_traits>
 #include <vector>
 
-using namespace vfv;
-
 // ================================================================ errors / buffers
-static thread_local std::string g_err;
-
-struct vfv_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    DevStatus* h_status = nullptr;  // pinned
-    double* h_scalar = nullptr;     // pinned scratch for small reads
-    int64_t launches = 0;           // kernels launched by this context (graph nodes counted per replay)
-};
-
-namespace {
-
-int set_err(vfv_ctx* ctx, int code, const std::string& msg) {
-    if (ctx) ctx->err = msg;
-    g_err = msg;
-    return code;
+std::string& vfv_thread_error() {
+    static thread_local std::string e;
+    return e;
 }
 
-#define CK(call)                                                                                           \
-    do {                                                                                                   \
-        cudaError_t e_ = (call);                                                                           \
-        if (e_ != cudaSuccess) return set_err(ctx, VFV_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-template <typename T>
-struct DBuf {  // device buffer, freed with its owner
-    T* p = nullptr;
-    size_t n = 0;
-    DBuf() = default;
-    DBuf(const DBuf&) = delete;
-    DBuf& operator=(const DBuf&) = delete;
-    ~DBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    cudaError_t alloc(size_t count) {
-        release();
-        n = count;
-        if (count == 0) return cudaSuccess;
-        return cudaMalloc(&p, count * sizeof(T));
-    }
-    cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
-        cudaError_t e = alloc(count);
-        if (e != cudaSuccess || count == 0) return e;
-        e = cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) return e;
-        return cudaStreamSynchronize(s);
-    }
-};
-
-inline int grid_for(int64_t threads, int block = 256) { return (int)std::max<int64_t>(1, (threads + block - 1) / block); }
+namespace {
 
 // LSD radix sort of (key, index) by key, stable; keys < 2^bits.
 void radix_sort_pairs(std::vector<uint64_t>& key, std::vector<int64_t>& idx, int bits) {
@@ -107,44 +56,6 @@ void radix_sort_pairs(std::vector<uint64_t>& key, std::vector<int64_t>& idx, int
 }
 
 }  // namespace
-
-// ================================================================ ILU structure (host-built)
-struct IluStruct {
-    int order = -1;
-    int nlev = 0;
-    std::vector<int32_t> lev_ptr;  // [nlev+1] row ranges in the permuted numbering
-    std::vector<int32_t> h_perm;   // new -> old
-    DBuf<int32_t> d_lev_ptr;       // same, on the device (read by the cycle kernel)
-    DBuf<int32_t> perm, rp, ci, dg, src;
-    DBuf<double> lu64;
-    DBuf<float> lu32;
-    DBuf<int> bad;
-
-
-    uint64_t version64 = ~0ull, version32 = ~0ull;
-};
-
-struct SolverBase {
-    virtual ~SolverBase() = default;
-};
-
-struct vfv_pattern {
-    vfv_ctx* ctx = nullptr;
-    int64_t n = 0, nnz = 0, ntrip = 0;
-    int spmv_lanes[2] = {kSpG, kSpG};  // lanes per row of the SpMV for double / float values (autotuned)
-    std::vector<int32_t> h_rp, h_ci;
-    DBuf<int32_t> rp, ci, diag_pos;
-    DBuf<double> val;
-    DBuf<float> val32;
-    uint64_t version = 0, version32 = ~0ull;
-    DBuf<int64_t> slot_ptr, slot_trip;
-    DBuf<double> trip_vals;
-    std::vector<int64_t> blocks;          // row ranges of the diagonal blocks of a block-diagonal system (may be empty)
-    const vfv_pattern* same_as = nullptr;  // a pattern with identical rows/columns (ILU orderings are shared)
-    std::map<int, std::unique_ptr<IluStruct>> ilu;
-    std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<SolverBase>> solvers;
-    DBuf<double> tmp_b, tmp_x;  // staging for host-pointer solves
-};
 
 // ================================================================ GMRES driver
 namespace {
@@ -1114,6 +1025,8 @@ struct Gmres : SolverBase {
     }
 };
 
+}  // namespace
+
 int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
     if (!o) return set_err(ctx, VFV_BAD_INPUT, "opts is NULL");
     if (!(o->tol > 0.0)) return set_err(ctx, VFV_BAD_INPUT, "tol must be positive (LinearGmresNonPositiveTolerance)");
@@ -1132,7 +1045,7 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
 }
 
 int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info,
-              int nblk = 0, const int64_t* blk_d = nullptr) {
+              int nblk, const int64_t* blk_d) {
     const auto key = std::make_tuple(o->precision, o->precond, o->precond == VFV_PRECOND_ILU0 ? o->ilu_order : 0, o->restart, o->engine);
     auto it = p->solvers.find(key);
     if (it == p->solvers.end()) {
@@ -1153,6 +1066,8 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
     if (o->precision == VFV_MIXED) return static_cast<Gmres<float>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info, nblk, blk_d);
     return static_cast<Gmres<double>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info, nblk, blk_d);
 }
+
+namespace {
 
 int finish_pattern(vfv_ctx* ctx, vfv_pattern* p) {
     const int64_t n = p->n;
@@ -1198,73 +1113,14 @@ int make_transpose(vfv_ctx* ctx, const vfv_pattern* p, vfv_pattern** out, DBuf<i
     return VFV_OK;
 }
 
-// ================================================================ mesh / heat handles
-struct vfv_mesh {
-    Mesh m;
-    Dual d;
-};
-
-struct vfv_heat {
-    vfv_ctx* ctx = nullptr;
-    int64_t n = 0, n_dir = 0, n_bsub = 0;
-    DBuf<int32_t> np, ni, kind, node_bnd, bp, bj, bk, dloc;
-    DBuf<double> area, dist, skew, gw, cvol, cskew, barea, bw;
-    DBuf<double> f, grad, b;  // f: [5][n] = k, q, s, T, bc_val ; grad: [4][3][n]
-    vfv_pattern* pat = nullptr;
-    // adjoint (built on first use): transpose pattern, value map, reverse faces, work arrays
-    vfv_pattern* pat_t = nullptr;
-    DBuf<int32_t> tmap, rev;
-    DBuf<double> adj_work;  // pv, pn [n_dir]; sk [3 n_dir]; gkm [n]; psi [3 n]; T, g, lambda, zero, dlogk, dq [n]
-    std::vector<int32_t> h_rev;
-    ~vfv_heat() {
-        delete pat_t;
-        delete pat;
-    }
-};
-
-// Concatenation of several meshes into one block-diagonal transport system (config 4).
-struct vfv_transport {
-    vfv_ctx* ctx = nullptr;
-    int nmesh = 0;
-    int64_t n = 0, n_dir = 0;
-    double dt = 0.0;
-    std::vector<int64_t> row_ptr;  // [nmesh+1] vertex (row) offsets of the meshes
-    DBuf<int64_t> d_row_ptr;
-    DBuf<int32_t> np, ni, dloc;
-    DBuf<double> area, dist, skew, norm, gw, cvol, flux, fields, grads, b, c0, c1;
-    vfv_pattern* pat = nullptr;
-    // transient adjoint: transpose pattern and work space
-    vfv_pattern* pat_t = nullptr;
-    DBuf<int32_t> tmap;
-    DBuf<double> adj;        // checkpoints, one segment of states, two adjoint vectors, rhs, zero, partials, terms
-    DBuf<unsigned> adj_counter;
-    TransportDev dev() const {
-        TransportDev T{};
-        T.n = n;
-        T.n_dir = n_dir;
-        T.np = np.p;
-        T.ni = ni.p;
-        T.area = area.p;
-        T.dist = dist.p;
-        T.skew = skew.p;
-        T.norm = norm.p;
-        T.cvol = cvol.p;
-        T.rp = pat->rp.p;
-        T.dloc = dloc.p;
-        T.D = fields.p;
-        T.gD = grads.p;
-        T.vel = fields.p + n;
-        T.gvel = grads.p + 3 * n;
-        T.flux = flux.p;
-        T.dt = dt;
-        T.val = pat->val.p;
-        return T;
-    }
-    ~vfv_transport() {
-        delete pat_t;
-        delete pat;
-    }
-};
+// values of A^T into its pattern: a gather of A's through the transpose map
+int gather_transpose_values(vfv_ctx* ctx, const vfv_pattern* p, vfv_pattern* pt, const int32_t* tmap) {
+    k_gather_vals<double><<<grid_for(p->nnz), 256, 0, ctx->stream>>>(p->nnz, tmap, p->val.p, pt->val.p);
+    ctx->launches += 1;
+    pt->version++;
+    CK(cudaGetLastError());
+    return VFV_OK;
+}
 
 // ================================================================ C ABI
 extern "C" {
@@ -1311,7 +1167,7 @@ void vfv_ctx_destroy(vfv_ctx* ctx) {
     delete ctx;
 }
 
-const char* vfv_last_error(const vfv_ctx* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+const char* vfv_last_error(const vfv_ctx* ctx) { return ctx ? ctx->err.c_str() : vfv_thread_error().c_str(); }
 
 int vfv_ctx_synchronize(vfv_ctx* ctx) {
     if (!ctx) return set_err(nullptr, VFV_BAD_INPUT, "ctx is NULL");
@@ -1639,901 +1495,6 @@ int vfv_ilu0_ordering(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int32_t* perm
     if (nlev) *nlev = S.nlev;
     if (perm) std::memcpy(perm, S.h_perm.data(), S.h_perm.size() * sizeof(int32_t));
     if (lev_ptr) std::memcpy(lev_ptr, S.lev_ptr.data(), S.lev_ptr.size() * sizeof(int32_t));
-    return VFV_OK;
-}
-
-// ---------------------------------------------------------------- mesh
-static int mesh_finish(vfv_mesh* mh, vfv_mesh** out) {
-    std::string e = delaunay(mh->m);
-    if (e.empty()) e = build_dual(mh->m, mh->d);
-    if (!e.empty()) {
-        delete mh;
-        return set_err(nullptr, VFV_BAD_INPUT, e);
-    }
-    *out = mh;
-    return VFV_OK;
-}
-
-int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out) {
-    if (!out) return set_err(nullptr, VFV_BAD_INPUT, "out is NULL");
-    *out = nullptr;
-    if (n < 3 || n > 400) return set_err(nullptr, VFV_BAD_INPUT, "grid size n must be in [3, 400]");
-    if (!(jitter >= 0.0 && jitter < 0.5)) return set_err(nullptr, VFV_BAD_INPUT, "jitter must be in [0, 0.5)");
-    auto* mh = new vfv_mesh();
-    mh->m = make_jitter_cube(n, seed, jitter);
-    return mesh_finish(mh, out);
-}
-
-int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out) {
-    if (!out || !pos || (n_nds > 0 && !node_bnd)) return set_err(nullptr, VFV_BAD_INPUT, "NULL argument");
-    *out = nullptr;
-    if (n_pts < 0 || n_nds < 0 || n_pts + n_nds < 4) return set_err(nullptr, VFV_BAD_INPUT, "need at least four vertices");
-    auto* mh = new vfv_mesh();
-    mh->m.n_pts = n_pts;
-    mh->m.n_nds = n_nds;
-    mh->m.pos.assign(pos, pos + 3 * (n_pts + n_nds));
-    mh->m.node_bnd.assign(node_bnd, node_bnd + n_nds);
-    return mesh_finish(mh, out);
-}
-
-void vfv_mesh_destroy(vfv_mesh* m) { delete m; }
-
-int vfv_mesh_jitter_cubes(int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out) {
-    if (count <= 0 || !n || !seeds || !out) return set_err(nullptr, VFV_BAD_INPUT, "invalid batch arguments");
-    for (int i = 0; i < count; ++i) {
-        out[i] = nullptr;
-        if (n[i] < 3 || n[i] > 400) return set_err(nullptr, VFV_BAD_INPUT, "grid size n must be in [3, 400]");
-    }
-    if (!(jitter >= 0.0 && jitter < 0.5)) return set_err(nullptr, VFV_BAD_INPUT, "jitter must be in [0, 0.5)");
-    std::vector<std::string> errs(count);
-    // meshes in parallel (largest first); the per-mesh OpenMP loops run serially inside
-    std::vector<int> order(count);
-    for (int i = 0; i < count; ++i) order[i] = i;
-    std::sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int t = 0; t < count; ++t) {
-        const int i = order[t];
-        auto* mh = new vfv_mesh();
-        mh->m = make_jitter_cube(n[i], seeds[i], jitter);
-        std::string e = delaunay(mh->m);
-        if (e.empty()) e = build_dual(mh->m, mh->d);
-        if (!e.empty()) {
-            errs[i] = e;
-            delete mh;
-        } else {
-            out[i] = mh;
-        }
-    }
-    for (int i = 0; i < count; ++i)
-        if (!errs[i].empty()) {
-            for (int j = 0; j < count; ++j) {
-                delete out[j];
-                out[j] = nullptr;
-            }
-            return set_err(nullptr, VFV_BAD_INPUT, "mesh " + std::to_string(i) + ": " + errs[i]);
-        }
-    return VFV_OK;
-}
-
-int vfv_mesh_info(const vfv_mesh* m, int64_t* n_pts, int64_t* n_nds, int64_t* n_tet, int64_t* n_dir, int64_t* n_bsub) {
-    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
-    if (n_pts) *n_pts = m->m.n_pts;
-    if (n_nds) *n_nds = m->m.n_nds;
-    if (n_tet) *n_tet = m->m.n_tet();
-    if (n_dir) *n_dir = m->d.n_dir;
-    if (n_bsub) *n_bsub = m->d.bnd_ptr.empty() ? 0 : m->d.bnd_ptr.back();
-    return VFV_OK;
-}
-
-int vfv_mesh_export(const vfv_mesh* m, double* pos, int32_t* node_bnd, int32_t* tets) {
-    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
-    if (pos) std::memcpy(pos, m->m.pos.data(), m->m.pos.size() * sizeof(double));
-    if (node_bnd) std::memcpy(node_bnd, m->m.node_bnd.data(), m->m.node_bnd.size() * sizeof(int32_t));
-    if (tets) std::memcpy(tets, m->m.tets.data(), m->m.tets.size() * sizeof(int32_t));
-    return VFV_OK;
-}
-
-int vfv_mesh_export_dual(const vfv_mesh* m, int64_t* nbr_ptr, int32_t* nbr_idx, double* dist, double* area, double* norm, double* skew,
-                         double* grad_wgt, double* cvol, double* cskew, int64_t* bnd_ptr, int32_t* bnd_j, int32_t* bnd_k,
-                         double* bnd_area, double* bnd_norm, double* bnd_wgt) {
-    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
-    const Dual& d = m->d;
-    auto cp = [](auto* dst, const auto& v) {
-        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
-    };
-    cp(nbr_ptr, d.nbr_ptr);
-    cp(nbr_idx, d.nbr_idx);
-    cp(dist, d.dist);
-    cp(area, d.area);
-    cp(norm, d.norm);
-    cp(skew, d.skew);
-    cp(grad_wgt, d.gw);
-    cp(cvol, d.cvol);
-    cp(cskew, d.cskew);
-    cp(bnd_ptr, d.bnd_ptr);
-    cp(bnd_j, d.bnd_j);
-    cp(bnd_k, d.bnd_k);
-    cp(bnd_area, d.bnd_area);
-    cp(bnd_norm, d.bnd_norm);
-    cp(bnd_wgt, d.bnd_wgt);
-    return VFV_OK;
-}
-
-// ---------------------------------------------------------------- heat operator
-int vfv_heat_create(vfv_ctx* ctx, const vfv_mesh* mh, int32_t n_bnd, const int32_t* bnd_kind, vfv_heat** out) {
-    if (!ctx || !mh || !out || (n_bnd > 0 && !bnd_kind)) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    *out = nullptr;
-    const Mesh& m = mh->m;
-    const Dual& d = mh->d;
-    const int64_t n = d.n_tot;
-    if (d.n_dir >= (int64_t)1 << 31 || n + d.n_dir >= (int64_t)1 << 31) return set_err(ctx, VFV_BAD_INPUT, "mesh too large for 32-bit indices");
-    std::vector<int32_t> kind(n, ROW_POINT), nb(n, -1);
-    for (int64_t v = m.n_pts; v < n; ++v) {
-        const int32_t b = m.node_bnd[v - m.n_pts];
-        if (b < 0 || b >= n_bnd) return set_err(ctx, VFV_BAD_INPUT, "node boundary id without a boundary condition");
-        if (bnd_kind[b] != VFV_BC_TEMP && bnd_kind[b] != VFV_BC_FLUX) return set_err(ctx, VFV_BAD_INPUT, "unknown boundary kind");
-        kind[v] = bnd_kind[b] == VFV_BC_TEMP ? ROW_DIRICHLET : ROW_FLUX;
-        nb[v] = b;
-    }
-    // matrix pattern: row v = its neighbours and itself (ascending); Dirichlet rows only the diagonal
-    std::vector<int32_t> np(n + 1), dloc(n, 0), rp(n + 1, 0), ci;
-    ci.reserve(d.n_dir + n);
-    for (int64_t v = 0; v < n; ++v) {
-        np[v] = (int32_t)d.nbr_ptr[v];
-        const int64_t b0 = d.nbr_ptr[v], e0 = d.nbr_ptr[v + 1];
-        if (kind[v] == ROW_DIRICHLET) {
-            ci.push_back((int32_t)v);
-        } else {
-            int32_t dl = 0;
-            while (b0 + dl < e0 && d.nbr_idx[b0 + dl] < v) ++dl;
-            dloc[v] = dl;
-            for (int64_t i = b0; i < b0 + dl; ++i) ci.push_back(d.nbr_idx[i]);
-            ci.push_back((int32_t)v);
-            for (int64_t i = b0 + dl; i < e0; ++i) ci.push_back(d.nbr_idx[i]);
-        }
-        rp[v + 1] = (int32_t)ci.size();
-    }
-    np[n] = (int32_t)d.nbr_ptr[n];
-    auto h = std::make_unique<vfv_heat>();
-    h->ctx = ctx;
-    h->n = n;
-    h->n_dir = d.n_dir;
-    h->n_bsub = d.bnd_ptr[n];
-    vfv_pattern* pat = nullptr;
-    int rc = vfv_pattern_from_csr(ctx, n, rp.data(), ci.data(), &pat);
-    if (rc) return rc;
-    h->pat = pat;
-    cudaStream_t s = ctx->stream;
-    std::vector<int32_t> bp(n + 1);
-    for (int64_t v = 0; v <= n; ++v) bp[v] = (int32_t)d.bnd_ptr[v];
-    CK(h->np.upload(np.data(), n + 1, s));
-    CK(h->ni.upload(d.nbr_idx.data(), d.n_dir, s));
-    CK(h->kind.upload(kind.data(), n, s));
-    CK(h->node_bnd.upload(nb.data(), n, s));
-    CK(h->dloc.upload(dloc.data(), n, s));
-    CK(h->bp.upload(bp.data(), n + 1, s));
-    CK(h->bj.upload(d.bnd_j.data(), d.bnd_j.size(), s));
-    CK(h->bk.upload(d.bnd_k.data(), d.bnd_k.size(), s));
-    CK(h->area.upload(d.area.data(), d.area.size(), s));
-    CK(h->dist.upload(d.dist.data(), d.dist.size(), s));
-    CK(h->skew.upload(d.skew.data(), d.skew.size(), s));
-    CK(h->gw.upload(d.gw.data(), d.gw.size(), s));
-    CK(h->cvol.upload(d.cvol.data(), d.cvol.size(), s));
-    CK(h->cskew.upload(d.cskew.data(), d.cskew.size(), s));
-    CK(h->barea.upload(d.bnd_area.data(), d.bnd_area.size(), s));
-    CK(h->bw.upload(d.bnd_wgt.data(), d.bnd_wgt.size(), s));
-    CK(h->f.alloc(5 * n));
-    CK(h->grad.alloc(12 * n));
-    CK(h->b.alloc(n));
-    h->h_rev.resize(d.n_dir);
-    for (int64_t i = 0; i < d.n_dir; ++i) h->h_rev[i] = (int32_t)d.nbr_rev[i];
-    *out = h.release();
-    return VFV_OK;
-}
-
-// Adjoint of the heat assembly (zero production): solve A^T lambda = dJ/dT with the GMRES of
-// vfv_solve, then dJ/d(log k) and dJ/dq by the gather kernels of kernels/adjoint.cu. Uses k, q
-// and their gradients from the last vfv_heat_assemble call.
-int vfv_heat_adjoint(vfv_ctx* ctx, vfv_heat* h, const double* T, const double* dJdT, const vfv_gmres_opts* opts, double* lambda,
-                     double* dJdlogk, double* dJdq, vfv_solve_info* info) {
-    if (!ctx || !h || !T || !dJdT) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    int rc = check_opts(ctx, opts);
-    if (rc) return rc;
-    if (info) std::memset(info, 0, sizeof(*info));
-    const int64_t n = h->n, E = h->n_dir;
-    cudaStream_t s = ctx->stream;
-    if (!h->pat_t) {
-        rc = make_transpose(ctx, h->pat, &h->pat_t, h->tmap);
-        if (rc) return rc;
-        CK(h->rev.upload(h->h_rev.data(), E, s));
-        CK(h->adj_work.alloc((size_t)5 * E + (size_t)10 * n));
-    }
-    double* w = h->adj_work.p;
-    double* pv = w;
-    double* pn = w + E;
-    double* sk = w + 2 * E;
-    double* gkm = w + 5 * E;
-    double* psi = gkm + n;
-    double* dT = psi + 3 * n;
-    double* dg = dT + n;
-    double* dl = dg + n;
-    double* dzero = dl + n;
-    double* ddk = dzero + n;
-    double* ddq = ddk + n;
-    k_gather_vals<double><<<grid_for(h->pat->nnz), 256, 0, s>>>(h->pat->nnz, h->tmap.p, h->pat->val.p, h->pat_t->val.p);
-    ctx->launches += 1;
-    h->pat_t->version++;
-    CK(cudaMemcpyAsync(dT, T, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(dg, dJdT, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(dzero, 0, n * sizeof(double), s));
-    rc = solve_dev(ctx, h->pat_t, dg, dzero, dl, opts, info);
-    if (rc) return rc;
-    AdjDev D{};
-    D.n = n;
-    D.n_dir = E;
-    D.np = h->np.p;
-    D.ni = h->ni.p;
-    D.rev = h->rev.p;
-    D.kind = h->kind.p;
-    D.area = h->area.p;
-    D.dist = h->dist.p;
-    D.skew = h->skew.p;
-    D.gw = h->gw.p;
-    D.cvol = h->cvol.p;
-    D.cskew = h->cskew.p;
-    D.k = h->f.p;
-    D.gk = h->grad.p;
-    D.T = dT;
-    D.lambda = dl;
-    D.pv = pv;
-    D.pn = pn;
-    D.sk = sk;
-    D.gkm = gkm;
-    D.psi = psi;
-    D.dlogk = ddk;
-    D.dq = ddq;
-    launch_adjoint_partials(s, D);
-    ctx->launches += 3;
-    CK(cudaGetLastError());
-    if (lambda) CK(cudaMemcpyAsync(lambda, dl, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (dJdlogk) CK(cudaMemcpyAsync(dJdlogk, ddk, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (dJdq) CK(cudaMemcpyAsync(dJdq, ddq, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    return VFV_OK;
-}
-
-void vfv_heat_destroy(vfv_heat* h) {
-    if (!h) return;
-    if (h->ctx) cudaStreamSynchronize(h->ctx->stream);
-    delete h;
-}
-
-vfv_pattern* vfv_heat_pattern(vfv_heat* h) { return h ? h->pat : nullptr; }
-
-const double* vfv_heat_rhs_device(vfv_heat* h) { return h ? h->b.p : nullptr; }
-
-int vfv_heat_assemble(vfv_ctx* ctx, vfv_heat* h, const double* k, const double* q, const double* s_, const double* T,
-                      const double* bc_val, int on_device, double* b_out) {
-    if (!ctx || !h || !k || !q || !s_ || !T || !bc_val) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    const int64_t n = h->n;
-    cudaStream_t s = ctx->stream;
-    const double* src[5] = {k, q, s_, T, bc_val};
-    const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    for (int f = 0; f < 5; ++f) CK(cudaMemcpyAsync(h->f.p + f * n, src[f], n * sizeof(double), kd, s));
-    const double* fl[4] = {h->f.p, h->f.p + n, h->f.p + 2 * n, h->f.p + 3 * n};
-    launch_grad(s, n, h->np.p, h->ni.p, h->gw.p, h->n_dir, 4, fl, h->grad.p);
-    HeatDev H{};
-    H.n = n;
-    H.n_dir = h->n_dir;
-    H.n_bsub = h->n_bsub;
-    H.np = h->np.p;
-    H.ni = h->ni.p;
-    H.area = h->area.p;
-    H.dist = h->dist.p;
-    H.skew = h->skew.p;
-    H.cvol = h->cvol.p;
-    H.cskew = h->cskew.p;
-    H.kind = h->kind.p;
-    H.node_bnd = h->node_bnd.p;
-    H.bp = h->bp.p;
-    H.bj = h->bj.p;
-    H.bk = h->bk.p;
-    H.barea = h->barea.p;
-    H.bw = h->bw.p;
-    H.rp = h->pat->rp.p;
-    H.dloc = h->dloc.p;
-    H.k = fl[0];
-    H.q = fl[1];
-    H.s = fl[2];
-    H.T = fl[3];
-    H.bcv = h->f.p + 4 * n;
-    H.gk = h->grad.p;
-    H.gq = h->grad.p + 3 * n;
-    H.gs = h->grad.p + 6 * n;
-    H.gT = h->grad.p + 9 * n;
-    H.val = h->pat->val.p;
-    H.b = h->b.p;
-    launch_assemble_heat(s, H);
-    ctx->launches += 2;
-    CK(cudaGetLastError());
-    h->pat->version++;
-    if (b_out) {
-        CK(cudaMemcpyAsync(b_out, h->b.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-    }
-    return VFV_OK;
-}
-
-int vfv_update_grad(vfv_ctx* ctx, vfv_heat* h, const double* f, double* grad) {
-    if (!ctx || !h || !f || !grad) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    const int64_t n = h->n;
-    cudaStream_t s = ctx->stream;
-    DBuf<double> fd, gd;
-    CK(fd.alloc(n));
-    CK(gd.alloc(3 * n));
-    CK(cudaMemcpyAsync(fd.p, f, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    const double* fl[1] = {fd.p};
-    launch_grad(s, n, h->np.p, h->ni.p, h->gw.p, h->n_dir, 1, fl, gd.p);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(grad, gd.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    return VFV_OK;
-}
-
-// ---------------------------------------------------------------- transient transport (config 4)
-int vfv_transport_create(vfv_ctx* ctx, int nmesh, vfv_mesh* const* meshes, double dt, vfv_transport** out) {
-    if (!ctx || nmesh <= 0 || !meshes || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    if (!(dt > 0.0)) return set_err(ctx, VFV_BAD_INPUT, "dt must be positive");
-    *out = nullptr;
-    auto t = std::make_unique<vfv_transport>();
-    t->ctx = ctx;
-    t->nmesh = nmesh;
-    t->dt = dt;
-    t->row_ptr.assign(nmesh + 1, 0);
-    int64_t ndir = 0;
-    for (int i = 0; i < nmesh; ++i) {
-        if (!meshes[i]) return set_err(ctx, VFV_BAD_INPUT, "NULL mesh");
-        t->row_ptr[i + 1] = t->row_ptr[i] + meshes[i]->d.n_tot;
-        ndir += meshes[i]->d.n_dir;
-    }
-    const int64_t n = t->row_ptr[nmesh];
-    if (n + ndir >= (int64_t)1 << 31) return set_err(ctx, VFV_BAD_INPUT, "batch too large for 32-bit indices");
-    t->n = n;
-    t->n_dir = ndir;
-    std::vector<int32_t> np(n + 1, 0), ni(ndir), dloc(n), rp(n + 1, 0), ci;
-    std::vector<double> area(ndir), dist(ndir), skew(3 * ndir), norm(3 * ndir), gw(3 * ndir), cvol(n);
-    ci.reserve(ndir + n);
-    int64_t e0 = 0;
-    for (int i = 0; i < nmesh; ++i) {
-        const Dual& d = meshes[i]->d;
-        const int64_t v0 = t->row_ptr[i], D = d.n_dir;
-        for (int64_t v = 0; v < d.n_tot; ++v) {
-            const int64_t gv = v0 + v;
-            np[gv] = (int32_t)(e0 + d.nbr_ptr[v]);
-            cvol[gv] = d.cvol[v];
-            const int64_t b = d.nbr_ptr[v], e = d.nbr_ptr[v + 1];
-            int32_t dl = 0;
-            while (b + dl < e && d.nbr_idx[b + dl] < v) ++dl;
-            dloc[gv] = dl;
-            for (int64_t k = b; k < b + dl; ++k) ci.push_back((int32_t)(v0 + d.nbr_idx[k]));
-            ci.push_back((int32_t)gv);
-            for (int64_t k = b + dl; k < e; ++k) ci.push_back((int32_t)(v0 + d.nbr_idx[k]));
-            rp[gv + 1] = (int32_t)ci.size();
-        }
-        for (int64_t k = 0; k < D; ++k) {
-            ni[e0 + k] = (int32_t)(v0 + d.nbr_idx[k]);
-            area[e0 + k] = d.area[k];
-            dist[e0 + k] = d.dist[k];
-            for (int c = 0; c < 3; ++c) {
-                skew[c * ndir + e0 + k] = d.skew[c * D + k];
-                norm[c * ndir + e0 + k] = d.norm[c * D + k];
-                gw[c * ndir + e0 + k] = d.gw[c * D + k];
-            }
-        }
-        e0 += D;
-    }
-    np[n] = (int32_t)ndir;
-    vfv_pattern* pat = nullptr;
-    int rc = vfv_pattern_from_csr(ctx, n, rp.data(), ci.data(), &pat);
-    if (rc) return rc;
-    t->pat = pat;
-    pat->blocks.assign(t->row_ptr.begin(), t->row_ptr.end());
-    cudaStream_t s = ctx->stream;
-    CK(t->d_row_ptr.upload(t->row_ptr.data(), nmesh + 1, s));
-    CK(t->np.upload(np.data(), n + 1, s));
-    CK(t->ni.upload(ni.data(), ndir, s));
-    CK(t->dloc.upload(dloc.data(), n, s));
-    CK(t->area.upload(area.data(), ndir, s));
-    CK(t->dist.upload(dist.data(), ndir, s));
-    CK(t->skew.upload(skew.data(), 3 * ndir, s));
-    CK(t->norm.upload(norm.data(), 3 * ndir, s));
-    CK(t->gw.upload(gw.data(), 3 * ndir, s));
-    CK(t->cvol.upload(cvol.data(), n, s));
-    CK(t->flux.alloc(ndir));
-    CK(t->fields.alloc(4 * n));   // D, u, v, w
-    CK(t->grads.alloc(12 * n));   // grad D, grad u, grad v, grad w
-    CK(t->b.alloc(n));
-    CK(t->c0.alloc(n));
-    CK(t->c1.alloc(n));
-    *out = t.release();
-    return VFV_OK;
-}
-
-void vfv_transport_destroy(vfv_transport* t) {
-    if (!t) return;
-    if (t->ctx) cudaStreamSynchronize(t->ctx->stream);
-    delete t;
-}
-
-vfv_pattern* vfv_transport_pattern(vfv_transport* t) { return t ? t->pat : nullptr; }
-
-int vfv_transport_info(const vfv_transport* t, int64_t* n_tot, int64_t* nnz, int32_t* nmesh, int64_t* row_ptr) {
-    if (!t) return set_err(nullptr, VFV_BAD_INPUT, "transport is NULL");
-    if (n_tot) *n_tot = t->n;
-    if (nnz) *nnz = t->pat->nnz;
-    if (nmesh) *nmesh = t->nmesh;
-    if (row_ptr) std::memcpy(row_ptr, t->row_ptr.data(), (t->nmesh + 1) * sizeof(int64_t));
-    return VFV_OK;
-}
-
-int vfv_transport_assemble(vfv_ctx* ctx, vfv_transport* t, const double* D, const double* vel, int on_device) {
-    if (!ctx || !t || !D || !vel) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    const int64_t n = t->n;
-    cudaStream_t s = ctx->stream;
-    const cudaMemcpyKind kd = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    CK(cudaMemcpyAsync(t->fields.p, D, n * sizeof(double), kd, s));
-    CK(cudaMemcpyAsync(t->fields.p + n, vel, 3 * n * sizeof(double), kd, s));
-    const double* f4[4] = {t->fields.p, t->fields.p + n, t->fields.p + 2 * n, t->fields.p + 3 * n};
-    launch_grad(s, n, t->np.p, t->ni.p, t->gw.p, t->n_dir, 4, f4, t->grads.p);
-    const TransportDev T = t->dev();
-    launch_face_flux(s, T);
-    launch_assemble_transport(s, T);
-    ctx->launches += 3;
-    CK(cudaGetLastError());
-    t->pat->version++;
-    return VFV_OK;
-}
-
-// nsteps of implicit Euler from c0 (host) with the current matrix: b = -vol c / dt, one batched GMRES
-// per step with the per-mesh stopping rule; the state stays on the device between steps.
-int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, const vfv_gmres_opts* opts, double* c_out,
-                      int32_t* iters) {
-    if (!ctx || !t || !c0 || !c_out || nsteps < 0) return set_err(ctx, VFV_BAD_INPUT, "invalid argument");
-    int rc = check_opts(ctx, opts);
-    if (rc) return rc;
-    const int64_t n = t->n;
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemcpyAsync(t->c0.p, c0, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    double* cur = t->c0.p;
-    double* nxt = t->c1.p;
-    for (int k = 0; k < nsteps; ++k) {
-        launch_transport_rhs(s, n, t->cvol.p, t->dt, cur, t->b.p);
-        ctx->launches += 1;
-        vfv_solve_info info{};
-        rc = solve_dev(ctx, t->pat, t->b.p, cur, nxt, opts, &info, t->nmesh, t->d_row_ptr.p);
-        if (rc) return rc;
-        if (iters) iters[k] = info.iters;
-        std::swap(cur, nxt);
-    }
-    CK(cudaMemcpyAsync(c_out, cur, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    return VFV_OK;
-}
-
-// dJ/dD for J = 0.5 ||c_N - target||^2 after nsteps implicit-Euler steps from c0, for the uniform
-// diffusivity D of the last vfv_transport_assemble. Discrete adjoint: A^T lam_N = c_N - target,
-// A^T lam_k = M^T lam_{k+1} with M = diag(-vol/dt), dJ/dD = -sum_k lam_{k+1}^T (dA/dD) c_{k+1}.
-// The forward states are kept every `every` steps (checkpoints) and the states of one segment are
-// recomputed from its checkpoint while the backward sweep crosses it.
-int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, int every, const double* target,
-                            const vfv_gmres_opts* opts, double* J, double* dJdD, int32_t* adj_iters) {
-    if (!ctx || !t || !c0 || !target || nsteps <= 0 || every <= 0) return set_err(ctx, VFV_BAD_INPUT, "invalid argument");
-    int rc = check_opts(ctx, opts);
-    if (rc) return rc;
-    const int64_t n = t->n;
-    cudaStream_t s = ctx->stream;
-    const int nck = (nsteps + every - 1) / every + 1;
-    const int blocks = (int)((n + 255) / 256);
-    if (!t->pat_t) {
-        rc = make_transpose(ctx, t->pat, &t->pat_t, t->tmap);
-        if (rc) return rc;
-    }
-    const size_t need = (size_t)n * (nck + every + 5) + (size_t)blocks + (size_t)nsteps + 8;
-    if (t->adj.n < need) CK(t->adj.alloc(need));
-    if (!t->adj_counter.p) {
-        CK(t->adj_counter.alloc(1));
-        CK(cudaMemset(t->adj_counter.p, 0, sizeof(unsigned)));
-    }
-    double* ck = t->adj.p;                       // [nck][n] checkpoints c_0, c_every, ...
-    double* seg = ck + (size_t)nck * n;          // [every][n] states of one segment
-    double* lam = seg + (size_t)every * n;       // adjoint vectors
-    double* lam2 = lam + n;
-    double* rhs = lam2 + n;
-    double* zero = rhs + n;
-    double* tmp = zero + n;
-    double* part = tmp + n;
-    double* terms = part + blocks;               // [nsteps]
-    k_gather_vals<double><<<grid_for(t->pat->nnz), 256, 0, s>>>(t->pat->nnz, t->tmap.p, t->pat->val.p, t->pat_t->val.p);
-    t->pat_t->version++;
-    CK(cudaMemsetAsync(zero, 0, n * sizeof(double), s));
-    CK(cudaMemcpyAsync(ck, c0, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    const TransportDev T = t->dev();
-    auto step = [&](const double* cin, double* cout) -> int {
-        launch_transport_rhs(s, n, t->cvol.p, t->dt, cin, t->b.p);
-        vfv_solve_info info{};
-        return solve_dev(ctx, t->pat, t->b.p, cin, cout, opts, &info, t->nmesh, t->d_row_ptr.p);
-    };
-    // forward sweep, keeping checkpoints
-    CK(cudaMemcpyAsync(t->c0.p, ck, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    double* cur = t->c0.p;
-    double* nxt = t->c1.p;
-    for (int k = 0; k < nsteps; ++k) {
-        if ((rc = step(cur, nxt))) return rc;
-        std::swap(cur, nxt);
-        if ((k + 1) % every == 0 && (k + 1) / every < nck) CK(cudaMemcpyAsync(ck + (size_t)((k + 1) / every) * n, cur, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    }
-    // J and lam_N
-    std::vector<double> hc(n), ht(target, target + n);
-    CK(cudaMemcpyAsync(hc.data(), cur, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    double jsum = 0.0;
-    for (int64_t i = 0; i < n; ++i) {
-        const double r = hc[i] - ht[i];
-        jsum += r * r;
-        hc[i] = r;
-    }
-    if (J) *J = 0.5 * jsum;
-    CK(cudaMemcpyAsync(rhs, hc.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
-    vfv_solve_info info{};
-    if ((rc = solve_dev(ctx, t->pat_t, rhs, zero, lam, opts, &info, t->nmesh, t->d_row_ptr.p))) return rc;
-    if (adj_iters) adj_iters[nsteps - 1] = info.iters;
-    // backward sweep over the segments, last first
-    for (int k = nsteps - 1; k >= 0; --k) {
-        const int j = k / every;  // segment of state c_{k+1}: c_{j every + 1 .. j every + every}
-        if (k == nsteps - 1 || (k + 1) % every == 0) {
-            const int last = std::min(nsteps, j * every + every);
-            const double* from = ck + (size_t)j * n;
-            for (int q = j * every; q < last; ++q) {
-                double* to = seg + (size_t)(q - j * every) * n;
-                if ((rc = step(q == j * every ? from : seg + (size_t)(q - 1 - j * every) * n, to))) return rc;
-            }
-        }
-        const double* c_k1 = seg + (size_t)(k - j * every) * n;
-        launch_transport_dAdD_dot(s, T, lam, c_k1, part, t->adj_counter.p, terms + k);
-        if (k > 0) {
-            launch_transport_rhs(s, n, t->cvol.p, t->dt, lam, rhs);  // M^T lam = -vol lam / dt
-            if ((rc = solve_dev(ctx, t->pat_t, rhs, lam, lam2, opts, &info, t->nmesh, t->d_row_ptr.p))) return rc;
-            if (adj_iters) adj_iters[k - 1] = info.iters;
-            std::swap(lam, lam2);
-        }
-    }
-    std::vector<double> ht2(nsteps);
-    CK(cudaMemcpyAsync(ht2.data(), terms, nsteps * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    CK(cudaGetLastError());
-    double g = 0.0;
-    for (int k = 0; k < nsteps; ++k) g -= ht2[k];
-    if (dJdD) *dJdD = g;
-    (void)tmp;
-    return VFV_OK;
-}
-
-}  // extern "C"
-
-// ================================================================ coupled Navier-Stokes (SteadyFlow)
-// Field-major [u | v | w | p] system of SteadyFlow::assemble_matrix (src/steady/core/steady_flow.rs:
-// 255-303) for one domain whose six faces are velocity boundaries, with the pressure fixed at one
-// vertex: assembled on the device from the flow data (flow_helper.rs) and solved by the GMRES of
-// vfv_solve (GMRES(m) + 4x4 block-Jacobi for the configuration this serves) inside the damped
-// Picard loop of SteadyBase::solve (src/steady/steady_base.rs:70-112).
-struct vfv_flow {
-    vfv_ctx* ctx = nullptr;
-    int64_t n = 0, n_pts = 0, n_dir = 0, n_bsub = 0, n_gc = 0, ntrip = 0, pref_vid = 0;
-    double pref = 0.0, rho_max = 0.0;
-    DBuf<int32_t> np, ni, bp, bj, bk, gcp, gcv, div_off, pst_off, sub_off, slot_loc;
-    DBuf<double> dist, area, norm, skew, gw, cvol, cskew, barea, bnorm, bw, gcc;
-    DBuf<double> den, visc, fce, bc_vel, gfix, gvel, rc, mom, flux, tv, b, x, xu;
-    DBuf<int64_t> trip_ptr, slot_ptr;
-    vfv_pattern* pat = nullptr;
-    ~vfv_flow() {
-        if (pat) vfv_pattern_destroy(pat);
-    }
-    NsDev dev(const double* xs) const {
-        NsDev D{};
-        D.n = n;
-        D.n_pts = n_pts;
-        D.n_dir = n_dir;
-        D.n_bsub = n_bsub;
-        D.n_gc = n_gc;
-        D.pref_vid = pref_vid;
-        D.pref = pref;
-        D.np = np.p;
-        D.ni = ni.p;
-        D.dist = dist.p;
-        D.area = area.p;
-        D.norm = norm.p;
-        D.skew = skew.p;
-        D.gw = gw.p;
-        D.cvol = cvol.p;
-        D.cskew = cskew.p;
-        D.bp = bp.p;
-        D.bj = bj.p;
-        D.bk = bk.p;
-        D.barea = barea.p;
-        D.bnorm = bnorm.p;
-        D.bw = bw.p;
-        D.gcp = gcp.p;
-        D.gcv = gcv.p;
-        D.gcc = gcc.p;
-        D.den = den.p;
-        D.visc = visc.p;
-        D.fce = fce.p;
-        D.bc_vel = bc_vel.p;
-        D.x = xs;
-        D.gvel = gvel.p;
-        D.gden = gfix.p;
-        D.gvisc = gfix.p + 3 * n;
-        D.gfce = gfix.p + 6 * n;
-        D.rc = rc.p;
-        D.mom = mom.p;
-        D.flux = flux.p;
-        D.trip_ptr = trip_ptr.p;
-        D.div_off = div_off.p;
-        D.pst_off = pst_off.p;
-        D.sub_off = sub_off.p;
-        D.tv = tv.p;
-        D.b = b.p;
-        D.rp = pat->rp.p;
-        D.slot_ptr = slot_ptr.p;
-        D.slot_loc = slot_loc.p;
-        D.val = pat->val.p;
-        return D;
-    }
-};
-
-namespace {
-
-__global__ void k_damp(int64_t n, double damp, double* __restrict__ x, const double* __restrict__ xu) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) x[i] = (1.0 - damp) * x[i] + damp * xu[i];
-}
-
-// Picard change measure of scaled_residual (src/base/scaling.rs:113-136) for the pressure field
-// (scale: max(range p, rho_max |u|max^2), round-off dead band 1e-11 max|p|) and the velocity field
-// (scale: max |u|); the larger of the two. NaN if the new state is not finite.
-double flow_scaled_residual(int64_t n, double rho_max, const std::vector<double>& xo, const std::vector<double>& xn) {
-    for (double v : xn)
-        if (!std::isfinite(v)) return std::nan("");
-    const double floor_ = 1e-30;
-    double vmax = 0.0;
-    for (const std::vector<double>* x : {&xo, &xn})
-        for (int64_t i = 0; i < n; ++i) {
-            const double a = (*x)[i], b = (*x)[n + i], c = (*x)[2 * n + i];
-            vmax = std::max(vmax, std::sqrt(a * a + b * b + c * c));
-        }
-    double pmin = 1e308, pmax = -1e308, pabs = 0.0;
-    for (const std::vector<double>* x : {&xo, &xn})
-        for (int64_t i = 3 * n; i < 4 * n; ++i) {
-            pmin = std::min(pmin, (*x)[i]);
-            pmax = std::max(pmax, (*x)[i]);
-            pabs = std::max(pabs, std::fabs((*x)[i]));
-        }
-    const double dead = 1e-11 * pabs;
-    double sp = 0.0, sv = 0.0;
-    for (int64_t i = 3 * n; i < 4 * n; ++i) {
-        const double d = std::max(std::fabs(xn[i] - xo[i]) - dead, 0.0);
-        sp += d * d;
-    }
-    for (int64_t i = 0; i < 3 * n; ++i) {
-        const double d = std::fabs(xn[i] - xo[i]);
-        sv += d * d;
-    }
-    const double nn = (double)std::max<int64_t>(n, 1);
-    const double rp = std::sqrt(sp / nn) / std::max(std::max(pmax - pmin, rho_max * vmax * vmax), floor_);
-    const double rv = std::sqrt(sv / nn) / std::max(vmax, floor_);
-    return std::max(rp, rv);
-}
-
-int flow_assemble(vfv_ctx* ctx, vfv_flow* f, const double* xs) {
-    cudaStream_t s = ctx->stream;
-    const int64_t n = f->n;
-    const double* fv[3] = {xs, xs + n, xs + 2 * n};
-    launch_grad(s, n, f->np.p, f->ni.p, f->gw.p, f->n_dir, 3, fv, f->gvel.p);
-    launch_ns_assemble(s, f->dev(xs));
-    ctx->launches += 8;
-    f->pat->version++;
-    CK(cudaGetLastError());
-    return VFV_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-int vfv_flow_pattern_host(const vfv_mesh* mh, int64_t pref_vid, int64_t* nnz, int64_t* ntrip, int32_t* rowptr, int32_t* colind) {
-    if (!mh) return set_err(nullptr, VFV_BAD_INPUT, "NULL mesh");
-    NsLayout L;
-    const std::string e = build_ns_layout(mh->d, pref_vid, L);
-    if (!e.empty()) return set_err(nullptr, VFV_BAD_INPUT, e);
-    if (nnz) *nnz = L.nnz();
-    if (ntrip) *ntrip = L.ntrip();
-    if (rowptr) std::copy(L.rp.begin(), L.rp.end(), rowptr);
-    if (colind) std::copy(L.ci.begin(), L.ci.end(), colind);
-    return VFV_OK;
-}
-
-int vfv_flow_create(vfv_ctx* ctx, const vfv_mesh* mh, const double* rho, const double* mu, const double* fce, const double* bc_vel,
-                    int64_t pref_vid, double pref, vfv_flow** out) {
-    if (!ctx || !mh || !rho || !mu || !fce || !bc_vel || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    *out = nullptr;
-    const Dual& d = mh->d;
-    const int64_t n = d.n_tot;
-    if (n + d.n_dir >= (int64_t)1 << 31) return set_err(ctx, VFV_BAD_INPUT, "mesh too large for 32-bit indices");
-    for (int64_t v = mh->m.n_pts; v < n; ++v) {
-        const int32_t bnd = mh->m.node_bnd[v - mh->m.n_pts];
-        if (bnd < 0 || bnd >= NUM_BND) return set_err(ctx, VFV_BAD_INPUT, "every node must lie on a velocity boundary");
-    }
-    NsLayout L;
-    const std::string e = build_ns_layout(d, pref_vid, L);
-    if (!e.empty()) return set_err(ctx, VFV_BAD_INPUT, e);
-    auto f = std::make_unique<vfv_flow>();
-    f->ctx = ctx;
-    f->n = n;
-    f->n_pts = d.n_pts;
-    f->n_dir = d.n_dir;
-    f->n_bsub = d.bnd_ptr[n];
-    f->n_gc = (int64_t)L.gcv.size();
-    f->ntrip = L.ntrip();
-    f->pref_vid = pref_vid;
-    f->pref = pref;
-    for (int64_t v = 0; v < n; ++v) f->rho_max = std::max(f->rho_max, std::fabs(rho[v]));
-    vfv_pattern* pat = nullptr;
-    int rc = vfv_pattern_from_csr(ctx, 4 * n, L.rp.data(), L.ci.data(), &pat);
-    if (rc) return rc;
-    f->pat = pat;
-    rc = vfv_pattern_autotune(ctx, pat, nullptr, nullptr);  // rows of 16 to 400 entries: measure the SpMV shape
-    if (rc) return rc;
-    cudaStream_t s = ctx->stream;
-    std::vector<int32_t> np(n + 1), bp(n + 1);
-    for (int64_t v = 0; v <= n; ++v) {
-        np[v] = (int32_t)d.nbr_ptr[v];
-        bp[v] = (int32_t)d.bnd_ptr[v];
-    }
-    CK(f->np.upload(np.data(), n + 1, s));
-    CK(f->ni.upload(d.nbr_idx.data(), d.n_dir, s));
-    CK(f->bp.upload(bp.data(), n + 1, s));
-    CK(f->bj.upload(d.bnd_j.data(), d.bnd_j.size(), s));
-    CK(f->bk.upload(d.bnd_k.data(), d.bnd_k.size(), s));
-    CK(f->dist.upload(d.dist.data(), d.dist.size(), s));
-    CK(f->area.upload(d.area.data(), d.area.size(), s));
-    CK(f->norm.upload(d.norm.data(), d.norm.size(), s));
-    CK(f->skew.upload(d.skew.data(), d.skew.size(), s));
-    CK(f->gw.upload(d.gw.data(), d.gw.size(), s));
-    CK(f->cvol.upload(d.cvol.data(), d.cvol.size(), s));
-    CK(f->cskew.upload(d.cskew.data(), d.cskew.size(), s));
-    CK(f->barea.upload(d.bnd_area.data(), d.bnd_area.size(), s));
-    CK(f->bnorm.upload(d.bnd_norm.data(), d.bnd_norm.size(), s));
-    CK(f->bw.upload(d.bnd_wgt.data(), d.bnd_wgt.size(), s));
-    CK(f->gcp.upload(L.gcp.data(), L.gcp.size(), s));
-    CK(f->gcv.upload(L.gcv.data(), L.gcv.size(), s));
-    CK(f->gcc.upload(L.gcc.data(), L.gcc.size(), s));
-    CK(f->trip_ptr.upload(L.trip_ptr.data(), L.trip_ptr.size(), s));
-    CK(f->div_off.upload(L.div_off.data(), L.div_off.size(), s));
-    CK(f->pst_off.upload(L.pst_off.data(), L.pst_off.size(), s));
-    CK(f->sub_off.upload(L.sub_off.data(), L.sub_off.size(), s));
-    CK(f->slot_ptr.upload(L.slot_ptr.data(), L.slot_ptr.size(), s));
-    CK(f->slot_loc.upload(L.slot_loc.data(), L.slot_loc.size(), s));
-    CK(f->den.upload(rho, n, s));
-    CK(f->visc.upload(mu, n, s));
-    CK(f->fce.upload(fce, 3 * n, s));
-    CK(f->bc_vel.upload(bc_vel, 3 * n, s));
-    CK(f->gfix.alloc(15 * n));
-    CK(f->gvel.alloc(9 * n));
-    CK(f->rc.alloc(n));
-    CK(f->mom.alloc(3 * n));
-    CK(f->flux.alloc(d.n_dir));
-    CK(f->tv.alloc(f->ntrip));
-    CK(f->b.alloc(4 * n));
-    CK(f->x.alloc(4 * n));
-    CK(f->xu.alloc(4 * n));
-    // gradients of the fixed fields: (rho, mu, fce_x, fce_y) and fce_z -> gfix [rho | mu | fce (9)]
-    const double* f4[4] = {f->den.p, f->visc.p, f->fce.p, f->fce.p + n};
-    launch_grad(s, n, f->np.p, f->ni.p, f->gw.p, f->n_dir, 4, f4, f->gfix.p);
-    const double* f1[1] = {f->fce.p + 2 * n};
-    launch_grad(s, n, f->np.p, f->ni.p, f->gw.p, f->n_dir, 1, f1, f->gfix.p + 12 * n);
-    ctx->launches += 2;
-    CK(cudaStreamSynchronize(s));
-    CK(cudaGetLastError());
-    *out = f.release();
-    return VFV_OK;
-}
-
-void vfv_flow_destroy(vfv_flow* f) {
-    if (!f) return;
-    if (f->ctx) cudaStreamSynchronize(f->ctx->stream);
-    delete f;
-}
-
-vfv_pattern* vfv_flow_pattern(vfv_flow* f) { return f ? f->pat : nullptr; }
-
-int vfv_flow_info(const vfv_flow* f, int64_t* n_unknowns, int64_t* nnz, int64_t* ntrip) {
-    if (!f) return set_err(nullptr, VFV_BAD_INPUT, "NULL flow");
-    if (n_unknowns) *n_unknowns = 4 * f->n;
-    if (nnz) *nnz = f->pat->nnz;
-    if (ntrip) *ntrip = f->ntrip;
-    return VFV_OK;
-}
-
-int vfv_flow_assemble_device(vfv_ctx* ctx, vfv_flow* f, const double* x, double* b) {
-    if (!ctx || !f || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    int rc = flow_assemble(ctx, f, x);
-    if (rc) return rc;
-    if (b) CK(cudaMemcpyAsync(b, f->b.p, 4 * f->n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    return VFV_OK;
-}
-
-int vfv_flow_assemble(vfv_ctx* ctx, vfv_flow* f, const double* x, double* b) {
-    if (!ctx || !f || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    CK(cudaMemcpyAsync(f->x.p, x, 4 * f->n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    int rc = flow_assemble(ctx, f, f->x.p);
-    if (rc) return rc;
-    if (b) CK(cudaMemcpyAsync(b, f->b.p, 4 * f->n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    return VFV_OK;
-}
-
-int vfv_flow_picard(vfv_ctx* ctx, vfv_flow* f, double* x, int max_iter, double tol, double damp, const vfv_gmres_opts* opts,
-                    double* res, int32_t* lin_iters, int32_t* iters_done, double* solve_seconds) {
-    if (!ctx || !f || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    if (max_iter <= 0) return set_err(ctx, VFV_BAD_INPUT, "max_iter must be positive (SolverNonPositiveMaxIter)");
-    if (!(tol > 0.0)) return set_err(ctx, VFV_BAD_INPUT, "tol must be positive (SolverNonPositiveTolerance)");
-    if (!(damp > 0.0 && damp <= 1.0)) return set_err(ctx, VFV_BAD_INPUT, "damping must be in (0, 1] (SolverInvalidDamping)");
-    int rc = check_opts(ctx, opts);
-    if (rc) return rc;
-    cudaStream_t s = ctx->stream;
-    const int64_t N4 = 4 * f->n;
-    CK(cudaMemcpyAsync(f->x.p, x, N4 * sizeof(double), cudaMemcpyHostToDevice, s));
-    std::vector<double> xo(x, x + N4), xn(N4);
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    double tsolve = 0.0;
-    int it = 0;
-    bool conv = false;
-    for (; it < max_iter && !conv; ++it) {
-        if ((rc = flow_assemble(ctx, f, f->x.p))) break;
-        CK(cudaEventRecord(e0, s));
-        vfv_solve_info info{};
-        rc = solve_dev(ctx, f->pat, f->b.p, f->x.p, f->xu.p, opts, &info);
-        CK(cudaEventRecord(e1, s));
-        CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        tsolve += ms * 1e-3;
-        if (lin_iters) lin_iters[it] = info.iters;
-        if (rc) break;
-        k_damp<<<grid_for(N4), 256, 0, s>>>(N4, damp, f->x.p, f->xu.p);
-        ctx->launches += 1;
-        CK(cudaMemcpyAsync(xn.data(), f->x.p, N4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        const double r = flow_scaled_residual(f->n, f->rho_max, xo, xn);
-        if (res) res[it] = r;
-        xo.swap(xn);
-        if (!std::isfinite(r)) {
-            rc = set_err(ctx, VFV_NONFINITE, "Picard: non-finite residual (SteadyNonFiniteResidual)");
-            ++it;
-            break;
-        }
-        conv = r < tol;
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    std::copy(xo.begin(), xo.end(), x);
-    if (iters_done) *iters_done = it;
-    if (solve_seconds) *solve_seconds = tsolve;
-    if (rc) return rc;
-    if (!conv) return set_err(ctx, VFV_NOT_CONVERGED, "Picard iteration did not reach the tolerance (SteadyDidNotConverge)");
     return VFV_OK;
 }
 

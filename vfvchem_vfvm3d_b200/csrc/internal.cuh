@@ -1,0 +1,125 @@
+// Internal declarations shared by the translation units of libvfvgpu (not part of the C ABI):
+// the context and pattern structures behind the opaque handles, device buffers, error helpers,
+// and the GMRES entry used by the operator handles.
+#pragma once
+#include "../../include/vfv_gpu.h"
+#include "common.cuh"
+#include "host/mesh.hpp"
+
+#include <algorithm>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+using namespace vfv;
+
+// ================================================================ errors / buffers
+// the last error of calls without a context (thread-local), defined in api.cu
+std::string& vfv_thread_error();
+
+struct vfv_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    DevStatus* h_status = nullptr;  // pinned
+    double* h_scalar = nullptr;     // pinned scratch for small reads
+    int64_t launches = 0;           // kernels launched by this context (graph nodes counted per replay)
+};
+
+inline int set_err(vfv_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    vfv_thread_error() = msg;
+    return code;
+}
+
+#define CK(call)                                                                                           \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return set_err(ctx, VFV_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+struct DBuf {  // device buffer, freed with its owner
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(&p, count * sizeof(T));
+    }
+    cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
+        cudaError_t e = alloc(count);
+        if (e != cudaSuccess || count == 0) return e;
+        e = cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return e;
+        return cudaStreamSynchronize(s);
+    }
+};
+
+inline int grid_for(int64_t threads, int block = 256) { return (int)std::max<int64_t>(1, (threads + block - 1) / block); }
+
+
+// ================================================================ ILU structure (host-built)
+struct IluStruct {
+    int order = -1;
+    int nlev = 0;
+    std::vector<int32_t> lev_ptr;  // [nlev+1] row ranges in the permuted numbering
+    std::vector<int32_t> h_perm;   // new -> old
+    DBuf<int32_t> d_lev_ptr;       // same, on the device (read by the cycle kernel)
+    DBuf<int32_t> perm, rp, ci, dg, src;
+    DBuf<double> lu64;
+    DBuf<float> lu32;
+    DBuf<int> bad;
+
+
+    uint64_t version64 = ~0ull, version32 = ~0ull;
+};
+
+struct SolverBase {
+    virtual ~SolverBase() = default;
+};
+
+struct vfv_pattern {
+    vfv_ctx* ctx = nullptr;
+    int64_t n = 0, nnz = 0, ntrip = 0;
+    int spmv_lanes[2] = {4, 4};  // lanes per row of the SpMV for double / float values (autotuned; kSpG by default)
+    std::vector<int32_t> h_rp, h_ci;
+    DBuf<int32_t> rp, ci, diag_pos;
+    DBuf<double> val;
+    DBuf<float> val32;
+    uint64_t version = 0, version32 = ~0ull;
+    DBuf<int64_t> slot_ptr, slot_trip;
+    DBuf<double> trip_vals;
+    std::vector<int64_t> blocks;          // row ranges of the diagonal blocks of a block-diagonal system (may be empty)
+    const vfv_pattern* same_as = nullptr;  // a pattern with identical rows/columns (ILU orderings are shared)
+    std::map<int, std::unique_ptr<IluStruct>> ilu;
+    std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<SolverBase>> solvers;
+    DBuf<double> tmp_b, tmp_x;  // staging for host-pointer solves
+};
+
+struct vfv_mesh {
+    Mesh m;
+    Dual d;
+};
+
+// GMRES solve on device arrays (the solver of vfv_solve): cached per pattern and options.
+int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info,
+              int nblk = 0, const int64_t* blk_d = nullptr);
+// argument checks of the reference's LinearGmres constructor and solve options
+int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o);
+// transpose of a pattern (tmap: slot in A of every entry of A^T) and the gather of A's values into it
+int make_transpose(vfv_ctx* ctx, const vfv_pattern* p, vfv_pattern** out, DBuf<int32_t>& tmap_d);
+int gather_transpose_values(vfv_ctx* ctx, const vfv_pattern* p, vfv_pattern* pt, const int32_t* tmap);

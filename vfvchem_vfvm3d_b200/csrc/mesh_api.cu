@@ -1,0 +1,127 @@
+// Mesh handles of libvfvgpu: seeded jittered cubes, meshes from given vertices, and the export of
+// the Delaunay tetrahedra and the Voronoi dual (host code: csrc/host/mesh.cpp).
+#include "internal.cuh"
+
+#include <cstring>
+#include <omp.h>
+
+// Delaunay tetrahedralisation and Voronoi dual of a mesh whose vertices are set; takes ownership.
+static int mesh_finish(vfv_mesh* mh, vfv_mesh** out) {
+    std::string e = delaunay(mh->m);
+    if (e.empty()) e = build_dual(mh->m, mh->d);
+    if (!e.empty()) {
+        delete mh;
+        return set_err(nullptr, VFV_BAD_INPUT, e);
+    }
+    *out = mh;
+    return VFV_OK;
+}
+
+extern "C" {
+
+int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out) {
+    if (!out) return set_err(nullptr, VFV_BAD_INPUT, "out is NULL");
+    *out = nullptr;
+    if (n < 3 || n > 400) return set_err(nullptr, VFV_BAD_INPUT, "grid size n must be in [3, 400]");
+    if (!(jitter >= 0.0 && jitter < 0.5)) return set_err(nullptr, VFV_BAD_INPUT, "jitter must be in [0, 0.5)");
+    auto* mh = new vfv_mesh();
+    mh->m = make_jitter_cube(n, seed, jitter);
+    return mesh_finish(mh, out);
+}
+
+int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out) {
+    if (!out || !pos || (n_nds > 0 && !node_bnd)) return set_err(nullptr, VFV_BAD_INPUT, "NULL argument");
+    *out = nullptr;
+    if (n_pts < 0 || n_nds < 0 || n_pts + n_nds < 4) return set_err(nullptr, VFV_BAD_INPUT, "need at least four vertices");
+    auto* mh = new vfv_mesh();
+    mh->m.n_pts = n_pts;
+    mh->m.n_nds = n_nds;
+    mh->m.pos.assign(pos, pos + 3 * (n_pts + n_nds));
+    mh->m.node_bnd.assign(node_bnd, node_bnd + n_nds);
+    return mesh_finish(mh, out);
+}
+
+void vfv_mesh_destroy(vfv_mesh* m) { delete m; }
+
+int vfv_mesh_jitter_cubes(int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out) {
+    if (count <= 0 || !n || !seeds || !out) return set_err(nullptr, VFV_BAD_INPUT, "invalid batch arguments");
+    for (int i = 0; i < count; ++i) {
+        out[i] = nullptr;
+        if (n[i] < 3 || n[i] > 400) return set_err(nullptr, VFV_BAD_INPUT, "grid size n must be in [3, 400]");
+    }
+    if (!(jitter >= 0.0 && jitter < 0.5)) return set_err(nullptr, VFV_BAD_INPUT, "jitter must be in [0, 0.5)");
+    std::vector<std::string> errs(count);
+    // meshes in parallel (largest first); the per-mesh OpenMP loops run serially inside
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int t = 0; t < count; ++t) {
+        const int i = order[t];
+        auto* mh = new vfv_mesh();
+        mh->m = make_jitter_cube(n[i], seeds[i], jitter);
+        std::string e = delaunay(mh->m);
+        if (e.empty()) e = build_dual(mh->m, mh->d);
+        if (!e.empty()) {
+            errs[i] = e;
+            delete mh;
+        } else {
+            out[i] = mh;
+        }
+    }
+    for (int i = 0; i < count; ++i)
+        if (!errs[i].empty()) {
+            for (int j = 0; j < count; ++j) {
+                delete out[j];
+                out[j] = nullptr;
+            }
+            return set_err(nullptr, VFV_BAD_INPUT, "mesh " + std::to_string(i) + ": " + errs[i]);
+        }
+    return VFV_OK;
+}
+
+int vfv_mesh_info(const vfv_mesh* m, int64_t* n_pts, int64_t* n_nds, int64_t* n_tet, int64_t* n_dir, int64_t* n_bsub) {
+    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
+    if (n_pts) *n_pts = m->m.n_pts;
+    if (n_nds) *n_nds = m->m.n_nds;
+    if (n_tet) *n_tet = m->m.n_tet();
+    if (n_dir) *n_dir = m->d.n_dir;
+    if (n_bsub) *n_bsub = m->d.bnd_ptr.empty() ? 0 : m->d.bnd_ptr.back();
+    return VFV_OK;
+}
+
+int vfv_mesh_export(const vfv_mesh* m, double* pos, int32_t* node_bnd, int32_t* tets) {
+    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
+    if (pos) std::memcpy(pos, m->m.pos.data(), m->m.pos.size() * sizeof(double));
+    if (node_bnd) std::memcpy(node_bnd, m->m.node_bnd.data(), m->m.node_bnd.size() * sizeof(int32_t));
+    if (tets) std::memcpy(tets, m->m.tets.data(), m->m.tets.size() * sizeof(int32_t));
+    return VFV_OK;
+}
+
+int vfv_mesh_export_dual(const vfv_mesh* m, int64_t* nbr_ptr, int32_t* nbr_idx, double* dist, double* area, double* norm, double* skew,
+                         double* grad_wgt, double* cvol, double* cskew, int64_t* bnd_ptr, int32_t* bnd_j, int32_t* bnd_k,
+                         double* bnd_area, double* bnd_norm, double* bnd_wgt) {
+    if (!m) return set_err(nullptr, VFV_BAD_INPUT, "mesh is NULL");
+    const Dual& d = m->d;
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(nbr_ptr, d.nbr_ptr);
+    cp(nbr_idx, d.nbr_idx);
+    cp(dist, d.dist);
+    cp(area, d.area);
+    cp(norm, d.norm);
+    cp(skew, d.skew);
+    cp(grad_wgt, d.gw);
+    cp(cvol, d.cvol);
+    cp(cskew, d.cskew);
+    cp(bnd_ptr, d.bnd_ptr);
+    cp(bnd_j, d.bnd_j);
+    cp(bnd_k, d.bnd_k);
+    cp(bnd_area, d.bnd_area);
+    cp(bnd_norm, d.bnd_norm);
+    cp(bnd_wgt, d.bnd_wgt);
+    return VFV_OK;
+}
+
+}  // extern "C"
