@@ -7,6 +7,7 @@ symmetry and zero row sums of the diffusion block, the FP64 LU solution and the 
 of examples/heat/heat_analytic.rs:9.
 """
 import numpy as np
+import scipy.sparse as sp
 import pytest
 from scipy.spatial import Delaunay
 
@@ -204,3 +205,28 @@ def test_oracle_adjoint_matches_finite_differences(lib_built):
         ad = gk @ dk + gq @ dq
         worst = max(worst, abs(fd - ad) / max(abs(ad), 1e-30))
     assert worst < 1e-6
+
+
+def test_transport_operator_preserves_uniform_fields(lib_built):
+    """Transport oracle (time + diffusion + power-law advection, zero-flux walls): every spatial
+    row sums to zero (diffusion pairs c, -c; the non-conservative advection pairs coeff, -coeff),
+    so A 1 = -vol/dt and a uniform field is a fixed point of the implicit step; with zero velocity
+    the diffusion block is symmetric."""
+    from vfvchem_vfvm3d_b200 import Mesh
+    from vfvchem_vfvm3d_b200.problems import transport_fields
+    m = Mesh.jitter_cubes([6], [31])[0]
+    vel, _ = transport_fields([m])
+    d = m.dual()
+    _, nb, _ = m.export()
+    node_bnd = np.full(m.n_tot, -1, np.int32)
+    node_bnd[m.n_pts:] = nb
+    dt = 1e-2
+    for v in (vel, np.zeros_like(vel)):
+        r, c, val = oracle.transport_triplets(d, m.n_pts, node_bnd, 1e-3, v, dt)
+        rp, ci, va = oracle.csr_from_triplets(m.n_tot, r, c, val)
+        A = sp.csr_matrix((va, ci, rp), shape=(m.n_tot, m.n_tot))
+        rows = np.asarray(A.sum(axis=1)).ravel()
+        scale = np.max(np.abs(va))
+        assert np.max(np.abs(rows + d["cvol"] / dt)) <= 1e-12 * scale
+    asym = A - A.T  # zero velocity: pure time + diffusion
+    assert abs(asym).max() <= 1e-14 * scale
