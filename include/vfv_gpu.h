@@ -190,7 +190,7 @@ int vfv_heat_adjoint(vfv_ctx* ctx, vfv_heat* h, const double* T, const double* d
 /* gradient of one field on the heat mesh: grad[3][n_tot] (host arrays) */
 int vfv_update_grad(vfv_ctx* ctx, vfv_heat* h, const double* f, double* grad);
 
-/* ---- batched transient transport (config 4): one species, implicit Euler, zero-flux walls.
+/* ---- batched transient transport: one species, implicit Euler, zero-flux walls.
  * The meshes are concatenated into one block-diagonal system; every kernel runs over all of them.
  * Per row, in push order: OpSclDomTimeUnity (opscl_dom_timeunity.rs:32-58), OpSclDomDiffusion
  * (opscl_dom_diff.rs:40-91), OpSclDomAdvection (power law, opscl_dom_adv.rs:49-125) with the face mass

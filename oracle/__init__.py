@@ -115,7 +115,7 @@ def heat_triplets(dual: dict, n_pts: int, node_bnd: np.ndarray, bnd_order, bnd_k
 
 
 def transport_triplets(dual: dict, n_pts: int, node_bnd: np.ndarray, D, vel, dt: float):
-    """Triplets of the config-4 transport operator (time + diffusion + power-law advection) of one
+    """Triplets of the transient transport operator (time + diffusion + power-law advection) of one
     mesh in push order. vel is [3][n]; gradients come from oracle.grad."""
     n = dual["nbr_ptr"].size - 1
     d, keep = _orc_dual(dual, n_pts)

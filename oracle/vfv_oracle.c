@@ -170,7 +170,7 @@ int64_t orc_heat_triplets(const orc_dual* d, const int32_t* node_bnd, int32_t n_
 
 /* ------------------------------------------------------------------------------------------ */
 /*
- * Transient advection-diffusion (config 4) for one mesh, in push order per operator: time
+ * Transient advection-diffusion for one mesh, in push order per operator: time
  * (OpSclDomTimeUnity::apply_time, opscl_dom_timeunity.rs:32-58) over points, diffusion
  * (opscl_dom_diff.rs:55-87) over points, advection (OpSclDomAdvection, opscl_dom_adv.rs:49-125)
  * over points, then the boundary twins (opscl_bnd_timeunity, opscl_bnd_diff, opscl_bnd_adv) for

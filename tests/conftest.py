@@ -27,7 +27,7 @@ def lib_built():
 
 @pytest.fixture(scope="session")
 def c1(lib_built):
-    """Config 1: n=20 cube (8,000 vertices), k=1, q=s=0, T=0/1 on x=0/1, zero flux elsewhere."""
+    """Uniform heat slab: n=20 cube (8,000 vertices), k=1, q=s=0, T=0/1 on x=0/1, zero flux elsewhere."""
     from vfvchem_vfvm3d_b200.problems import steady_heat
     return steady_heat(20)
 

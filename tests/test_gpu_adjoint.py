@@ -1,4 +1,4 @@
-"""Config 3 (adjoint gradient) on the GPU through the C ABI: vfv_heat_adjoint against the oracle's
+"""Adjoint gradient of the steady heat solution on the GPU through the C ABI: vfv_heat_adjoint against the oracle's
 independently built adjoint and against central finite differences (step 1e-6) of the oracle's
 forward model on 64 random unit directions in (log k, q)."""
 import numpy as np

@@ -257,8 +257,8 @@ def test_engines_agree(gpu_ctx, c1h_system, c1_hetero):
     assert _rel(res[0][0], res[1][0]) <= 1e-12
 
 
-def test_config1_gmres30_jacobi(gpu_ctx, c1, c1_system):
-    """Config 1: GMRES(30) + Jacobi to 1e-10 relative residual against the FP64 LU solution."""
+def test_uniform_heat_gmres30_jacobi(gpu_ctx, c1, c1_system):
+    """Uniform heat slab (n=20): GMRES(30) + Jacobi to 1e-10 relative residual against the FP64 LU solution."""
     from vfvchem_vfvm3d_b200 import GmresOptions, Pattern
     (rp, ci, va), b, _ = c1_system
     p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)

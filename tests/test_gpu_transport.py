@@ -1,4 +1,4 @@
-"""Config 4 (batched transient advection-diffusion) on the GPU through the C ABI, against the
+"""Batched transient advection-diffusion on the GPU through the C ABI, against the
 oracle's restatement of the same operator composition and SuperLU time stepping."""
 import numpy as np
 import pytest

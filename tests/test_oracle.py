@@ -185,7 +185,7 @@ def test_heat_slab_profile(lib_built):
 
 
 def test_oracle_adjoint_matches_finite_differences(lib_built):
-    """Config 3 check at small size: the oracle's adjoint gradient against central differences
+    """Heat adjoint check at small size: the oracle's adjoint gradient against central differences
     (step 1e-6) of the oracle's own forward model, on random unit directions in (log k, q)."""
     from oracle import adjoint
     from vfvchem_vfvm3d_b200.problems import steady_heat

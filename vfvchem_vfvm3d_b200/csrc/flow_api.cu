@@ -13,7 +13,7 @@
 // Field-major [u | v | w | p] system of SteadyFlow::assemble_matrix (src/steady/core/steady_flow.rs:
 // 255-303) for one domain whose six faces are velocity boundaries, with the pressure fixed at one
 // vertex: assembled on the device from the flow data (flow_helper.rs) and solved by the GMRES of
-// vfv_solve (GMRES(m) + 4x4 block-Jacobi for the configuration this serves) inside the damped
+// vfv_solve (GMRES(m) + 4x4 block-Jacobi for the lid-driven cavity) inside the damped
 // Picard loop of SteadyBase::solve (src/steady/steady_base.rs:70-112).
 struct vfv_flow {
     vfv_ctx* ctx = nullptr;

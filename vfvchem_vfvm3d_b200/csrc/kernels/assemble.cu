@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(256) k_assemble_heat(HeatDev H) {
     H.b[v] = bb;
 }
 
-// ---------------------------------------------------------------- transient transport (config 4)
+// ---------------------------------------------------------------- transient transport (batched meshes)
 // Face mass flux with zero pressure and body force (flow_helper.rs:72-179 with vel_rc = 0):
 //   F = rho_f (u_f . n) A,  rho = 1,  u_f = skew-corrected arithmetic mean of the vertex velocities.
 __global__ void __launch_bounds__(256) k_face_flux(TransportDev T) {

@@ -69,7 +69,7 @@ void launch_assemble_transport(cudaStream_t s, const TransportDev& T);
 void launch_transport_rhs(cudaStream_t s, int64_t n, const double* cvol, double dt, const double* c_prev, double* b);
 
 // part[blk] = sum over this block's rows v of lam_v sum_faces s_e (c_n - c_v), where
-// s_e = d(cond + coeff)/dD for a uniform diffusivity D (transient adjoint, config 4)
+// s_e = d(cond + coeff)/dD for a uniform diffusivity D (transient adjoint of the transport batch)
 void launch_transport_dAdD_dot(cudaStream_t s, const TransportDev& T, const double* lam, const double* c, double* part, unsigned* counter,
                                double* out);
 

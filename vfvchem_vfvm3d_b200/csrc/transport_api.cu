@@ -9,7 +9,7 @@
 #include <cmath>
 #include <vector>
 
-// Concatenation of several meshes into one block-diagonal transport system (config 4).
+// Concatenation of several meshes into one block-diagonal transport system.
 struct vfv_transport {
     vfv_ctx* ctx = nullptr;
     int nmesh = 0;
@@ -56,7 +56,7 @@ struct vfv_transport {
 
 extern "C" {
 
-// ---------------------------------------------------------------- transient transport (config 4)
+// ---------------------------------------------------------------- transient transport (batched meshes)
 int vfv_transport_create(vfv_ctx* ctx, int nmesh, vfv_mesh* const* meshes, double dt, vfv_transport** out) {
     if (!ctx || nmesh <= 0 || !meshes || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (!(dt > 0.0)) return set_err(ctx, VFV_BAD_INPUT, "dt must be positive");

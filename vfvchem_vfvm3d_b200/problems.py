@@ -71,7 +71,7 @@ class TransportBatch:
 
 def transport_batch(count: int = 256, nmin: int = 2000, nmax: int = 50000, seed: int = 4, D: float = 1e-3, dt: float = 1e-2,
                     steps: int = 100) -> TransportBatch:
-    """Config 4: `count` jittered cubes with vertex counts N_i drawn log-uniform in [nmin, nmax]
+    """Transport batch: `count` jittered cubes with vertex counts N_i drawn log-uniform in [nmin, nmax]
     (numpy PCG64, `seed`), n_i = round(N_i^(1/3)) grid points per axis, mesh seeds 1000 + i."""
     rng = np.random.default_rng(seed)
     N = np.exp(rng.uniform(np.log(nmin), np.log(nmax), count))

@@ -1,4 +1,4 @@
-"""Batched transient advection-diffusion (config 4) over many independent meshes.
+"""Batched transient advection-diffusion over many independent meshes.
 
 The meshes are concatenated into one block-diagonal system (``vfv_transport``); every kernel of
 the assembly and of the GMRES runs over all meshes at once, and each time step's solve stops when
