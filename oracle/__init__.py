@@ -1,7 +1,7 @@
 """CPU oracle for the assemble-and-solve path — TEST INFRASTRUCTURE ONLY.
 
 Imported only by tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg, always as
-the checker (never as the thing measured or shipped). Parity is UNPINNED against outputs of the
+the reference answer (never as the thing measured or shipped). Parity is UNPINNED against outputs of the
 reference itself (a Rust crate that cannot be built here and ships no golden vectors for this
 path); the restatement is pinned to known answers instead — see tests/test_oracle.py.
 

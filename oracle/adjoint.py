@@ -2,7 +2,7 @@
 
 J(T) = 0.5 sum_{i in sensors} (T_i - d_i)^2 with A(k) T = b(q) the system of
 SteadyHeat::assemble_matrix (src/steady/core/steady_heat.rs:143-171) at zero production.
-The reference has no adjoint; this is the checker of the product's one. It is built differently
+The reference has no adjoint; this is the oracle for the product's one. It is built differently
 from the product's gather kernels: explicit sparse Jacobians (selectors, the least-squares gradient
 operator of ScalarDomain::update_grad, src/base/scl_dom.rs:146-164) and scipy's SuperLU for the
 transposed solve. `tests/test_oracle.py` pins it against central finite differences of the

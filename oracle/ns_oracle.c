@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the coupled Navier-Stokes assembly (lid-driven cavity) — TEST INFRASTRUCTURE ONLY.
  *
- * Used by tests/ as the checker; the product (libvfvgpu.so) never links or calls it.
+ * Used by tests/ as the reference answer; the product (libvfvgpu.so) never links or calls it.
  * Parity UNPINNED against reference outputs (the reference is Rust and cannot be built here); the
  * restatement is pinned to known answers in tests/test_oracle_ns.py (pressure-gradient
  * coefficients exact for linear fields and zero for constants, the LU solution of the assembled

@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the assemble-and-solve path of vfvchem-vfvm3d — TEST INFRASTRUCTURE ONLY.
  *
- * Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker; the
+ * Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the reference answer; the
  * product (libvfvgpu.so) never links or calls it.
  *
  * Parity status: UNPINNED against reference-produced outputs. The reference is Rust (no cargo or

@@ -62,7 +62,7 @@ def test_shard_meshes_is_a_balanced_partition(world):
 
 
 def test_reference_arm_under_torchrun_two_ranks(lib_built):
-    """bench.py --impl reference launched like the N=2 driver run, with gloo: rank 0 prints one
+    """bench.py --impl reference launched under two-rank torchrun, with gloo: rank 0 prints one
     JSON line, rank 1 exits without work, both exit 0."""
     env = dict(os.environ, VFV_DIST_BACKEND="gloo", OMP_NUM_THREADS="2")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr", "127.0.0.1",

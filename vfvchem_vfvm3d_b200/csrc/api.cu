@@ -781,7 +781,7 @@ struct Gmres : SolverBase {
     // one-thread kernel before each node sets the condition from the device `done` flag, so the
     // groups after convergence cost one tiny launch each instead of ~25 kernels per step (a step of
     // a running group that finds the solve done still returns at once, as in the straight graph). Returns an error (and leaves no graph) where the
-    // driver cannot build it; the caller then captures the straight graph.
+    // CUDA driver cannot build it; the caller then captures the straight graph.
     cudaError_t build_conditional_graph(cudaStream_t s, vfv_pattern* p, cudaGraph_t* out, int64_t* top_nodes, int64_t* step_nodes) {
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaGraphCreate(&g, 0);
