@@ -88,3 +88,28 @@ def test_no_cpu_fallback_without_device(lib_built):
     from vfvchem_vfvm3d_b200 import Context, VFVChemError
     with pytest.raises(VFVChemError):
         Context(0)
+
+
+_DUAL_DIGEST = """
+import hashlib, numpy as np
+from vfvchem_vfvm3d_b200 import Mesh
+m = Mesh.jitter_cube(14, 5, 0.25)
+h = hashlib.sha256()
+for k, a in sorted(m.dual().items()):
+    h.update(k.encode()); h.update(np.ascontiguousarray(a).tobytes())
+print(h.hexdigest())
+"""
+
+
+def test_dual_does_not_depend_on_thread_count(lib_built):
+    """The Voronoi dual is built by parallel passes whose sums run in a fixed order (tetrahedron,
+    edge, side), so one thread and several give the same bits."""
+    import subprocess
+    import sys
+    digests = []
+    for threads in ("1", "3"):
+        env = dict(os.environ, OMP_NUM_THREADS=threads)
+        out = subprocess.run([sys.executable, "-c", _DUAL_DIGEST], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        digests.append(out.stdout.strip().splitlines()[-1])
+    assert digests[0] == digests[1]

@@ -16,6 +16,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <numeric>
 
 namespace vfv {
@@ -381,181 +382,253 @@ std::string delaunay(Mesh& mesh) {
 }
 
 // ---------------------------------------------------------------- Voronoi dual
+namespace {
+
+constexpr int kEdgeEnds[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+
+// The two Voronoi face pieces that tetrahedron tv (circumcentre c_t) contributes to its local edge
+// e (geom_tet.rs:122-171): per side, the area of the triangle (edge midpoint, circumcentre of the
+// face towards that side, c_t) signed along the normal pointing away from the other side, and the
+// triangle's centroid.
+inline void face_pieces(const Mesh& mesh, const int32_t* tv, V3 c_t, int e, double area[2], V3 cent[2]) {
+    auto P = [&](int64_t v) { return V3{mesh.pos[3 * v], mesh.pos[3 * v + 1], mesh.pos[3 * v + 2]}; };
+    const int li = kEdgeEnds[e][0], lj = kEdgeEnds[e][1];
+    int oth[2], no = 0;
+    for (int l = 0; l < 4; ++l)
+        if (l != li && l != lj) oth[no++] = l;
+    const V3 pi = P(tv[li]), pj = P(tv[lj]);
+    const double dist = len3(sub3(pj, pi));
+    const V3 ee = scale3(1.0 / dist, sub3(pj, pi));
+    const V3 m = scale3(0.5, add3(pi, pj));
+    for (int side = 0; side < 2; ++side) {
+        const V3 pa = P(tv[oth[side]]), pb = P(tv[oth[1 - side]]);
+        const V3 c_f = circumcircle3(pi, pj, pa);
+        V3 u = sub3(sub3(pa, m), scale3(dot3(sub3(pa, m), ee), ee));
+        u = scale3(1.0 / len3(u), u);
+        V3 n = cross3(ee, u);
+        if (dot3(sub3(pb, m), n) < 0.0) n = scale3(-1.0, n);
+        const double s1 = dot3(sub3(c_f, m), u);
+        const double s2 = dot3(sub3(c_t, c_f), n);
+        area[side] = 0.5 * s1 * s2;
+        cent[side] = scale3(1.0 / 3.0, add3(m, add3(c_f, c_t)));
+    }
+}
+
+}  // namespace
+
+// Every step is a data-parallel pass over tetrahedra, vertices or edges. Each sum runs in the
+// order of the serial tetrahedron loop of the reference (tetrahedron, then local edge, then side),
+// so the result does not depend on the thread count.
 std::string build_dual(const Mesh& mesh, Dual& d) {
     const int64_t N = mesh.n_tot(), T = mesh.n_tet();
     const int32_t* tet = mesh.tets.data();
     auto P = [&](int64_t v) { return V3{mesh.pos[3 * v], mesh.pos[3 * v + 1], mesh.pos[3 * v + 2]}; };
-    static const int EP[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+    if (N >= (int64_t)INT32_MAX || T >= (int64_t)INT32_MAX) return "dual: mesh too large for 32-bit indices";
+    for (int64_t i = 0; i < 4 * T; ++i)
+        if (tet[i] < 0 || tet[i] >= N) return "dual: tetrahedron vertex out of range";
 
-    // ---- boundary faces: faces of exactly one tetrahedron (geom_tet.rs:101-116)
-    std::vector<std::pair<std::array<int32_t, 3>, int64_t>> fk(4 * T);
-    for (int64_t t = 0; t < T; ++t)
-        for (int k = 0; k < 4; ++k) {
-            std::array<int32_t, 3> key = {tet[4 * t + (k + 1) % 4], tet[4 * t + (k + 2) % 4], tet[4 * t + (k + 3) % 4]};
-            std::sort(key.begin(), key.end());
-            fk[4 * t + k] = {key, 4 * t + k};
-        }
-    std::sort(fk.begin(), fk.end());
-    std::vector<uint8_t> is_bface(4 * T, 0);
-    for (size_t i = 0; i < fk.size();) {
-        size_t j = i + 1;
-        while (j < fk.size() && fk[j].first == fk[i].first) ++j;
-        if (j - i == 1) is_bface[fk[i].second] = 1;
-        i = j;
+    // ---- vertex -> tetrahedra, ascending tetrahedron index per vertex
+    std::vector<int64_t> vt_ptr(N + 1, 0);
+    for (int64_t i = 0; i < 4 * T; ++i) vt_ptr[tet[i] + 1]++;
+    for (int64_t v = 0; v < N; ++v) vt_ptr[v + 1] += vt_ptr[v];
+    std::vector<int32_t> vt_idx(4 * T);
+    {
+        std::vector<int64_t> cur(vt_ptr.begin(), vt_ptr.end() - 1);
+        for (int64_t t = 0; t < T; ++t)
+            for (int k = 0; k < 4; ++k) vt_idx[cur[tet[4 * t + k]]++] = (int32_t)t;
     }
-    std::vector<std::pair<std::array<int32_t, 3>, int64_t>>().swap(fk);
-    static const int FO[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};  // counterclockwise from outside
-    std::vector<int32_t> surf;
-    for (int64_t t = 0; t < T; ++t)
-        for (int k = 0; k < 4; ++k)
-            if (is_bface[4 * t + k])
-                surf.insert(surf.end(), {tet[4 * t + FO[k][0]], tet[4 * t + FO[k][1]], tet[4 * t + FO[k][2]]});
-    for (int32_t v : surf)
-        if (v < mesh.n_pts) return "dual: a boundary face joins an interior point";
 
-    // ---- unique sorted edge list (geom_tet.rs:173-177)
-    std::vector<uint64_t> tkey(6 * T);
-    for (int64_t t = 0; t < T; ++t)
-        for (int e = 0; e < 6; ++e) {
-            const uint64_t a = (uint32_t)tet[4 * t + EP[e][0]], b = (uint32_t)tet[4 * t + EP[e][1]];
-            tkey[6 * t + e] = (std::min(a, b) << 32) | std::max(a, b);
-        }
-    std::vector<uint64_t> ekey(tkey);
-    std::sort(ekey.begin(), ekey.end());
-    ekey.erase(std::unique(ekey.begin(), ekey.end()), ekey.end());
-    const int64_t E = (int64_t)ekey.size();
-    std::vector<int32_t> teid(6 * T);
-#pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < 6 * T; ++i) teid[i] = (int32_t)(std::lower_bound(ekey.begin(), ekey.end(), tkey[i]) - ekey.begin());
-    std::vector<uint64_t>().swap(tkey);
-
-    // ---- Voronoi face pieces (geom_tet.rs:122-171): computed in parallel per chunk of
-    //      tetrahedra, accumulated serially in tetrahedron order
-    std::vector<double> e_area(E, 0.0), e_skew(3 * E, 0.0), cent_sum(3 * N, 0.0);
-    const int64_t CH = 1 << 16;
-    std::vector<double> pa_(CH * 12), pc_(CH * 36);
-    for (int64_t t0 = 0; t0 < T; t0 += CH) {
-        const int64_t t1 = std::min(T, t0 + CH);
-#pragma omp parallel for schedule(static)
-        for (int64_t t = t0; t < t1; ++t) {
-            const int32_t* tv = &tet[4 * t];
-            const V3 c_t = circumsphere3(P(tv[0]), P(tv[1]), P(tv[2]), P(tv[3]));
-            for (int e = 0; e < 6; ++e) {
-                const int li = EP[e][0], lj = EP[e][1];
-                int oth[2], no = 0;
-                for (int l = 0; l < 4; ++l)
-                    if (l != li && l != lj) oth[no++] = l;
-                const V3 pi = P(tv[li]), pj = P(tv[lj]);
-                const double dist = len3(sub3(pj, pi));
-                const V3 ee = scale3(1.0 / dist, sub3(pj, pi));
-                const V3 m = scale3(0.5, add3(pi, pj));
-                for (int side = 0; side < 2; ++side) {
-                    const V3 pa = P(tv[oth[side]]), pb = P(tv[oth[1 - side]]);
-                    const V3 c_f = circumcircle3(pi, pj, pa);
-                    V3 u = sub3(sub3(pa, m), scale3(dot3(sub3(pa, m), ee), ee));
-                    u = scale3(1.0 / len3(u), u);
-                    V3 n = cross3(ee, u);
-                    if (dot3(sub3(pb, m), n) < 0.0) n = scale3(-1.0, n);
-                    const double s1 = dot3(sub3(c_f, m), u);
-                    const double s2 = dot3(sub3(c_t, c_f), n);
-                    const double area = 0.5 * s1 * s2;
-                    const V3 cent = scale3(1.0 / 3.0, add3(m, add3(c_f, c_t)));
-                    const int64_t pidx = (t - t0) * 12 + e * 2 + side;
-                    pa_[pidx] = area;
-                    pc_[3 * pidx] = cent.x;
-                    pc_[3 * pidx + 1] = cent.y;
-                    pc_[3 * pidx + 2] = cent.z;
-                }
-            }
-        }
-        for (int64_t t = t0; t < t1; ++t) {
-            const int32_t* tv = &tet[4 * t];
-            for (int e = 0; e < 6; ++e) {
-                const int32_t vi = tv[EP[e][0]], vj = tv[EP[e][1]];
-                const V3 pi = P(vi), pj = P(vj);
-                const double dist = len3(sub3(pj, pi));
-                const V3 m = scale3(0.5, add3(pi, pj));
-                const int32_t eid = teid[6 * t + e];
-                for (int side = 0; side < 2; ++side) {
-                    const int64_t pidx = (t - t0) * 12 + e * 2 + side;
-                    const double area = pa_[pidx];
-                    const V3 cent{pc_[3 * pidx], pc_[3 * pidx + 1], pc_[3 * pidx + 2]};
-                    e_area[eid] += area;
-                    const V3 sk = scale3(area, sub3(cent, m));
-                    e_skew[3 * eid] += sk.x;
-                    e_skew[3 * eid + 1] += sk.y;
-                    e_skew[3 * eid + 2] += sk.z;
-                    const double vol = area * dist / 6.0;
-                    const V3 ci = scale3(vol * 0.75, sub3(cent, pi));
-                    const V3 cj = scale3(vol * 0.75, sub3(cent, pj));
-                    cent_sum[3 * vi] += ci.x;
-                    cent_sum[3 * vi + 1] += ci.y;
-                    cent_sum[3 * vi + 2] += ci.z;
-                    cent_sum[3 * vj] += cj.x;
-                    cent_sum[3 * vj + 1] += cj.y;
-                    cent_sum[3 * vj + 2] += cj.z;
-                }
-            }
-        }
-    }
-    std::vector<int32_t>().swap(teid);
-
-    // ---- neighbour CSR and per-face data (geom_tet.rs:178-206)
+    // ---- neighbour CSR (geom_tet.rs:173-206): the sorted edge list read per vertex is its
+    //      neighbours in ascending order, so the lists come from the incident tetrahedra directly
     d = Dual();
     d.n_tot = N;
     d.n_pts = mesh.n_pts;
-    d.n_dir = 2 * E;
-    const int64_t D = 2 * E;
+    auto gather = [&](int64_t v, std::vector<int32_t>& buf) {
+        buf.clear();
+        for (int64_t q = vt_ptr[v]; q < vt_ptr[v + 1]; ++q) {
+            const int32_t* tv = &tet[4 * (int64_t)vt_idx[q]];
+            for (int k = 0; k < 4; ++k)
+                if (tv[k] != v) buf.push_back(tv[k]);
+        }
+        std::sort(buf.begin(), buf.end());
+        buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+    };
     d.nbr_ptr.assign(N + 1, 0);
-    for (int64_t e = 0; e < E; ++e) {
-        d.nbr_ptr[(ekey[e] >> 32) + 1]++;
-        d.nbr_ptr[(ekey[e] & 0xffffffffULL) + 1]++;
+#pragma omp parallel
+    {
+        std::vector<int32_t> buf;
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t v = 0; v < N; ++v) {
+            gather(v, buf);
+            d.nbr_ptr[v + 1] = (int64_t)buf.size();
+        }
     }
     for (int64_t v = 0; v < N; ++v) d.nbr_ptr[v + 1] += d.nbr_ptr[v];
+    const int64_t D = d.nbr_ptr[N];
+    d.n_dir = D;
     d.nbr_idx.assign(D, 0);
+#pragma omp parallel
+    {
+        std::vector<int32_t> buf;
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t v = 0; v < N; ++v) {
+            gather(v, buf);
+            std::copy(buf.begin(), buf.end(), d.nbr_idx.begin() + d.nbr_ptr[v]);
+        }
+    }
+    auto nbr_pos = [&](int64_t v, int32_t n) {  // position of n in v's list (present by construction)
+        return (int64_t)(std::lower_bound(d.nbr_idx.begin() + d.nbr_ptr[v], d.nbr_idx.begin() + d.nbr_ptr[v + 1], n) - d.nbr_idx.begin());
+    };
+
+    // ---- Voronoi face pieces of every tetrahedron edge (geom_tet.rs:122-171)
+    // every entry is written below; left uninitialised so that the parallel loop first-touches it
+    std::unique_ptr<double[]> pc_area(new double[12 * T]), pc_cent(new double[36 * T]);
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < T; ++t) {
+        const int32_t* tv = &tet[4 * t];
+        const V3 c_t = circumsphere3(P(tv[0]), P(tv[1]), P(tv[2]), P(tv[3]));
+        for (int e = 0; e < 6; ++e) {
+            double a[2];
+            V3 c[2];
+            face_pieces(mesh, tv, c_t, e, a, c);
+            for (int side = 0; side < 2; ++side) {
+                const int64_t q = 12 * t + 2 * e + side;
+                pc_area[q] = a[side];
+                pc_cent[3 * q] = c[side].x;
+                pc_cent[3 * q + 1] = c[side].y;
+                pc_cent[3 * q + 2] = c[side].z;
+            }
+        }
+    }
+
+    // ---- per edge (a, b), a < b: area and skew summed over its tetrahedra in ascending order,
+    //      then the data of both directed entries
     d.nbr_rev.assign(D, 0);
     d.dist.assign(D, 0.0);
     d.area.assign(D, 0.0);
     d.norm.assign(3 * D, 0.0);
     d.skew.assign(3 * D, 0.0);
-    d.cvol.assign(N, 0.0);
-    std::vector<int64_t> cur(d.nbr_ptr.begin(), d.nbr_ptr.end() - 1);
-    for (int64_t e = 0; e < E; ++e) {
-        const int64_t a = (int64_t)(ekey[e] >> 32), b = (int64_t)(ekey[e] & 0xffffffffULL);
-        const V3 pa = P(a), pb = P(b);
-        const double dist = len3(sub3(pb, pa));
-        const V3 nrm = scale3(1.0 / dist, sub3(pb, pa));
-        const double area = e_area[e];
-        const V3 ss{e_skew[3 * e], e_skew[3 * e + 1], e_skew[3 * e + 2]};
-        const V3 skew = (std::fabs(area) > 1e-12 * dist * dist) ? scale3(1.0 / area, ss) : V3{0.0, 0.0, 0.0};
-        const int64_t ia = cur[a]++, ib = cur[b]++;
-        d.nbr_idx[ia] = (int32_t)b;
-        d.nbr_idx[ib] = (int32_t)a;
-        d.nbr_rev[ia] = ib;
-        d.nbr_rev[ib] = ia;
-        d.dist[ia] = d.dist[ib] = dist;
-        d.area[ia] = d.area[ib] = area;
-        const V3 mn = scale3(-1.0, nrm);
-        d.norm[ia] = nrm.x;
-        d.norm[D + ia] = nrm.y;
-        d.norm[2 * D + ia] = nrm.z;
-        d.norm[ib] = mn.x;
-        d.norm[D + ib] = mn.y;
-        d.norm[2 * D + ib] = mn.z;
-        d.skew[ia] = d.skew[ib] = skew.x;
-        d.skew[D + ia] = d.skew[D + ib] = skew.y;
-        d.skew[2 * D + ia] = d.skew[2 * D + ib] = skew.z;
-        d.cvol[a] += area * dist / 6.0;
-        d.cvol[b] += area * dist / 6.0;
-    }
-    d.cskew.assign(3 * N, 0.0);
-    for (int64_t v = 0; v < N; ++v) {
-        const double s = 1.0 / d.cvol[v];
-        d.cskew[v] = s * cent_sum[3 * v];
-        d.cskew[N + v] = s * cent_sum[3 * v + 1];
-        d.cskew[2 * N + v] = s * cent_sum[3 * v + 2];
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t a = 0; a < N; ++a) {
+        for (int64_t ia = d.nbr_ptr[a]; ia < d.nbr_ptr[a + 1]; ++ia) {
+            const int32_t b = d.nbr_idx[ia];
+            if (b < a) continue;
+            double s_area = 0.0, s_x = 0.0, s_y = 0.0, s_z = 0.0;
+            int64_t qa = vt_ptr[a], qb = vt_ptr[b];
+            while (qa < vt_ptr[a + 1] && qb < vt_ptr[b + 1]) {  // tetrahedra holding both ends
+                if (vt_idx[qa] < vt_idx[qb]) { ++qa; continue; }
+                if (vt_idx[qb] < vt_idx[qa]) { ++qb; continue; }
+                const int64_t t = vt_idx[qa];
+                ++qa;
+                ++qb;
+                const int32_t* tv = &tet[4 * t];
+                int e = 0;
+                while (!((tv[kEdgeEnds[e][0]] == a && tv[kEdgeEnds[e][1]] == b) || (tv[kEdgeEnds[e][0]] == b && tv[kEdgeEnds[e][1]] == a))) ++e;
+                const V3 m = scale3(0.5, add3(P(tv[kEdgeEnds[e][0]]), P(tv[kEdgeEnds[e][1]])));
+                for (int side = 0; side < 2; ++side) {
+                    const int64_t q = 12 * t + 2 * e + side;
+                    const double area = pc_area[q];
+                    const V3 cent{pc_cent[3 * q], pc_cent[3 * q + 1], pc_cent[3 * q + 2]};
+                    s_area += area;
+                    const V3 sk = scale3(area, sub3(cent, m));
+                    s_x += sk.x;
+                    s_y += sk.y;
+                    s_z += sk.z;
+                }
+            }
+            const V3 pa = P(a), pb = P(b);
+            const double dist = len3(sub3(pb, pa));
+            const V3 nrm = scale3(1.0 / dist, sub3(pb, pa));
+            const V3 skew = (std::fabs(s_area) > 1e-12 * dist * dist) ? scale3(1.0 / s_area, V3{s_x, s_y, s_z}) : V3{0.0, 0.0, 0.0};
+            const int64_t ib = nbr_pos(b, (int32_t)a);
+            d.nbr_rev[ia] = ib;
+            d.nbr_rev[ib] = ia;
+            d.dist[ia] = d.dist[ib] = dist;
+            d.area[ia] = d.area[ib] = s_area;
+            const V3 mn = scale3(-1.0, nrm);
+            d.norm[ia] = nrm.x;
+            d.norm[D + ia] = nrm.y;
+            d.norm[2 * D + ia] = nrm.z;
+            d.norm[ib] = mn.x;
+            d.norm[D + ib] = mn.y;
+            d.norm[2 * D + ib] = mn.z;
+            d.skew[ia] = d.skew[ib] = skew.x;
+            d.skew[D + ia] = d.skew[D + ib] = skew.y;
+            d.skew[2 * D + ia] = d.skew[2 * D + ib] = skew.z;
+        }
     }
 
+    // ---- per vertex: control volume (faces in neighbour order) and its centroid offset (pieces
+    //      in tetrahedron, edge, side order)
+    d.cvol.assign(N, 0.0);
+    d.cskew.assign(3 * N, 0.0);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t v = 0; v < N; ++v) {
+        double vol = 0.0;
+        for (int64_t i = d.nbr_ptr[v]; i < d.nbr_ptr[v + 1]; ++i) vol += d.area[i] * d.dist[i] / 6.0;
+        d.cvol[v] = vol;
+        double cx = 0.0, cy = 0.0, cz = 0.0;
+        for (int64_t q = vt_ptr[v]; q < vt_ptr[v + 1]; ++q) {
+            const int64_t t = vt_idx[q];
+            const int32_t* tv = &tet[4 * t];
+            for (int e = 0; e < 6; ++e) {
+                const int32_t vi = tv[kEdgeEnds[e][0]], vj = tv[kEdgeEnds[e][1]];
+                if (vi != v && vj != v) continue;
+                const V3 pi = P(vi), pj = P(vj);
+                const double dist = len3(sub3(pj, pi));
+                const V3 pv = vi == v ? pi : pj;
+                for (int side = 0; side < 2; ++side) {
+                    const int64_t pq = 12 * t + 2 * e + side;
+                    const double pvol = pc_area[pq] * dist / 6.0;
+                    const V3 c = scale3(pvol * 0.75, sub3(V3{pc_cent[3 * pq], pc_cent[3 * pq + 1], pc_cent[3 * pq + 2]}, pv));
+                    cx += c.x;
+                    cy += c.y;
+                    cz += c.z;
+                }
+            }
+        }
+        const double s = 1.0 / vol;
+        d.cskew[v] = s * cx;
+        d.cskew[N + v] = s * cy;
+        d.cskew[2 * N + v] = s * cz;
+    }
+    pc_area.reset();
+    pc_cent.reset();
+
+    // ---- boundary faces: faces of exactly one tetrahedron (geom_tet.rs:101-116), in
+    //      (tetrahedron, face) order; a face is shared when another tetrahedron at its first
+    //      vertex holds the other two
+    std::vector<uint8_t> bmask(T, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < T; ++t) {
+        const int32_t* tv = &tet[4 * t];
+        uint8_t mask = 0;
+        for (int k = 0; k < 4; ++k) {
+            const int32_t x = tv[(k + 1) % 4], y = tv[(k + 2) % 4], z = tv[(k + 3) % 4];
+            bool shared = false;
+            for (int64_t q = vt_ptr[x]; q < vt_ptr[x + 1] && !shared; ++q) {
+                const int64_t t2 = vt_idx[q];
+                if (t2 == t) continue;
+                const int32_t* w = &tet[4 * t2];
+                bool hy = false, hz = false;
+                for (int l = 0; l < 4; ++l) {
+                    hy = hy || w[l] == y;
+                    hz = hz || w[l] == z;
+                }
+                shared = hy && hz;
+            }
+            if (!shared) mask |= (uint8_t)(1u << k);
+        }
+        bmask[t] = mask;
+    }
+    static const int FO[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};  // counterclockwise from outside
+    std::vector<int32_t> surf;
+    for (int64_t t = 0; t < T; ++t)
+        if (bmask[t])
+            for (int k = 0; k < 4; ++k)
+                if (bmask[t] & (1u << k)) surf.insert(surf.end(), {tet[4 * t + FO[k][0]], tet[4 * t + FO[k][1]], tet[4 * t + FO[k][2]]});
+    for (int32_t v : surf)
+        if (v < mesh.n_pts) return "dual: a boundary face joins an interior point";
     // ---- boundary sub-faces (geom_tet.rs:208-259)
     const int64_t S = (int64_t)surf.size() / 3;
     d.bnd_ptr.assign(N + 1, 0);
