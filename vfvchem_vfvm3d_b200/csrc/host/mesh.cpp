@@ -72,6 +72,50 @@ inline i128 insphere_i(const IP& a, const IP& b, const IP& c, const IP& d, const
     return lb * m_acd - la * m_bcd + ld * m_abc - lc * m_abd;
 }
 
+// Floating-point filters of the two predicates: the same determinant in double with a bound on its
+// rounding error, |fl(det) - det| <= c eps * permanent (c is at most about 12 for these expression
+// trees; 1e-14 ~ 90 eps leaves a wide margin). Outside the bound the sign is certain; inside it the
+// exact 128-bit evaluation decides, so every sign equals the exact one.
+inline int orient_sgn(const IP& a, const IP& b, const IP& c, const IP& d) {
+    const double ax = (double)(a.x - d.x), ay = (double)(a.y - d.y), az = (double)(a.z - d.z);
+    const double bx = (double)(b.x - d.x), by = (double)(b.y - d.y), bz = (double)(b.z - d.z);
+    const double cx = (double)(c.x - d.x), cy = (double)(c.y - d.y), cz = (double)(c.z - d.z);
+    const double det = ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx);
+    const double perm = std::fabs(ax) * (std::fabs(by * cz) + std::fabs(bz * cy)) + std::fabs(ay) * (std::fabs(bx * cz) + std::fabs(bz * cx)) +
+                        std::fabs(az) * (std::fabs(bx * cy) + std::fabs(by * cx));
+    const double bound = 1e-14 * perm;
+    if (det > bound) return 1;
+    if (det < -bound) return -1;
+    const i128 e = orient_i(a, b, c, d);
+    return (e > 0) - (e < 0);
+}
+
+inline int insphere_sgn(const IP& a, const IP& b, const IP& c, const IP& d, const IP& e) {
+    const double ax = (double)(a.x - e.x), ay = (double)(a.y - e.y), az = (double)(a.z - e.z);
+    const double bx = (double)(b.x - e.x), by = (double)(b.y - e.y), bz = (double)(b.z - e.z);
+    const double cx = (double)(c.x - e.x), cy = (double)(c.y - e.y), cz = (double)(c.z - e.z);
+    const double dx = (double)(d.x - e.x), dy = (double)(d.y - e.y), dz = (double)(d.z - e.z);
+    const double la = ax * ax + ay * ay + az * az, lb = bx * bx + by * by + bz * bz;
+    const double lc = cx * cx + cy * cy + cz * cz, ld = dx * dx + dy * dy + dz * dz;
+    auto det3d = [](double px, double py, double pz, double qx, double qy, double qz, double rx, double ry, double rz, double& perm) {
+        perm = std::fabs(px) * (std::fabs(qy * rz) + std::fabs(qz * ry)) + std::fabs(py) * (std::fabs(qx * rz) + std::fabs(qz * rx)) +
+               std::fabs(pz) * (std::fabs(qx * ry) + std::fabs(qy * rx));
+        return px * (qy * rz - qz * ry) - py * (qx * rz - qz * rx) + pz * (qx * ry - qy * rx);
+    };
+    double p_bcd, p_acd, p_abd, p_abc;
+    const double m_bcd = det3d(bx, by, bz, cx, cy, cz, dx, dy, dz, p_bcd);
+    const double m_acd = det3d(ax, ay, az, cx, cy, cz, dx, dy, dz, p_acd);
+    const double m_abd = det3d(ax, ay, az, bx, by, bz, dx, dy, dz, p_abd);
+    const double m_abc = det3d(ax, ay, az, bx, by, bz, cx, cy, cz, p_abc);
+    const double det = lb * m_acd - la * m_bcd + ld * m_abc - lc * m_abd;
+    const double perm = lb * p_acd + la * p_bcd + ld * p_abc + lc * p_abd;
+    const double bound = 1e-14 * perm;
+    if (det > bound) return 1;
+    if (det < -bound) return -1;
+    const i128 x = insphere_i(a, b, c, d, e);
+    return (x > 0) - (x < 0);
+}
+
 inline IP to_ip(const double* p) {
     return IP{(int64_t)std::llround(std::ldexp(p[0], kQuantBits)), (int64_t)std::llround(std::ldexp(p[1], kQuantBits)),
               (int64_t)std::llround(std::ldexp(p[2], kQuantBits))};
@@ -189,7 +233,7 @@ std::string delaunay(Mesh& mesh) {
     tv.reserve(7 * N + 64);
     ta.reserve(7 * N + 64);
     tv.push_back({(int32_t)N, (int32_t)N + 1, (int32_t)N + 2, (int32_t)N + 3});
-    if (orient_i(P[N], P[N + 1], P[N + 2], P[N + 3]) < 0) std::swap(tv[0][0], tv[0][1]);
+    if (orient_sgn(P[N], P[N + 1], P[N + 2], P[N + 3]) < 0) std::swap(tv[0][0], tv[0][1]);
     ta.push_back({-1, -1, -1, -1});
     alive.push_back(1);
     incav.push_back(0);
@@ -213,8 +257,9 @@ std::string delaunay(Mesh& mesh) {
     std::vector<int32_t> cav;
     struct BF { int32_t t, k; };
     std::vector<BF> bfaces;
-    struct OpenEdge { int32_t a, b, t, m; };
-    std::vector<OpenEdge> open;
+    struct EdgeSlot { int64_t key; int32_t t, m; };  // key -1: empty; t -1: no tetrahedron waiting
+    std::vector<EdgeSlot> etab;
+    std::vector<int32_t> eused;
     std::vector<int32_t> newt;
     int32_t last = 0;
     unsigned turn = 0;
@@ -234,7 +279,7 @@ std::string delaunay(Mesh& mesh) {
                     for (int k = 0; k < 4 && in; ++k) {
                         tet_pts(s, q);
                         q[k] = p;
-                        in = orient_i(q[0], q[1], q[2], q[3]) >= 0;
+                        in = orient_sgn(q[0], q[1], q[2], q[3]) >= 0;
                     }
                     if (in) t = s;
                 }
@@ -247,7 +292,7 @@ std::string delaunay(Mesh& mesh) {
                 const int k = (int)((l + turn) & 3u);
                 tet_pts(t, q);
                 q[k] = p;
-                if (orient_i(q[0], q[1], q[2], q[3]) < 0) {
+                if (orient_sgn(q[0], q[1], q[2], q[3]) < 0) {
                     const int32_t o = ta[t][k];
                     if (o < 0) return "delaunay: point outside the super tetrahedron";
                     t = o;
@@ -271,7 +316,7 @@ std::string delaunay(Mesh& mesh) {
                 const int32_t o = ta[c][k];
                 if (o < 0 || incav[o]) continue;
                 tet_pts(o, q);
-                if (insphere_i(q[0], q[1], q[2], q[3], p) > 0) {
+                if (insphere_sgn(q[0], q[1], q[2], q[3], p) > 0) {
                     incav[o] = 1;
                     cav.push_back(o);
                 }
@@ -287,7 +332,7 @@ std::string delaunay(Mesh& mesh) {
                     if (o >= 0 && incav[o]) continue;
                     tet_pts(c, q);
                     q[k] = p;
-                    if (orient_i(q[0], q[1], q[2], q[3]) > 0) continue;
+                    if (orient_sgn(q[0], q[1], q[2], q[3]) > 0) continue;
                     if (o < 0) return "delaunay: cavity reaches the super tetrahedron hull";
                     incav[o] = 1;
                     cav.push_back(o);
@@ -316,7 +361,12 @@ std::string delaunay(Mesh& mesh) {
                 incav.push_back(0);
             }
         }
-        open.clear();
+        // edges of the cavity boundary in a hash table sized for load <= 1/4
+        int ebits = 4;
+        while ((size_t{1} << ebits) < 6 * bfaces.size()) ++ebits;
+        const uint64_t emask = (uint64_t{1} << ebits) - 1;
+        if (etab.size() < (size_t{1} << ebits)) etab.assign(size_t{1} << ebits, EdgeSlot{-1, -1, 0});
+        int64_t n_open = 0;
         for (size_t i = 0; i < bfaces.size(); ++i) {
             const int32_t c = bfaces[i].t, k = bfaces[i].k, nt = newt[i];
             std::array<int32_t, 4> nv = tv[c];
@@ -337,21 +387,29 @@ std::string delaunay(Mesh& mesh) {
                 int32_t e2[2], ne = 0;
                 for (int l = 0; l < 4; ++l)
                     if (l != k && l != mm) e2[ne++] = nv[l];
-                const int32_t a = std::min(e2[0], e2[1]), b = std::max(e2[0], e2[1]);
-                bool matched = false;
-                for (size_t s = 0; s < open.size(); ++s)
-                    if (open[s].a == a && open[s].b == b) {
-                        ta[nt][mm] = open[s].t;
-                        ta[open[s].t][open[s].m] = nt;
-                        open[s] = open.back();
-                        open.pop_back();
-                        matched = true;
-                        break;
-                    }
-                if (!matched) open.push_back({a, b, nt, mm});
+                const int64_t key = ((int64_t)std::min(e2[0], e2[1]) << 32) | (int64_t)std::max(e2[0], e2[1]);
+                uint64_t h = ((uint64_t)key * 0x9E3779B97F4A7C15ULL) >> (64 - ebits);
+                while (etab[h].key != key && etab[h].key != -1) h = (h + 1) & emask;
+                EdgeSlot& sl = etab[h];
+                if (sl.key == -1) {
+                    sl.key = key;
+                    eused.push_back((int32_t)h);
+                }
+                if (sl.t >= 0) {  // the other new tetrahedron on this edge
+                    ta[nt][mm] = sl.t;
+                    ta[sl.t][sl.m] = nt;
+                    sl.t = -1;
+                    --n_open;
+                } else {
+                    sl.t = nt;
+                    sl.m = mm;
+                    ++n_open;
+                }
             }
         }
-        if (!open.empty()) return "delaunay: cavity boundary is not closed";
+        for (int32_t h : eused) etab[h] = EdgeSlot{-1, -1, 0};
+        eused.clear();
+        if (n_open != 0) return "delaunay: cavity boundary is not closed";
         for (int32_t c : cav) {
             alive[c] = 0;
             incav[c] = 0;
