@@ -143,6 +143,12 @@ def extras_transport(ctx, count):
                         "GMRES(30)+ILU(0) mixed to 1e-10 relres per mesh and step; host arrays in/out"}
 
 
+# DRAM bytes (read + write) of one k_spmv<double> launch on the 10^6-vertex heat matrix with 4
+# lanes per row, from one ncu capture of that launch (profiles/k_spmv_1M.md); reported as the
+# roofline's traffic only when the bench runs that same matrix and lane count.
+SPMV_TRAFFIC_N100_4LANES = 209.2e6
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -386,7 +392,9 @@ def main():
         "spmv_fp64_gbs": gbs64, "spmv_fp32_gbs": gbs32, "spmv_fp64_ms": sp64 * 1e3, "spmv_fp32_ms": sp32 * 1e3,
         "assembly_ms": asm_s * 1e3, "mesh_setup_s": t_mesh,
         "roofline": {"bound": "hbm", "kernel": f"k_spmv<double> (CSR, {lanes64} lanes/row)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
-                     "frac": gbs64 / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": gbs64 / peak, "peak_kind": peak_kind,
+                     "traffic": SPMV_TRAFFIC_N100_4LANES if (args.n == 100 and lanes64 == 4) else None,
+                     "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                      "algorithmic_bytes_per_launch": bytes64},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * nnz + 16 * n, "d2h_bytes_per_step": 8 * n, "err": e2e_err},

@@ -3,12 +3,13 @@
     python -m vfvchem_vfvm3d_b200.workloads heat --n 100 --solves 1 --precision mixed --engine 2
     python -m vfvchem_vfvm3d_b200.workloads flow --n 32 --picard 2 --precision mixed
     python -m vfvchem_vfvm3d_b200.workloads transport --count 16 --steps 5
-    python -m vfvchem_vfvm3d_b200.workloads spmv --n 100 --reps 3
+    python -m vfvchem_vfvm3d_b200.workloads spmv --n 100 --reps 3 --lanes 4,4
 
 heat: the heterogeneous steady heat system (n^3 jittered cube, log k ~ N(0,1), q ~ U[0,1]) solved
 by GMRES(50) + ILU(0) to relres 1e-10; flow: the lid-driven cavity's damped Picard loop with
 GMRES(100) + 4x4 block-Jacobi; transport: the batched transient transport (meshes of 2,000-50,000
-vertices); spmv: the heat matrix's SpMV, FP64 then FP32. Each prints one summary line.
+vertices); spmv: the heat matrix's SpMV, FP64 then FP32 (lanes per row autotuned unless --lanes gives them;
+with --lanes the only k_spmv launches are the timed ones). Each prints one summary line.
 """
 from __future__ import annotations
 
@@ -78,7 +79,11 @@ def spmv(args):
     h = SteadyHeatGpu(prob.mesh, prob.bnd_kind, ctx=ctx)
     h.assemble(prob.k, prob.q, prob.s, prob.T0, prob.bc_val)
     p = h.pattern
-    lanes = p.autotune()
+    if args.lanes:
+        lanes = tuple(int(v) for v in args.lanes.split(","))
+        p.set_spmv_lanes(*lanes)
+    else:
+        lanes = p.autotune()
     x = torch.randn(p.n, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
     x32, y32 = x.float(), torch.empty(p.n, dtype=torch.float32, device="cuda")
@@ -109,6 +114,7 @@ def main(argv=None):
     a = sub.add_parser("spmv")
     a.add_argument("--n", type=int, default=100)
     a.add_argument("--reps", type=int, default=3)
+    a.add_argument("--lanes", default="", help="lanes per row 'f64,f32' instead of the autotuner (e.g. 4,4)")
     args = ap.parse_args(argv)
     {"heat": heat, "flow": flow, "transport": transport, "spmv": spmv}[args.case](args)
 
