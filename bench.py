@@ -4,8 +4,12 @@ Workload (one "step"): the 1,000,000-vertex heterogeneous steady heat system (10
 cube, log k ~ N(0,1), q ~ U[0,1], Dirichlet T=0/1 on x=0/1, zero flux elsewhere) solved by
 GMRES(50) + ILU(0) to 1e-8 relative 2-norm error against a reference solution — the
 FP32-inner / FP64-refinement solver is the timed `value`; the plain FP64 solver is timed beside
-it. Inputs are resident in HBM; the matrix (15.3 M non-zeros, 190 MB of CSR) exceeds the 126 MB
-L2, so no L2 flush is needed between steps.
+it. Inputs are resident in HBM; the matrix (16.1 M non-zeros, 193 MB of FP64 values and
+columns) exceeds the 126 MB L2, so no L2 flush is needed between steps.
+
+`roofline` is the float ILU(0) level sweeps, the largest share of the mixed solve's kernel time,
+timed alone with CUDA events on the library's stream; `roofline_spmv` is the FP64 SpMV timed the
+same way.
 
 `--impl reference` times the reference's own algorithm for this path on the host cores
 (Jacobi-preconditioned restarted GMRES(50), FP64, the oracle port), on a bounded sample.
@@ -328,6 +332,17 @@ def main():
     gbs64 = bytes64 / sp64 / 1e9
     gbs32 = bytes32 / sp32 / 1e9
 
+    # ILU(0) sweeps with the float factor, timed alone: the mixed solve's preconditioner, whose
+    # 2 x levels launches per apply are the largest share of the solve's kernel time. Algorithmic
+    # bytes per apply: L+U values and columns (8 nnz), row pointer, diagonal position and
+    # permutation per sweep (2 x 12 n), r in and z out (8 n); the intermediate t stays in L2.
+    rs32, ts32, zs32 = xs32.clone(), torch.empty_like(xs32), torch.empty_like(xs32)
+    torch.cuda.synchronize()
+    ilu_nlev = pat.ilu0_apply_device_f32(rs32.data_ptr(), ts32.data_ptr(), zs32.data_ptr())
+    ilu_s = spmv_time(lambda: pat.ilu0_apply_device_f32(rs32.data_ptr(), ts32.data_ptr(), zs32.data_ptr()), reps=20)
+    bytes_ilu32 = 8 * nnz + 28 * n
+    gbs_ilu32 = bytes_ilu32 / ilu_s / 1e9
+
     # assembly (gradients + face coefficients + b), timed alone
     def asm():
         heat.assemble_device(k_d.data_ptr(), q_d.data_ptr(), s_d.data_ptr(), T_d.data_ptr(), bc_d.data_ptr())
@@ -391,11 +406,14 @@ def main():
         "err_mixed": e_mx, "err_fp64": e_64, "ref_relres": info_ref.relres,
         "spmv_fp64_gbs": gbs64, "spmv_fp32_gbs": gbs32, "spmv_fp64_ms": sp64 * 1e3, "spmv_fp32_ms": sp32 * 1e3,
         "assembly_ms": asm_s * 1e3, "mesh_setup_s": t_mesh,
-        "roofline": {"bound": "hbm", "kernel": f"k_spmv<double> (CSR, {lanes64} lanes/row)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
-                     "frac": gbs64 / peak, "peak_kind": peak_kind,
-                     "traffic": SPMV_TRAFFIC_N100_4LANES if (args.n == 100 and lanes64 == 4) else None,
-                     "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
-                     "algorithmic_bytes_per_launch": bytes64},
+        "roofline": {"bound": "hbm", "kernel": f"k_ilu0_level<float> ({2 * ilu_nlev} level launches per apply)", "achieved": gbs_ilu32,
+                     "peak": peak, "unit": "GB/s", "frac": gbs_ilu32 / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_apply": bytes_ilu32, "apply_us": ilu_s * 1e6, "launch_us": ilu_s * 1e6 / (2 * ilu_nlev)},
+        "roofline_spmv": {"bound": "hbm", "kernel": f"k_spmv<double> (CSR, {lanes64} lanes/row)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
+                          "frac": gbs64 / peak, "peak_kind": peak_kind,
+                          "traffic": SPMV_TRAFFIC_N100_4LANES if (args.n == 100 and lanes64 == 4) else None,
+                          "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+                          "algorithmic_bytes_per_launch": bytes64},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * nnz + 16 * n, "d2h_bytes_per_step": 8 * n, "err": e2e_err},
         "gpu_launches": int(launches_mx),

@@ -137,6 +137,10 @@ int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t
 int vfv_pattern_set_spmv_lanes(vfv_ctx* ctx, vfv_pattern* p, int32_t lanes64, int32_t lanes32);
 /* z = M^-1 r for the ILU(0) preconditioner of the pattern's current values (device arrays, double) */
 int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels);
+/* z = M^-1 r with the float copy of the factor (the mixed-precision inner preconditioner), exposed
+ * for measurement: enqueued on the context's stream without synchronising; t is a work vector of n
+ * floats that must not alias r or z (r and z may alias). */
+int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const float* r, float* t, float* z, int32_t* levels);
 /* Same result as vfv_ilu0_apply_device, allocating nothing. No counterpart in the reference: for
  * callers that may not allocate device memory while they run (a time-step loop under a fixed
  * memory budget, a host framework whose allocator owns the device memory, code that must not

@@ -186,6 +186,33 @@ def test_ilu0_apply_matches_oracle(gpu_ctx, c1h_system, c1_hetero, order):
     assert _rel(zd.cpu().numpy(), zo) <= 1e-12
 
 
+def test_ilu0_apply_f32_matches_oracle(gpu_ctx, c1h_system, c1_hetero):
+    """The float sweeps of the mixed-precision solver: same levels as the double apply, the
+    oracle's ILU(0) on the same permutation to float accuracy, identical bits on a repeat call,
+    and a work vector that aliases r or z is rejected."""
+    import torch
+    from vfvchem_vfvm3d_b200 import Pattern, VFVChemError
+    (rp, ci, va), _, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    r = np.random.default_rng(11).standard_normal(c1_hetero.n)
+    rd = torch.tensor(r, device="cuda", dtype=torch.float32)
+    td = torch.empty_like(rd)
+    zd = torch.empty_like(rd)
+    z2 = torch.empty_like(rd)
+    torch.cuda.synchronize()
+    nlev = p.ilu0_apply_device_f32(rd.data_ptr(), td.data_ptr(), zd.data_ptr())
+    assert p.ilu0_apply_device_f32(rd.data_ptr(), td.data_ptr(), z2.data_ptr()) == nlev
+    gpu_ctx.synchronize()
+    perm, lev_ptr = p.ilu0_ordering(0)
+    assert lev_ptr.size == nlev + 1
+    zo = oracle.Ilu0(rp, ci, va, perm).apply(r.astype(np.float32).astype(np.float64))
+    assert _rel(zd.cpu().numpy().astype(np.float64), zo) <= 1e-4
+    assert torch.equal(zd, z2)
+    with pytest.raises(VFVChemError):
+        p.ilu0_apply_device_f32(rd.data_ptr(), rd.data_ptr(), zd.data_ptr())
+
+
 @pytest.mark.parametrize("engine", [0, 1])
 @pytest.mark.parametrize("precond", [0, 1, 2])
 @pytest.mark.parametrize("precision", [0, 1])

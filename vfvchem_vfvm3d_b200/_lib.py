@@ -73,6 +73,7 @@ SIGNATURES = [
     ("vfv_spmv_device", C.c_int, [_P, _P, _P, _P]),
     ("vfv_spmv_device_f32", C.c_int, [_P, _P, _P, _P]),
     ("vfv_ilu0_apply_device", C.c_int, [_P, _P, C.c_int, _P, _P, _I32P]),
+    ("vfv_ilu0_apply_device_f32", C.c_int, [_P, _P, C.c_int, _P, _P, _P, _I32P]),
     ("vfv_pattern_autotune", C.c_int, [_P, _P, _I32P, _I32P]),
     ("vfv_pattern_set_spmv_lanes", C.c_int, [_P, _P, C.c_int32, C.c_int32]),
     ("vfv_ilu0_ordering", C.c_int, [_P, _P, C.c_int, _I32P, _I32P, _I32P]),

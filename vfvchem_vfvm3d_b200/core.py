@@ -193,6 +193,14 @@ class Pattern:
                                                                C.c_void_p(z_ptr), C.byref(lev)))
         return lev.value
 
+    def ilu0_apply_device_f32(self, r_ptr: int, t_ptr: int, z_ptr: int, order: int = L.ILU_MULTICOLOR) -> int:
+        """z = M^-1 r with the float factor, enqueued on the context's stream (no synchronisation);
+        t is a float work vector of n entries. Returns the number of colour levels."""
+        lev = C.c_int32()
+        _check(self.ctx.handle, L.load().vfv_ilu0_apply_device_f32(self.ctx.handle, self._h, int(order), C.c_void_p(r_ptr),
+                                                                   C.c_void_p(t_ptr), C.c_void_p(z_ptr), C.byref(lev)))
+        return lev.value
+
     def autotune(self):
         """Pick the SpMV lanes per row (double, float) by measurement; call before the first solve."""
         a, b = C.c_int32(), C.c_int32()

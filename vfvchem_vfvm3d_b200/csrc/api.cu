@@ -1365,6 +1365,31 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
     return VFV_OK;
 }
 
+// z = M^-1 r with the float copy of the ILU(0) factor: the level kernels the mixed-precision solver
+// runs. Enqueued on the context's stream with no synchronisation; t is the caller's work vector of
+// n floats, so calls after the first (which builds the factor) allocate nothing and can be timed
+// back to back.
+int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const float* r, float* t, float* z, int32_t* levels) {
+    if (!ctx || !p || !r || !t || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (t == r || t == z) return set_err(ctx, VFV_BAD_INPUT, "the work vector aliases r or z");
+    if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
+    auto it = p->ilu.find(ilu_order);
+    if (it == p->ilu.end()) {
+        auto S = std::make_unique<IluStruct>();
+        int rc = build_ilu_struct(ctx, p, ilu_order, *S);
+        if (rc) return rc;
+        it = p->ilu.emplace(ilu_order, std::move(S)).first;
+    }
+    IluStruct& S = *it->second;
+    int rc = ilu_refresh(ctx, p, S, true);
+    if (rc) return rc;
+    ilu_apply<float>(ctx->stream, S, S.lu32.p, r, t, z, nullptr);
+    ctx->launches += 2 * S.nlev;
+    CK(cudaGetLastError());
+    if (levels) *levels = S.nlev;
+    return VFV_OK;
+}
+
 // ---------------------------------------------------------------- ILU(0) apply without allocation
 // For callers that may not allocate device memory once they are running: code that drives the
 // solver from inside a time-step loop under a fixed memory budget, or from a host framework whose
