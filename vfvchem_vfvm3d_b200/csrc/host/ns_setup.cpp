@@ -44,18 +44,24 @@ void gc_push_order(const Dual& d, int64_t v, std::vector<GcEnt>& e) {
     }
 }
 
-// stable sort by vertex, then sums of equal vertices in push order (slice::sort_by_key + dedup_by)
-void gc_merge(std::vector<GcEnt>& e) {
-    std::stable_sort(e.begin(), e.end(), [](const GcEnt& a, const GcEnt& b) { return a.vid < b.vid; });
-    size_t w = 0;
-    for (size_t r = 0; r < e.size(); ++r) {
-        if (w > 0 && e[w - 1].vid == e[r].vid) {
-            for (int q = 0; q < 3; ++q) e[w - 1].c[q] += e[r].c[q];
+// The merge of slice::sort_by_key + dedup_by: a stable sort by vertex, then the entries of equal
+// vertices summed in push order. Computed without sorting the entries: the first entry of a vertex
+// keeps its place in `out` and the later ones are added to it in push order (the same sums), then
+// the distinct vertices are sorted. stamp[u] == v marks vertex u as seen while merging vertex v's
+// list; slot[u] is its place in `out`.
+void gc_merge(const std::vector<GcEnt>& e, int32_t v, std::vector<int32_t>& stamp, std::vector<int32_t>& slot, std::vector<GcEnt>& out) {
+    out.clear();
+    for (const GcEnt& g : e) {
+        if (stamp[g.vid] != v) {
+            stamp[g.vid] = v;
+            slot[g.vid] = (int32_t)out.size();
+            out.push_back(g);
         } else {
-            e[w++] = e[r];
+            GcEnt& o = out[slot[g.vid]];
+            for (int q = 0; q < 3; ++q) o.c[q] += g.c[q];
         }
     }
-    e.resize(w);
+    std::sort(out.begin(), out.end(), [](const GcEnt& a, const GcEnt& b) { return a.vid < b.vid; });
 }
 
 int64_t deg(const Dual& d, int64_t v) { return d.nbr_ptr[v + 1] - d.nbr_ptr[v]; }
@@ -125,12 +131,13 @@ void build_grad_coeff(const Dual& d, NsLayout& L) {
     std::vector<std::vector<GcEnt>> per(n);
 #pragma omp parallel
     {
-        std::vector<GcEnt> e;
+        std::vector<GcEnt> e, m;
+        std::vector<int32_t> stamp(n, -1), slot(n, 0);
 #pragma omp for schedule(dynamic, 256)
         for (int64_t v = 0; v < n; ++v) {
             gc_push_order(d, v, e);
-            gc_merge(e);
-            per[v] = e;
+            gc_merge(e, (int32_t)v, stamp, slot, m);
+            per[v] = m;
         }
     }
     L.gcp.assign(n + 1, 0);
@@ -180,16 +187,26 @@ std::string build_ns_layout(const Dual& d, int64_t pref_vid, NsLayout& L) {
         cnt[P + v] = v == pref_vid ? 1 : off;
     }
     for (int64_t r = 0; r < R; ++r) L.trip_ptr[r + 1] = L.trip_ptr[r] + cnt[r];
+    // Distinct columns of a row are found with a per-thread stamp array over all R columns
+    // (stamp[c] == r: column c already seen in row r); only those are sorted, and a per-thread
+    // position table gives every triplet its slot. A row is handled by one thread, so the stamps
+    // need no reset between rows.
     // pass 1: distinct columns per row
     std::vector<int64_t> nz(R, 0);
 #pragma omp parallel
     {
-        std::vector<int32_t> cols;
+        std::vector<int32_t> seq;
+        std::vector<int32_t> stamp(R, -1);
 #pragma omp for schedule(dynamic, 512)
         for (int64_t r = 0; r < R; ++r) {
-            row_columns(d, L, r, cols);
-            std::sort(cols.begin(), cols.end());
-            nz[r] = std::unique(cols.begin(), cols.end()) - cols.begin();
+            row_columns(d, L, r, seq);
+            int64_t k = 0;
+            for (int32_t c : seq)
+                if (stamp[c] != (int32_t)r) {
+                    stamp[c] = (int32_t)r;
+                    ++k;
+                }
+            nz[r] = k;
         }
     }
     L.rp.assign(R + 1, 0);
@@ -199,15 +216,16 @@ std::string build_ns_layout(const Dual& d, int64_t pref_vid, NsLayout& L) {
         if (tot >= (int64_t)INT_MAX) return "NS pattern too large for 32-bit slot indices";
         L.rp[r + 1] = (int32_t)tot;
     }
-    L.ci.resize(tot);
-    L.slot_ptr.assign(tot + 1, 0);
+    L.ci.resize(tot);  // ci, slot_ptr and slot_loc are written in full by pass 2
+    L.slot_ptr.resize(tot + 1);
     L.slot_loc.resize(L.ntrip());
     L.slot_ptr[tot] = L.ntrip();
     // pass 2: columns, slots and the push-order triplet lists of every slot
     std::string err;
 #pragma omp parallel
     {
-        std::vector<int32_t> seq, cols, slot, fill;
+        std::vector<int32_t> seq, cols, fill;
+        std::vector<int32_t> stamp(R, -1), pos(R, 0);
 #pragma omp for schedule(dynamic, 512)
         for (int64_t r = 0; r < R; ++r) {
             row_columns(d, L, r, seq);
@@ -216,21 +234,22 @@ std::string build_ns_layout(const Dual& d, int64_t pref_vid, NsLayout& L) {
                 err = "internal: triplet count mismatch";
                 continue;
             }
-            cols = seq;
+            cols.clear();
+            for (int32_t c : seq)
+                if (stamp[c] != (int32_t)r) {
+                    stamp[c] = (int32_t)r;
+                    cols.push_back(c);
+                }
             std::sort(cols.begin(), cols.end());
-            cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
             const int64_t base = L.rp[r];
             std::copy(cols.begin(), cols.end(), L.ci.begin() + base);
-            slot.resize(seq.size());
+            for (size_t s = 0; s < cols.size(); ++s) pos[cols[s]] = (int32_t)s;
             fill.assign(cols.size() + 1, 0);
-            for (size_t t = 0; t < seq.size(); ++t) {
-                slot[t] = (int32_t)(std::lower_bound(cols.begin(), cols.end(), seq[t]) - cols.begin());
-                fill[slot[t] + 1]++;
-            }
+            for (int32_t c : seq) fill[pos[c] + 1]++;
             for (size_t s = 0; s < cols.size(); ++s) fill[s + 1] += fill[s];
             const int64_t tb = L.trip_ptr[r];
             for (size_t s = 0; s < cols.size(); ++s) L.slot_ptr[base + s] = tb + fill[s];
-            for (size_t t = 0; t < seq.size(); ++t) L.slot_loc[tb + fill[slot[t]]++] = (int32_t)t;
+            for (size_t t = 0; t < seq.size(); ++t) L.slot_loc[tb + fill[pos[seq[t]]]++] = (int32_t)t;
         }
     }
     return err;

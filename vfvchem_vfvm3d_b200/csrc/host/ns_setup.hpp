@@ -16,12 +16,34 @@
 //   p row of the reference vertex: the single diagonal (OpSclDomPressureReference drops the rest)
 #pragma once
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "mesh.hpp"
 
 namespace vfv {
+
+// Allocator whose value-less construct default-initialises, so resize() of the large layout
+// arrays leaves their (trivial) elements unset instead of zeroing gigabytes that the setup then
+// overwrites; the parallel pass that writes them touches the pages first.
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind { using other = UninitAlloc<U>; };
+    UninitAlloc() = default;
+    template <typename U>
+    UninitAlloc(const UninitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) { ::new (static_cast<void*>(p)) U; }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
+};
+template <typename T>
+using uninit_vector = std::vector<T, UninitAlloc<T>>;
 
 struct NsLayout {
     int64_t n = 0, n_pts = 0, pref_vid = 0;
@@ -35,9 +57,10 @@ struct NsLayout {
     std::vector<int32_t> pst_off;    // [n_dir] offset of face i's stabiliser block within that row
     std::vector<int32_t> sub_off;    // [n] offset of the boundary sub-face block within the p row (nodes)
     // pattern and slot lists
-    std::vector<int32_t> rp, ci;     // CSR of the 4n x 4n matrix
-    std::vector<int64_t> slot_ptr;   // [nnz + 1] into slot_loc
-    std::vector<int32_t> slot_loc;   // [ntrip] triplet index within its row, push order per slot
+    std::vector<int32_t> rp;         // CSR of the 4n x 4n matrix: row pointer [4n + 1]
+    uninit_vector<int32_t> ci;       // [nnz] columns
+    uninit_vector<int64_t> slot_ptr; // [nnz + 1] into slot_loc
+    uninit_vector<int32_t> slot_loc; // [ntrip] triplet index within its row, push order per slot
     int64_t nnz() const { return (int64_t)ci.size(); }
     int64_t ntrip() const { return trip_ptr.empty() ? 0 : trip_ptr.back(); }
 };
