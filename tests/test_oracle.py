@@ -90,6 +90,31 @@ def test_control_volumes_closed(lib_built):
     assert np.allclose(d["bnd_norm"][0][sel], out[sel])
 
 
+def test_unjittered_grid_degenerate_delaunay(lib_built):
+    """A regular grid (jitter 0): the eight corners of every cell are cospherical, so every cell is
+    split by the tie rule and every in-sphere decision there is an exact zero. The result must
+    still be a positively oriented tetrahedralisation of the cube whose dual equals the numpy
+    restatement on the same tetrahedra and whose control volumes close."""
+    from vfvchem_vfvm3d_b200 import Mesh
+    m = Mesh.jitter_cube(6, 1, 0.0)
+    pos, _, tets = m.export()
+    p = [pos[tets[:, i]] for i in range(4)]
+    det = np.einsum("ij,ij->i", p[0] - p[3], np.cross(p[1] - p[3], p[2] - p[3]))
+    assert np.all(det > 0)
+    assert abs(det.sum() / 6.0 - 1.0) < 1e-12
+    d = m.dual()
+    od = geom_tet.build_dual(pos, tets, m.n_pts)
+    for k in ["nbr_ptr", "nbr_idx", "bnd_ptr", "bnd_j", "bnd_k"]:
+        assert np.array_equal(d[k], od[k]), k
+    for k in ["dist", "area", "norm", "skew", "cvol", "bnd_area", "bnd_norm"]:
+        scale = max(np.max(np.abs(od[k])), 1e-300)
+        assert np.max(np.abs(d[k] - od[k])) <= 1e-12 * scale, k
+    assert abs(d["cvol"].sum() - 1.0) < 1e-12
+    # every interior control volume is the cell cube h^3, up to the 2^-18 rounding of the vertices
+    h = 1.0 / 5.0
+    assert np.allclose(d["cvol"][:m.n_pts], h ** 3, rtol=1e-4)
+
+
 def test_lsq_gradient_exact_for_linear(lib_built):
     m = _mesh(9)
     pos, _, _ = m.export()
