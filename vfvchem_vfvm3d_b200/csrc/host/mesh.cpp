@@ -310,20 +310,28 @@ std::string delaunay(Mesh& mesh) {
         cav.clear();
         cav.push_back(t);
         incav[t] = 1;
+        bool tie = false;  // p on the circumsphere of a tetrahedron next to the cavity
         for (size_t i = 0; i < cav.size(); ++i) {
             const int32_t c = cav[i];
             for (int k = 0; k < 4; ++k) {
                 const int32_t o = ta[c][k];
                 if (o < 0 || incav[o]) continue;
                 tet_pts(o, q);
-                if (insphere_sgn(q[0], q[1], q[2], q[3], p) > 0) {
+                const int sg = insphere_sgn(q[0], q[1], q[2], q[3], p);
+                if (sg > 0) {
                     incav[o] = 1;
                     cav.push_back(o);
+                } else if (sg == 0) {
+                    tie = true;
                 }
             }
         }
-        // grow until every boundary face sees p with positive orientation (cospherical ties)
-        for (bool star = false; !star;) {
+        // grow until every boundary face sees p with positive orientation (cospherical ties).
+        // Without a tie the cavity is already star-shaped: a boundary face joins c (p strictly
+        // inside its circumsphere) and o (p strictly outside); the two spheres meet in the face's
+        // circle and, the triangulation being Delaunay, o's ball holds c's on o's side of the
+        // face's plane, so p lies strictly on c's side and the loop would add nothing.
+        for (bool star = !tie; !star;) {
             star = true;
             for (size_t i = 0; i < cav.size(); ++i) {
                 const int32_t c = cav[i];
