@@ -509,23 +509,29 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
     d = Dual();
     d.n_tot = N;
     d.n_pts = mesh.n_pts;
-    auto gather = [&](int64_t v, std::vector<int32_t>& buf) {
+    // distinct vertices of v's tetrahedra: stamp[u] == v marks u as taken (one stamp array per
+    // thread and pass; a vertex is handled by one thread), then the few distinct ones are sorted
+    auto gather = [&](int64_t v, std::vector<int32_t>& buf, std::vector<int32_t>& stamp) {
         buf.clear();
         for (int64_t q = vt_ptr[v]; q < vt_ptr[v + 1]; ++q) {
             const int32_t* tv = &tet[4 * (int64_t)vt_idx[q]];
-            for (int k = 0; k < 4; ++k)
-                if (tv[k] != v) buf.push_back(tv[k]);
+            for (int k = 0; k < 4; ++k) {
+                const int32_t u = tv[k];
+                if (u != v && stamp[u] != (int32_t)v) {
+                    stamp[u] = (int32_t)v;
+                    buf.push_back(u);
+                }
+            }
         }
         std::sort(buf.begin(), buf.end());
-        buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
     };
     d.nbr_ptr.assign(N + 1, 0);
 #pragma omp parallel
     {
-        std::vector<int32_t> buf;
+        std::vector<int32_t> buf, stamp(N, -1);
 #pragma omp for schedule(dynamic, 1024)
         for (int64_t v = 0; v < N; ++v) {
-            gather(v, buf);
+            gather(v, buf, stamp);
             d.nbr_ptr[v + 1] = (int64_t)buf.size();
         }
     }
@@ -535,10 +541,10 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
     d.nbr_idx.assign(D, 0);
 #pragma omp parallel
     {
-        std::vector<int32_t> buf;
+        std::vector<int32_t> buf, stamp(N, -1);
 #pragma omp for schedule(dynamic, 1024)
         for (int64_t v = 0; v < N; ++v) {
-            gather(v, buf);
+            gather(v, buf, stamp);
             std::copy(buf.begin(), buf.end(), d.nbr_idx.begin() + d.nbr_ptr[v]);
         }
     }
@@ -568,59 +574,95 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
     }
 
     // ---- per edge (a, b), a < b: area and skew summed over its tetrahedra in ascending order,
-    //      then the data of both directed entries
+    //      then the data of both directed entries. The tetrahedra of every edge (a, b > a) come
+    //      from one scan of a's tetrahedra (ascending, so each edge's list is ascending too).
+    //      Boundary faces (geom_tet.rs:101-116: faces of exactly one tetrahedron) are found here
+    //      as well: a face whose two smallest vertices are a < b and whose third is z > b is a
+    //      boundary face when one tetrahedron of edge (a, b) holds z; each face is visited once.
     d.nbr_rev.assign(D, 0);
     d.dist.assign(D, 0.0);
     d.area.assign(D, 0.0);
     d.norm.assign(3 * D, 0.0);
     d.skew.assign(3 * D, 0.0);
-#pragma omp parallel for schedule(dynamic, 1024)
-    for (int64_t a = 0; a < N; ++a) {
-        for (int64_t ia = d.nbr_ptr[a]; ia < d.nbr_ptr[a + 1]; ++ia) {
-            const int32_t b = d.nbr_idx[ia];
-            if (b < a) continue;
-            double s_area = 0.0, s_x = 0.0, s_y = 0.0, s_z = 0.0;
-            int64_t qa = vt_ptr[a], qb = vt_ptr[b];
-            while (qa < vt_ptr[a + 1] && qb < vt_ptr[b + 1]) {  // tetrahedra holding both ends
-                if (vt_idx[qa] < vt_idx[qb]) { ++qa; continue; }
-                if (vt_idx[qb] < vt_idx[qa]) { ++qb; continue; }
-                const int64_t t = vt_idx[qa];
-                ++qa;
-                ++qb;
-                const int32_t* tv = &tet[4 * t];
-                int e = 0;
-                while (!((tv[kEdgeEnds[e][0]] == a && tv[kEdgeEnds[e][1]] == b) || (tv[kEdgeEnds[e][0]] == b && tv[kEdgeEnds[e][1]] == a))) ++e;
-                const V3 m = scale3(0.5, add3(P(tv[kEdgeEnds[e][0]]), P(tv[kEdgeEnds[e][1]])));
-                for (int side = 0; side < 2; ++side) {
-                    const int64_t q = 12 * t + 2 * e + side;
-                    const double area = pc_area[q];
-                    const V3 cent{pc_cent[3 * q], pc_cent[3 * q + 1], pc_cent[3 * q + 2]};
-                    s_area += area;
-                    const V3 sk = scale3(area, sub3(cent, m));
-                    s_x += sk.x;
-                    s_y += sk.y;
-                    s_z += sk.z;
-                }
+    std::vector<uint8_t> bface(4 * T, 0);  // [4 t + k]: face opposite local vertex k is a boundary face
+#pragma omp parallel
+    {
+        std::vector<int32_t> slot(N, 0), cnt, fill, lst;
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t a = 0; a < N; ++a) {
+            const int64_t u0 = std::upper_bound(d.nbr_idx.begin() + d.nbr_ptr[a], d.nbr_idx.begin() + d.nbr_ptr[a + 1], (int32_t)a) - d.nbr_idx.begin();
+            const int64_t up = d.nbr_ptr[a + 1] - u0;  // neighbours above a
+            if (up == 0) continue;
+            for (int64_t k = 0; k < up; ++k) slot[d.nbr_idx[u0 + k]] = (int32_t)k;
+            cnt.assign(up + 1, 0);
+            for (int64_t q = vt_ptr[a]; q < vt_ptr[a + 1]; ++q) {
+                const int32_t* tv = &tet[4 * (int64_t)vt_idx[q]];
+                for (int l = 0; l < 4; ++l)
+                    if (tv[l] > a) cnt[slot[tv[l]] + 1]++;
             }
-            const V3 pa = P(a), pb = P(b);
-            const double dist = len3(sub3(pb, pa));
-            const V3 nrm = scale3(1.0 / dist, sub3(pb, pa));
-            const V3 skew = (std::fabs(s_area) > 1e-12 * dist * dist) ? scale3(1.0 / s_area, V3{s_x, s_y, s_z}) : V3{0.0, 0.0, 0.0};
-            const int64_t ib = nbr_pos(b, (int32_t)a);
-            d.nbr_rev[ia] = ib;
-            d.nbr_rev[ib] = ia;
-            d.dist[ia] = d.dist[ib] = dist;
-            d.area[ia] = d.area[ib] = s_area;
-            const V3 mn = scale3(-1.0, nrm);
-            d.norm[ia] = nrm.x;
-            d.norm[D + ia] = nrm.y;
-            d.norm[2 * D + ia] = nrm.z;
-            d.norm[ib] = mn.x;
-            d.norm[D + ib] = mn.y;
-            d.norm[2 * D + ib] = mn.z;
-            d.skew[ia] = d.skew[ib] = skew.x;
-            d.skew[D + ia] = d.skew[D + ib] = skew.y;
-            d.skew[2 * D + ia] = d.skew[2 * D + ib] = skew.z;
+            for (int64_t k = 0; k < up; ++k) cnt[k + 1] += cnt[k];
+            fill.assign(cnt.begin(), cnt.end() - 1);
+            lst.resize(cnt[up]);
+            for (int64_t q = vt_ptr[a]; q < vt_ptr[a + 1]; ++q) {
+                const int32_t* tv = &tet[4 * (int64_t)vt_idx[q]];
+                for (int l = 0; l < 4; ++l)
+                    if (tv[l] > a) lst[fill[slot[tv[l]]]++] = vt_idx[q];
+            }
+            for (int64_t k = 0; k < up; ++k) {
+                const int64_t ia = u0 + k;
+                const int32_t b = d.nbr_idx[ia];
+                double s_area = 0.0, s_x = 0.0, s_y = 0.0, s_z = 0.0;
+                for (int32_t j = cnt[k]; j < cnt[k + 1]; ++j) {
+                    const int64_t t = lst[j];
+                    const int32_t* tv = &tet[4 * t];
+                    int e = 0;
+                    while (!((tv[kEdgeEnds[e][0]] == a && tv[kEdgeEnds[e][1]] == b) || (tv[kEdgeEnds[e][0]] == b && tv[kEdgeEnds[e][1]] == a))) ++e;
+                    const V3 m = scale3(0.5, add3(P(tv[kEdgeEnds[e][0]]), P(tv[kEdgeEnds[e][1]])));
+                    for (int side = 0; side < 2; ++side) {
+                        const int64_t q = 12 * t + 2 * e + side;
+                        const double area = pc_area[q];
+                        const V3 cent{pc_cent[3 * q], pc_cent[3 * q + 1], pc_cent[3 * q + 2]};
+                        s_area += area;
+                        const V3 sk = scale3(area, sub3(cent, m));
+                        s_x += sk.x;
+                        s_y += sk.y;
+                        s_z += sk.z;
+                    }
+                    for (int l = 0; l < 4; ++l) {  // faces (a, b, z) with z > b
+                        const int32_t z = tv[l];
+                        if (z <= b) continue;
+                        int holders = 0;
+                        for (int32_t j2 = cnt[k]; j2 < cnt[k + 1] && holders < 2; ++j2) {
+                            const int32_t* w = &tet[4 * (int64_t)lst[j2]];
+                            holders += (w[0] == z) | (w[1] == z) | (w[2] == z) | (w[3] == z);
+                        }
+                        if (holders == 1) {
+                            int opp = 0;  // the local vertex not on the face
+                            while (tv[opp] == a || tv[opp] == b || tv[opp] == z) ++opp;
+                            bface[4 * t + opp] = 1;
+                        }
+                    }
+                }
+                const V3 pa = P(a), pb = P(b);
+                const double dist = len3(sub3(pb, pa));
+                const V3 nrm = scale3(1.0 / dist, sub3(pb, pa));
+                const V3 skew = (std::fabs(s_area) > 1e-12 * dist * dist) ? scale3(1.0 / s_area, V3{s_x, s_y, s_z}) : V3{0.0, 0.0, 0.0};
+                const int64_t ib = nbr_pos(b, (int32_t)a);
+                d.nbr_rev[ia] = ib;
+                d.nbr_rev[ib] = ia;
+                d.dist[ia] = d.dist[ib] = dist;
+                d.area[ia] = d.area[ib] = s_area;
+                const V3 mn = scale3(-1.0, nrm);
+                d.norm[ia] = nrm.x;
+                d.norm[D + ia] = nrm.y;
+                d.norm[2 * D + ia] = nrm.z;
+                d.norm[ib] = mn.x;
+                d.norm[D + ib] = mn.y;
+                d.norm[2 * D + ib] = mn.z;
+                d.skew[ia] = d.skew[ib] = skew.x;
+                d.skew[D + ia] = d.skew[D + ib] = skew.y;
+                d.skew[2 * D + ia] = d.skew[2 * D + ib] = skew.z;
+            }
         }
     }
 
@@ -661,38 +703,12 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
     pc_area.reset();
     pc_cent.reset();
 
-    // ---- boundary faces: faces of exactly one tetrahedron (geom_tet.rs:101-116), in
-    //      (tetrahedron, face) order; a face is shared when another tetrahedron at its first
-    //      vertex holds the other two
-    std::vector<uint8_t> bmask(T, 0);
-#pragma omp parallel for schedule(static)
-    for (int64_t t = 0; t < T; ++t) {
-        const int32_t* tv = &tet[4 * t];
-        uint8_t mask = 0;
-        for (int k = 0; k < 4; ++k) {
-            const int32_t x = tv[(k + 1) % 4], y = tv[(k + 2) % 4], z = tv[(k + 3) % 4];
-            bool shared = false;
-            for (int64_t q = vt_ptr[x]; q < vt_ptr[x + 1] && !shared; ++q) {
-                const int64_t t2 = vt_idx[q];
-                if (t2 == t) continue;
-                const int32_t* w = &tet[4 * t2];
-                bool hy = false, hz = false;
-                for (int l = 0; l < 4; ++l) {
-                    hy = hy || w[l] == y;
-                    hz = hz || w[l] == z;
-                }
-                shared = hy && hz;
-            }
-            if (!shared) mask |= (uint8_t)(1u << k);
-        }
-        bmask[t] = mask;
-    }
+    // ---- boundary faces in (tetrahedron, face) order
     static const int FO[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};  // counterclockwise from outside
     std::vector<int32_t> surf;
     for (int64_t t = 0; t < T; ++t)
-        if (bmask[t])
-            for (int k = 0; k < 4; ++k)
-                if (bmask[t] & (1u << k)) surf.insert(surf.end(), {tet[4 * t + FO[k][0]], tet[4 * t + FO[k][1]], tet[4 * t + FO[k][2]]});
+        for (int k = 0; k < 4; ++k)
+            if (bface[4 * t + k]) surf.insert(surf.end(), {tet[4 * t + FO[k][0]], tet[4 * t + FO[k][1]], tet[4 * t + FO[k][2]]});
     for (int32_t v : surf)
         if (v < mesh.n_pts) return "dual: a boundary face joins an interior point";
     // ---- boundary sub-faces (geom_tet.rs:208-259)
