@@ -103,13 +103,17 @@ print(h.hexdigest())
 
 def test_dual_does_not_depend_on_thread_count(lib_built):
     """The Voronoi dual is built by parallel passes whose sums run in a fixed order (tetrahedron,
-    edge, side), so one thread and several give the same bits."""
+    edge, side), so one thread and several give the same bits; so do stored and recomputed face
+    pieces (VFV_DUAL_PIECE_STORE_MB=0 forces the recomputation large meshes use)."""
     import subprocess
     import sys
     digests = []
-    for threads in ("1", "3"):
+    for threads, store_mb in (("1", None), ("3", None), ("3", "0")):
         env = dict(os.environ, OMP_NUM_THREADS=threads)
+        env.pop("VFV_DUAL_PIECE_STORE_MB", None)
+        if store_mb is not None:
+            env["VFV_DUAL_PIECE_STORE_MB"] = store_mb
         out = subprocess.run([sys.executable, "-c", _DUAL_DIGEST], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
         assert out.returncode == 0, out.stderr
         digests.append(out.stdout.strip().splitlines()[-1])
-    assert digests[0] == digests[1]
+    assert digests[0] == digests[1] == digests[2]

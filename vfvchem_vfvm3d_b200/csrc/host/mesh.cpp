@@ -485,7 +485,7 @@ inline void face_pieces(const Mesh& mesh, const int32_t* tv, V3 c_t, int e, doub
 // Every step is a data-parallel pass over tetrahedra, vertices or edges. Each sum runs in the
 // order of the serial tetrahedron loop of the reference (tetrahedron, then local edge, then side),
 // so the result does not depend on the thread count.
-std::string build_dual(const Mesh& mesh, Dual& d) {
+std::string build_dual(const Mesh& mesh, Dual& d, double piece_store_bytes) {
     const int64_t N = mesh.n_tot(), T = mesh.n_tet();
     const int32_t* tet = mesh.tets.data();
     auto P = [&](int64_t v) { return V3{mesh.pos[3 * v], mesh.pos[3 * v + 1], mesh.pos[3 * v + 2]}; };
@@ -552,13 +552,28 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
         return (int64_t)(std::lower_bound(d.nbr_idx.begin() + d.nbr_ptr[v], d.nbr_idx.begin() + d.nbr_ptr[v + 1], n) - d.nbr_idx.begin());
     };
 
-    // ---- Voronoi face pieces of every tetrahedron edge (geom_tet.rs:122-171)
+    // ---- Voronoi face pieces of every tetrahedron edge (geom_tet.rs:122-171): stored (384 bytes
+    //      per tetrahedron) while that fits the budget, else recomputed where needed from the
+    //      stored circumcentres (24 bytes per tetrahedron; the same function, so the same bits)
+    const bool store = (double)T * 48.0 * sizeof(double) <= piece_store_bytes;
     // every entry is written below; left uninitialised so that the parallel loop first-touches it
-    std::unique_ptr<double[]> pc_area(new double[12 * T]), pc_cent(new double[36 * T]);
+    std::unique_ptr<double[]> pc_area, pc_cent, ctc;
+    if (store) {
+        pc_area.reset(new double[12 * T]);
+        pc_cent.reset(new double[36 * T]);
+    } else {
+        ctc.reset(new double[3 * T]);
+    }
 #pragma omp parallel for schedule(static)
     for (int64_t t = 0; t < T; ++t) {
         const int32_t* tv = &tet[4 * t];
         const V3 c_t = circumsphere3(P(tv[0]), P(tv[1]), P(tv[2]), P(tv[3]));
+        if (!store) {
+            ctc[3 * t] = c_t.x;
+            ctc[3 * t + 1] = c_t.y;
+            ctc[3 * t + 2] = c_t.z;
+            continue;
+        }
         for (int e = 0; e < 6; ++e) {
             double a[2];
             V3 c[2];
@@ -572,6 +587,17 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
             }
         }
     }
+    auto pieces = [&](int64_t t, int e, double a[2], V3 c[2]) {
+        if (store) {
+            for (int side = 0; side < 2; ++side) {
+                const int64_t q = 12 * t + 2 * e + side;
+                a[side] = pc_area[q];
+                c[side] = V3{pc_cent[3 * q], pc_cent[3 * q + 1], pc_cent[3 * q + 2]};
+            }
+        } else {
+            face_pieces(mesh, &tet[4 * t], V3{ctc[3 * t], ctc[3 * t + 1], ctc[3 * t + 2]}, e, a, c);
+        }
+    };
 
     // ---- per edge (a, b), a < b: area and skew summed over its tetrahedra in ascending order,
     //      then the data of both directed entries. The tetrahedra of every edge (a, b > a) come
@@ -618,10 +644,12 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
                     int e = 0;
                     while (!((tv[kEdgeEnds[e][0]] == a && tv[kEdgeEnds[e][1]] == b) || (tv[kEdgeEnds[e][0]] == b && tv[kEdgeEnds[e][1]] == a))) ++e;
                     const V3 m = scale3(0.5, add3(P(tv[kEdgeEnds[e][0]]), P(tv[kEdgeEnds[e][1]])));
+                    double pa[2];
+                    V3 pcen[2];
+                    pieces(t, e, pa, pcen);
                     for (int side = 0; side < 2; ++side) {
-                        const int64_t q = 12 * t + 2 * e + side;
-                        const double area = pc_area[q];
-                        const V3 cent{pc_cent[3 * q], pc_cent[3 * q + 1], pc_cent[3 * q + 2]};
+                        const double area = pa[side];
+                        const V3 cent = pcen[side];
                         s_area += area;
                         const V3 sk = scale3(area, sub3(cent, m));
                         s_x += sk.x;
@@ -685,10 +713,12 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
                 const V3 pi = P(vi), pj = P(vj);
                 const double dist = len3(sub3(pj, pi));
                 const V3 pv = vi == v ? pi : pj;
+                double pa[2];
+                V3 pcen[2];
+                pieces(t, e, pa, pcen);
                 for (int side = 0; side < 2; ++side) {
-                    const int64_t pq = 12 * t + 2 * e + side;
-                    const double pvol = pc_area[pq] * dist / 6.0;
-                    const V3 c = scale3(pvol * 0.75, sub3(V3{pc_cent[3 * pq], pc_cent[3 * pq + 1], pc_cent[3 * pq + 2]}, pv));
+                    const double pvol = pa[side] * dist / 6.0;
+                    const V3 c = scale3(pvol * 0.75, sub3(pcen[side], pv));
                     cx += c.x;
                     cy += c.y;
                     cz += c.z;
@@ -702,6 +732,7 @@ std::string build_dual(const Mesh& mesh, Dual& d) {
     }
     pc_area.reset();
     pc_cent.reset();
+    ctc.reset();
 
     // ---- boundary faces in (tetrahedron, face) order
     static const int FO[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};  // counterclockwise from outside

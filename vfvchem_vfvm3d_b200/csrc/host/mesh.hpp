@@ -67,8 +67,11 @@ Mesh make_jitter_cube(int n, uint64_t seed, double jitter);
 // Fills mesh.tets. Returns an empty string on success, else the error message.
 std::string delaunay(Mesh& mesh);
 
-// Voronoi dual of the tetrahedralisation (geom_tet.rs:122-293). Returns "" on success.
-std::string build_dual(const Mesh& mesh, Dual& dual);
+// Voronoi dual of the tetrahedralisation (geom_tet.rs:122-293). Returns "" on success. The face
+// pieces of all tetrahedra (384 bytes each) are kept while they fit piece_store_bytes, else
+// recomputed where needed; the result is the same bit for bit either way and for any thread count.
+constexpr double kDualPieceStoreBytes = 8.0 * 1024 * 1024 * 1024;
+std::string build_dual(const Mesh& mesh, Dual& dual, double piece_store_bytes = kDualPieceStoreBytes);
 
 // exact orientation / in-sphere signs on the quantised grid (exported for tests)
 int orient_sign(const double* a, const double* b, const double* c, const double* d);

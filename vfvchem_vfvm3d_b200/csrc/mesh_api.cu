@@ -2,13 +2,21 @@
 // the Delaunay tetrahedra and the Voronoi dual (host code: csrc/host/mesh.cpp).
 #include "internal.cuh"
 
+#include <cstdlib>
 #include <cstring>
 #include <omp.h>
+
+// Budget for the dual's stored face pieces; VFV_DUAL_PIECE_STORE_MB overrides it (0: always
+// recompute them), so that tests can check both ways give the same dual.
+static double dual_piece_store_bytes() {
+    if (const char* e = std::getenv("VFV_DUAL_PIECE_STORE_MB")) return std::atof(e) * 1024.0 * 1024.0;
+    return kDualPieceStoreBytes;
+}
 
 // Delaunay tetrahedralisation and Voronoi dual of a mesh whose vertices are set; takes ownership.
 static int mesh_finish(vfv_mesh* mh, vfv_mesh** out) {
     std::string e = delaunay(mh->m);
-    if (e.empty()) e = build_dual(mh->m, mh->d);
+    if (e.empty()) e = build_dual(mh->m, mh->d, dual_piece_store_bytes());
     if (!e.empty()) {
         delete mh;
         return set_err(nullptr, VFV_BAD_INPUT, e);
@@ -61,7 +69,7 @@ int vfv_mesh_jitter_cubes(int count, const int32_t* n, const uint64_t* seeds, do
         auto* mh = new vfv_mesh();
         mh->m = make_jitter_cube(n[i], seeds[i], jitter);
         std::string e = delaunay(mh->m);
-        if (e.empty()) e = build_dual(mh->m, mh->d);
+        if (e.empty()) e = build_dual(mh->m, mh->d, dual_piece_store_bytes());
         if (!e.empty()) {
             errs[i] = e;
             delete mh;
