@@ -14,6 +14,7 @@
 #include "kernels/krylov.cuh"
 #include "kernels/ns.cuh"
 #include "host/ns_setup.hpp"
+#include "host/sort.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -33,29 +34,6 @@ std::string& vfv_thread_error() {
     static thread_local std::string e;
     return e;
 }
-
-namespace {
-
-// LSD radix sort of (key, index) by key, stable; keys < 2^bits.
-void radix_sort_pairs(std::vector<uint64_t>& key, std::vector<int64_t>& idx, int bits) {
-    const size_t n = key.size();
-    std::vector<uint64_t> k2(n);
-    std::vector<int64_t> i2(n);
-    for (int shift = 0; shift < bits; shift += 16) {
-        std::vector<size_t> cnt(65537, 0);
-        for (size_t i = 0; i < n; ++i) cnt[((key[i] >> shift) & 0xffff) + 1]++;
-        for (int d = 0; d < 65536; ++d) cnt[d + 1] += cnt[d];
-        for (size_t i = 0; i < n; ++i) {
-            const size_t p = cnt[(key[i] >> shift) & 0xffff]++;
-            k2[p] = key[i];
-            i2[p] = idx[i];
-        }
-        key.swap(k2);
-        idx.swap(i2);
-    }
-}
-
-}  // namespace
 
 // ================================================================ GMRES driver
 namespace {
@@ -1187,12 +1165,17 @@ int vfv_pattern_from_triplets(vfv_ctx* ctx, int64_t n, int64_t ntrip, const uint
         return set_err(ctx, VFV_BAD_INPUT, "invalid matrix size or triplet arrays");
     std::vector<uint64_t> key(ntrip);
     std::vector<int64_t> idx(ntrip);
+    int64_t bad = ntrip;  // first out-of-range triplet
+#pragma omp parallel for schedule(static) reduction(min : bad)
     for (int64_t t = 0; t < ntrip; ++t) {
-        if (rows[t] >= (uint64_t)n || cols[t] >= (uint64_t)n)
-            return set_err(ctx, VFV_BAD_INPUT, "triplet index out of range at " + std::to_string(t));
+        if (rows[t] >= (uint64_t)n || cols[t] >= (uint64_t)n) {
+            bad = std::min(bad, t);
+            continue;
+        }
         key[t] = rows[t] * (uint64_t)n + cols[t];
         idx[t] = t;
     }
+    if (bad < ntrip) return set_err(ctx, VFV_BAD_INPUT, "triplet index out of range at " + std::to_string(bad));
     int bits = 1;
     while (bits < 64 && ((uint64_t)n * (uint64_t)n - 1) >> bits) ++bits;
     radix_sort_pairs(key, idx, bits);
