@@ -86,6 +86,20 @@ def test_triplet_pattern_and_values(gpu_ctx, c1h_system, c1_hetero):
     assert np.array_equal(gva, va)  # same push-order summation
 
 
+def test_triplet_index_out_of_range_is_reported(gpu_ctx, c1h_system, c1_hetero):
+    """A row or column >= n is rejected before any device work, naming the first bad triplet
+    (the keys are built in parallel, the reported index is still the smallest)."""
+    from vfvchem_vfvm3d_b200 import Pattern, VFVChemError
+    _, _, (r, c, _) = c1h_system
+    r = r.astype(np.uint64).copy()
+    c = c.astype(np.uint64).copy()
+    last = r.size - 5
+    r[last] = c1_hetero.n
+    c[r.size // 2] = c1_hetero.n + 7
+    with pytest.raises(VFVChemError, match=rf"out of range at {r.size // 2}$"):
+        Pattern.from_triplets(gpu_ctx, c1_hetero.n, r, c)
+
+
 def test_spmv_matches_oracle(gpu_ctx, c1h_system, c1_hetero):
     import torch
     from vfvchem_vfvm3d_b200 import Pattern
