@@ -36,7 +36,7 @@ extern "C" {
 #define VFV_NONFINITE 2     /* NaN/Inf in the residual or the Arnoldi process */
 #define VFV_BAD_INPUT 3     /* invalid argument (sizes, indices, options) */
 #define VFV_CUDA_ERROR 4    /* CUDA runtime failure or no device */
-#define VFV_TIMEOUT 5       /* reserved for bounded device waits */
+#define VFV_TIMEOUT 5       /* a bounded device wait gave up (see vfv_gmres_opts::wait_limit) */
 
 /* ---- preconditioners / precisions / orderings */
 #define VFV_PRECOND_NONE 0
@@ -76,6 +76,10 @@ typedef struct {
     int32_t ilu_order; /* VFV_ILU_* (ILU(0) only) */
     int32_t engine;    /* VFV_ENGINE_*: how a restart cycle is launched */
     double inner_rtol; /* VFV_MIXED: an inner cycle also ends once its estimate drops by this factor (0 = full cycles) */
+    int64_t wait_limit; /* polls before a bounded device wait gives up (0 = default 20,000,000; any wait also
+                           ends after 2 s): the persistent engine's grid barriers and the single-launch
+                           ILU(0) sweeps. A wait that gives up makes the solve return VFV_TIMEOUT and
+                           leaves the context usable. */
 } vfv_gmres_opts;
 
 typedef struct {
@@ -148,8 +152,9 @@ int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const
  * from a fixed 2 MiB device array inside the library, so n is limited to 262,144 rows (larger
  * patterns are rejected with VFV_BAD_INPUT). The pattern's ILU(0) storage must already exist:
  * call vfv_ilu0_apply_device (or an ILU(0) solve) on it once first. The first call on each device
- * looks up the array's device address (make it before any stream capture). All calls share the
- * array: calls that overlap on the GPU race. */
+ * looks up the array's device address (make it before any stream capture). Every call synchronises
+ * the context's stream before it returns. All calls in the process share the one array on a
+ * device: calls that overlap on the GPU race. */
 int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels);
 /* the symmetric permutation the ILU(0) factor lives on: perm[n] (new -> old) and the row ranges of
  * its levels lev_ptr[nlev+1] (any pointer may be NULL; call once with NULLs to learn nlev) */

@@ -21,6 +21,7 @@ from .errors import (  # noqa: F401
     LinearGmresNonFinite,
     LinearGmresBadInput,
     LinearGmresCudaError,
+    DeviceWaitTimeout,
     LinearGmresNonPositiveTolerance,
     LinearGmresNonPositiveRestart,
     LinearGmresNonPositiveMaxOuter,

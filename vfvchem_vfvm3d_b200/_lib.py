@@ -31,6 +31,7 @@ class GmresOpts(C.Structure):
         ("ilu_order", C.c_int32),
         ("engine", C.c_int32),
         ("inner_rtol", C.c_double),
+        ("wait_limit", C.c_int64),
     ]
 
 

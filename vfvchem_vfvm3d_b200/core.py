@@ -30,6 +30,7 @@ class GmresOptions:
     ilu_order: int = L.ILU_MULTICOLOR
     inner_rtol: float = 0.0
     engine: int = L.ENGINE_GRAPH
+    wait_limit: int = 0  # polls before a bounded device wait gives up (0: the library default)
 
     def to_c(self) -> L.GmresOpts:
         o = L.GmresOpts()
@@ -37,6 +38,7 @@ class GmresOptions:
         o.precond, o.precision, o.ilu_order = int(self.precond), int(self.precision), int(self.ilu_order)
         o.inner_rtol = float(self.inner_rtol)
         o.engine = int(self.engine)
+        o.wait_limit = int(self.wait_limit)
         return o
 
 

@@ -17,7 +17,9 @@
 #include "host/sort.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -380,10 +382,89 @@ cudaError_t launch_level(cudaStream_t s, const IluStruct& S, int l, bool pdl, co
 }
 
 template <typename T>
-void ilu_apply(cudaStream_t s, const IluStruct& S, const T* lu, const T* in, T* t, T* out, const DevStatus* st, int prio = 0,
-               bool use_prio = false) {
+void ilu_apply_levels(cudaStream_t s, const IluStruct& S, const T* lu, const T* in, T* t, T* out, const DevStatus* st, int prio = 0,
+                      bool use_prio = false) {
     for (int l = 0; l < S.nlev; ++l) launch_level<T, true>(s, S, l, l > 0, lu, in, t, out, st, prio, use_prio);
     for (int l = S.nlev - 1; l >= 0; --l) launch_level<T, false>(s, S, l, true, lu, in, t, out, st, prio, use_prio);
+}
+
+constexpr long long kDefaultWaitPolls = 20000000LL;  // polls before a bounded device wait gives up (2 s also ends it)
+
+template <typename T>
+constexpr int chain_slot() {
+    return std::is_same<T, double>::value ? 0 : 1;
+}
+
+// Work vectors refilled with the sentinel, claim/parity state cleared, poll limit set: the state
+// of a fresh chain (at set-up, and after a wait gave up, which leaves it undefined).
+template <typename T>
+int chain_reset(vfv_ctx* ctx, IluStruct& S, int64_t n, long long polls) {
+    IluStruct::Chain& C = S.chain[chain_slot<T>()];
+    cudaStream_t s = ctx->stream;
+    IluChainState h{};
+    h.poll_limit = polls > 0 ? polls : kDefaultWaitPolls;
+    CK(cudaMemsetAsync(C.work.p, 0xFF, C.work.n, s));
+    CK(cudaMemcpyAsync(C.state.p, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    *C.h_flag = 0;
+    return VFV_OK;
+}
+
+// Task table (row ranges of at most kChainThreads rows inside one level) and the chain state of
+// precision T; once per ILU structure and precision.
+template <typename T>
+int chain_setup(vfv_ctx* ctx, IluStruct& S, int64_t n) {
+    IluStruct::Chain& C = S.chain[chain_slot<T>()];
+    if (C.grid > 0) return VFV_OK;
+    if (!S.tasks.p) {
+        std::vector<int32_t> tk;
+        for (int l = 0; l < S.nlev; ++l)
+            for (int32_t r = S.lev_ptr[l]; r < S.lev_ptr[l + 1]; r += kChainThreads) tk.push_back(r);
+        tk.push_back(S.lev_ptr[S.nlev]);
+        S.ntask = (int)tk.size() - 1;
+        CK(S.tasks.upload(tk.data(), tk.size(), ctx->stream));
+    }
+    CK(C.work.alloc((size_t)4 * n * sizeof(T)));
+    CK(C.state.alloc(sizeof(IluChainState)));
+    CK(cudaHostAlloc((void**)&C.h_flag, sizeof(int), cudaHostAllocMapped));
+    *C.h_flag = 0;
+    CK(cudaHostGetDevicePointer((void**)&C.d_flag, C.h_flag, 0));
+    int per_sm = 0, sms = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu0_chain<T>, kChainThreads, 0));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    C.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * sms, 2 * (int64_t)S.ntask));
+    return chain_reset<T>(ctx, S, n, 0);
+}
+
+// poll limit of the chain's bounded waits for the launches that follow (enqueued on the stream)
+template <typename T>
+int chain_set_polls(vfv_ctx* ctx, IluStruct& S, long long polls) {
+    IluStruct::Chain& C = S.chain[chain_slot<T>()];
+    const long long v = polls > 0 ? polls : kDefaultWaitPolls;  // pageable source: staged before the call returns
+    CK(cudaMemcpyAsync(C.state.p + offsetof(IluChainState, poll_limit), &v, sizeof(v), cudaMemcpyHostToDevice, ctx->stream));
+    return VFV_OK;
+}
+
+// z = (LU)^-1 r in one launch (k_ilu0_chain). `timeout_flag` receives 1 if a bounded wait gave up.
+template <typename T>
+cudaError_t ilu_apply_chain(cudaStream_t s, IluStruct& S, int64_t n, const T* lu, const T* in, T* out, const DevStatus* st,
+                            int* timeout_flag, int prio = 0, bool use_prio = false) {
+    IluStruct::Chain& C = S.chain[chain_slot<T>()];
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)C.grid);
+    cfg.blockDim = dim3(kChainThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    if (use_prio) {
+        attr[0].id = cudaLaunchAttributePriority;
+        attr[0].val.priority = prio;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    using U = typename ChainWord<T>::U;
+    return cudaLaunchKernelEx(&cfg, k_ilu0_chain<T>, (int32_t)S.ntask, (const int32_t*)S.tasks.p, (const int32_t*)S.rp.p,
+                              (const int32_t*)S.ci.p, (const int32_t*)S.dg.p, lu, (const int32_t*)S.perm.p, n, in, out,
+                              reinterpret_cast<U*>(C.work.p), reinterpret_cast<IluChainState*>(C.state.p), timeout_flag, st);
 }
 
 constexpr int kStepsPerIf = 4;  // Arnoldi steps per IF node of a cycle graph
@@ -419,6 +500,8 @@ struct Gmres : SolverBase {
     cudaStream_t s2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int ilu_prio = 0;  // greatest stream priority: the sweeps' blocks go first when SM slots free up
+    bool ilu_chain = true;  // ILU(0) sweeps as one k_ilu0_chain launch (false: one launch per level)
+    long long wait_polls = kDefaultWaitPolls;  // bounded device waits of this solve (vfv_gmres_opts::wait_limit)
     ~Gmres() override {
         if (exec) cudaGraphExecDestroy(exec);
         if (ev_fork) cudaEventDestroy(ev_fork);
@@ -529,8 +612,20 @@ struct Gmres : SolverBase {
                 it = p->ilu.emplace(ilu_order, std::move(S)).first;
             }
             ilu = it->second.get();
+            if (const char* e = getenv("VFV_ILU_LEVELS")) ilu_chain = e[0] != '1';
+            if (ilu_chain) {
+                int rc = chain_setup<T>(ctx, *ilu, n);
+                if (rc) return rc;
+            }
         }
         return VFV_OK;
+    }
+
+    // z = M^-1 r for the ILU(0) preconditioner; `in` and `out` may alias. st: early exit once the
+    // solve is done (null: always run).
+    void apply_ilu(cudaStream_t s, const T* in, T* out, const DevStatus* stp, int prio = 0, bool use_prio = false) {
+        if (ilu_chain) ilu_apply_chain<T>(s, *ilu, n, lu_vals(), in, out, stp, &st.p->timeout, prio, use_prio);
+        else ilu_apply_levels<T>(s, *ilu, lu_vals(), in, z2.p, out, stp, prio, use_prio);
     }
 
     const T* krylov_vals(vfv_pattern* p) const {
@@ -585,7 +680,7 @@ struct Gmres : SolverBase {
         const T* in = uj;
         cudaEventRecord(ev[0], s);
         if (precond == VFV_PRECOND_ILU0) {
-            ilu_apply<T>(s, *ilu, lu_vals(), uj, z2.p, z.p, st.p);
+            apply_ilu(s, uj, z.p, st.p);
             in = z.p;
         }
         cudaEventRecord(ev[1], s);
@@ -648,7 +743,7 @@ struct Gmres : SolverBase {
         A.trace = trace.p;
         A.st = st.p;
         A.scal = scal.p;
-        A.spin_limit = 20000000LL;
+        A.spin_limit = wait_polls;
         return A;
     }
 
@@ -658,7 +753,7 @@ struct Gmres : SolverBase {
     // z_{j+1} = M^-1 w - sum_i c_i z_i, so the latency-bound ILU(0) sweeps of M^-1 w run on a second
     // stream while the bandwidth-bound CGS2 passes orthogonalise w; the correction of x is Z y.
     void enqueue_prologue(cudaStream_t s) {
-        if (engine == VFV_ENGINE_OVERLAP) ilu_apply<T>(s, *ilu, lu_vals(), V.p, z2.p, Zb.p, st.p);  // z_0 = M^-1 u_0
+        if (engine == VFV_ENGINE_OVERLAP) apply_ilu(s, V.p, Zb.p, st.p);  // z_0 = M^-1 u_0
     }
 
     void enqueue_step(cudaStream_t s, vfv_pattern* p, int j) {
@@ -669,7 +764,7 @@ struct Gmres : SolverBase {
             launch_spmv<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, Zb.p + (int64_t)j * ldv, abuf.p, inv_beta.p + j, st.p);
             cudaEventRecord(ev_fork, s);
             cudaStreamWaitEvent(s2, ev_fork, 0);
-            ilu_apply<T>(s2, *ilu, lu_vals(), abuf.p, z2.p, qbuf.p, st.p, ilu_prio, true);
+            apply_ilu(s2, abuf.p, qbuf.p, st.p, ilu_prio, true);
             cudaEventRecord(ev_join, s2);
             k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, abuf.p, j + 1);
             k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
@@ -683,7 +778,7 @@ struct Gmres : SolverBase {
         const T* uj = V.p + (int64_t)j * ldv;
         const T* in = uj;
         if (precond == VFV_PRECOND_ILU0) {
-            ilu_apply<T>(s, *ilu, lu_vals(), uj, z2.p, z.p, st.p);
+            apply_ilu(s, uj, z.p, st.p);
             in = z.p;
         } else if (precond == VFV_PRECOND_BJ4) {
             k_bj4_apply<T><<<grid_for(n / 4), 256, 0, s>>>(n / 4, bj_vals(), uj, z.p, st.p);
@@ -706,7 +801,7 @@ struct Gmres : SolverBase {
             k_combine<T, 0><<<vb, kBlk, 0, s>>>(K, Zb.p, x.p, nullptr, nullptr);
         } else if (precond == VFV_PRECOND_ILU0) {
             k_combine<T, 2><<<vb, kBlk, 0, s>>>(K, V.p, x.p, nullptr, z.p);
-            ilu_apply<T>(s, *ilu, lu_vals(), z.p, z2.p, z.p, nullptr);  // out may alias in: the upper sweep starts after the lower one
+            apply_ilu(s, z.p, z.p, nullptr);  // in place: row i's upper result is written after row i's input was read
             k_add_to_x<T><<<vb, 256, 0, s>>>(n, x.p, z.p);
         } else if (precond == VFV_PRECOND_BJ4) {
             k_combine<T, 2><<<vb, kBlk, 0, s>>>(K, V.p, x.p, nullptr, z.p);
@@ -828,6 +923,11 @@ struct Gmres : SolverBase {
         const bool mixed = !std::is_same<T, double>::value;
         CK(cudaMemcpyAsync(b.p, d_b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         CK(cudaMemcpyAsync(x.p, d_x0, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        wait_polls = o.wait_limit > 0 ? (long long)o.wait_limit : kDefaultWaitPolls;
+        if (ilu && ilu_chain) {
+            int rc = chain_set_polls<T>(ctx, *ilu, wait_polls);
+            if (rc) return rc;
+        }
         // matrix preparation for this solve
         if (precond == VFV_PRECOND_JACOBI) {
             k_jacobi_inv<<<grid_for(n), 256, 0, s>>>(n, p->diag_pos.p, p->val.p, dinv.p);
@@ -939,8 +1039,13 @@ struct Gmres : SolverBase {
             steps_seen = hst.total_steps;
             if (hst.timeout) {
                 rc = VFV_TIMEOUT;
-                CK(cudaMemsetAsync(bar.p, 0, 2 * kGenOffset * sizeof(unsigned), s));  // barrier state is undefined after a timeout
+                // the state of the wait that gave up is undefined: grid barrier, ILU sweep chain
+                if (bar.p) CK(cudaMemsetAsync(bar.p, 0, 2 * kGenOffset * sizeof(unsigned), s));
                 CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
+                if (ilu && ilu_chain) {
+                    int rc2 = chain_reset<T>(ctx, *ilu, n, wait_polls);
+                    if (rc2) return rc2;
+                }
                 break;
             }
             if (hst.nonfinite) {
@@ -998,7 +1103,7 @@ struct Gmres : SolverBase {
             return set_err(ctx, rc, "GMRES did not converge in " + std::to_string(o.max_outer) + " restart cycles (relres " +
                                         std::to_string(hst.beta0 / bnorm) + ")");
         if (rc == VFV_NONFINITE) return set_err(ctx, rc, "GMRES: non-finite residual");
-        if (rc == VFV_TIMEOUT) return set_err(ctx, rc, "GMRES cycle kernel: a grid barrier timed out");
+        if (rc == VFV_TIMEOUT) return set_err(ctx, rc, "GMRES: a bounded device wait gave up (grid barrier or ILU(0) sweep)");
         return VFV_OK;
     }
 };
@@ -1019,6 +1124,7 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
         return set_err(ctx, VFV_BAD_INPUT, "unknown engine");
     if (o->engine == VFV_ENGINE_OVERLAP && o->precond != VFV_PRECOND_ILU0)
         return set_err(ctx, VFV_BAD_INPUT, "the overlapped engine needs the ILU(0) preconditioner");
+    if (o->wait_limit < 0) return set_err(ctx, VFV_BAD_INPUT, "wait_limit must be >= 0 (0 = default)");
     return VFV_OK;
 }
 
@@ -1114,6 +1220,7 @@ void vfv_gmres_default_opts(vfv_gmres_opts* o) {
     o->ilu_order = VFV_ILU_MULTICOLOR;
     o->engine = VFV_ENGINE_GRAPH;
     o->inner_rtol = 0.0;
+    o->wait_limit = 0;
 }
 
 int vfv_ctx_create(int device, vfv_ctx** out) {
@@ -1325,8 +1432,13 @@ int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y) 
     return VFV_OK;
 }
 
-int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels) {
-    if (!ctx || !p || !r || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+}  // extern "C"
+
+namespace {
+// Finds or builds the ILU(0) structure of an ordering, refreshes its numeric factor and sets up the
+// single-launch sweeps of precision T.
+template <typename T>
+int ilu_for_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, IluStruct** out) {
     if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
     auto it = p->ilu.find(ilu_order);
     if (it == p->ilu.end()) {
@@ -1336,40 +1448,61 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
         it = p->ilu.emplace(ilu_order, std::move(S)).first;
     }
     IluStruct& S = *it->second;
-    int rc = ilu_refresh(ctx, p, S, false);
+    int rc = ilu_refresh(ctx, p, S, !std::is_same<T, double>::value);
     if (rc) return rc;
-    DBuf<double> t;
-    CK(t.alloc(p->n));
-    ilu_apply<double>(ctx->stream, S, S.lu64.p, r, t.p, z, nullptr);
-    ctx->launches += 2 * S.nlev;
-    CK(cudaStreamSynchronize(ctx->stream));
-    CK(cudaGetLastError());
-    if (levels) *levels = S.nlev;
+    rc = chain_setup<T>(ctx, S, p->n);
+    if (rc) return rc;
+    *out = &S;
     return VFV_OK;
 }
 
-// z = M^-1 r with the float copy of the ILU(0) factor: the level kernels the mixed-precision solver
-// runs. Enqueued on the context's stream with no synchronisation; t is the caller's work vector of
-// n floats, so calls after the first (which builds the factor) allocate nothing and can be timed
-// back to back.
+// A chain wait of an earlier standalone apply gave up: restore the chain and report it.
+template <typename T>
+int chain_check_flag(vfv_ctx* ctx, IluStruct& S, int64_t n) {
+    IluStruct::Chain& C = S.chain[chain_slot<T>()];
+    if (!*(volatile int*)C.h_flag) return VFV_OK;
+    CK(cudaStreamSynchronize(ctx->stream));
+    int rc = chain_reset<T>(ctx, S, n, 0);
+    if (rc) return rc;
+    return set_err(ctx, VFV_TIMEOUT, "ILU(0) sweeps: a bounded device wait gave up");
+}
+}  // namespace
+
+extern "C" {
+
+int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels) {
+    if (!ctx || !p || !r || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    IluStruct* S = nullptr;
+    int rc = ilu_for_apply<double>(ctx, p, ilu_order, &S);
+    if (rc) return rc;
+    rc = chain_check_flag<double>(ctx, *S, p->n);
+    if (rc) return rc;
+    CK(ilu_apply_chain<double>(ctx->stream, *S, p->n, S->lu64.p, r, z, nullptr, S->chain[0].d_flag));
+    ctx->launches += 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    rc = chain_check_flag<double>(ctx, *S, p->n);
+    if (rc) return rc;
+    if (levels) *levels = S->nlev;
+    return VFV_OK;
+}
+
+// z = M^-1 r with the float copy of the factor: the kernel the mixed-precision solver runs.
+// Enqueued on the context's stream with no synchronisation, so calls after the first (which builds
+// the factor and the sweep state) allocate nothing and can be timed back to back. A bounded wait
+// that gave up is reported by the next call on the pattern. t is unused (kept for the ABI).
 int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const float* r, float* t, float* z, int32_t* levels) {
     if (!ctx || !p || !r || !t || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (t == r || t == z) return set_err(ctx, VFV_BAD_INPUT, "the work vector aliases r or z");
-    if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
-    auto it = p->ilu.find(ilu_order);
-    if (it == p->ilu.end()) {
-        auto S = std::make_unique<IluStruct>();
-        int rc = build_ilu_struct(ctx, p, ilu_order, *S);
-        if (rc) return rc;
-        it = p->ilu.emplace(ilu_order, std::move(S)).first;
-    }
-    IluStruct& S = *it->second;
-    int rc = ilu_refresh(ctx, p, S, true);
+    IluStruct* S = nullptr;
+    int rc = ilu_for_apply<float>(ctx, p, ilu_order, &S);
     if (rc) return rc;
-    ilu_apply<float>(ctx->stream, S, S.lu32.p, r, t, z, nullptr);
-    ctx->launches += 2 * S.nlev;
+    rc = chain_check_flag<float>(ctx, *S, p->n);
+    if (rc) return rc;
+    CK(ilu_apply_chain<float>(ctx->stream, *S, p->n, S->lu32.p, r, z, nullptr, S->chain[1].d_flag));
+    ctx->launches += 1;
     CK(cudaGetLastError());
-    if (levels) *levels = S.nlev;
+    if (levels) *levels = S->nlev;
     return VFV_OK;
 }
 
@@ -1377,21 +1510,26 @@ int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const
 // For callers that may not allocate device memory once they are running: code that drives the
 // solver from inside a time-step loop under a fixed memory budget, or from a host framework whose
 // allocator owns all device memory, or that must not hit the implicit device-wide synchronisation
-// of cudaMalloc/cudaFree in the middle of a step. vfv_ilu0_apply_device allocates its work vector
-// on every call; this variant takes it from one fixed device array compiled into the library.
+// of cudaMalloc/cudaFree in the middle of a step. vfv_ilu0_apply_device allocates its sweep state
+// when it first meets a pattern; this variant never allocates: its work vector is one fixed device
+// array compiled into the library (the per-level sweeps, which need one work vector and give the
+// same bits as the single-launch sweeps).
 //
 // The array is a file-scope __device__ variable: every GPU that loads the library holds its
 // 2 MiB until the process exits. Host code cannot use the variable's name as a device address,
 // so the device address is looked up with cudaGetSymbolAddress once per device, with that device
 // current, by the first call on that device — make that first call before any stream capture.
-// Every call shares the array and it keeps the last call's contents; nothing in it has to start
-// at zero (the sweeps write every element before reading it). Calls that overlap on the GPU, from
-// any context or thread, race on the array.
+// The address is cached per device index (atomically, so threads that race on a first call all
+// store the same value); the cache assumes the primary context of each device, which the runtime
+// API uses, is never reset while the library is loaded. Every call synchronises the context's
+// stream before it returns. Every call shares the array and it keeps the last call's contents;
+// nothing in it has to start at zero (the sweeps write every element before reading it). Calls
+// that overlap on the GPU, from any context or thread, race on the array.
 namespace {
 constexpr int64_t kNoAllocMaxRows = 1 << 18;  // 262,144 rows of doubles: 2 MiB
 __device__ __align__(256) double g_ilu_scratch[kNoAllocMaxRows];
 constexpr int kNoAllocMaxDevices = 64;
-double* g_ilu_scratch_ptr[kNoAllocMaxDevices] = {};
+std::atomic<double*> g_ilu_scratch_ptr[kNoAllocMaxDevices] = {};
 }  // namespace
 
 int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels) {
@@ -1407,7 +1545,7 @@ int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, c
                        "vfv_ilu0_apply_device_noalloc: the pattern's ILU(0) storage is not set up; call vfv_ilu0_apply_device or an "
                        "ILU(0) solve on it once first (that call allocates)");
     IluStruct& S = *it->second;
-    double* scratch = g_ilu_scratch_ptr[ctx->device];
+    double* scratch = g_ilu_scratch_ptr[ctx->device].load(std::memory_order_acquire);
     if (!scratch) {
         int cur = -1;
         CK(cudaGetDevice(&cur));
@@ -1415,11 +1553,11 @@ int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, c
         const cudaError_t e = cudaGetSymbolAddress((void**)&scratch, g_ilu_scratch);
         if (cur != ctx->device) cudaSetDevice(cur);
         if (e != cudaSuccess) return set_err(ctx, VFV_CUDA_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_ilu_scratch_ptr[ctx->device] = scratch;
+        g_ilu_scratch_ptr[ctx->device].store(scratch, std::memory_order_release);
     }
     int rc = ilu_refresh(ctx, p, S, false);  // numeric factor into the storage made at set-up
     if (rc) return rc;
-    ilu_apply<double>(ctx->stream, S, S.lu64.p, r, scratch, z, nullptr);
+    ilu_apply_levels<double>(ctx->stream, S, S.lu64.p, r, scratch, z, nullptr);
     ctx->launches += 2 * S.nlev;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());

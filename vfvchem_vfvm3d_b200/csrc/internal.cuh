@@ -83,9 +83,26 @@ struct IluStruct {
     DBuf<double> lu64;
     DBuf<float> lu32;
     DBuf<int> bad;
-
-
     uint64_t version64 = ~0ull, version32 = ~0ull;
+
+    // single-launch sweeps (k_ilu0_chain): row tasks inside levels, and per precision the four
+    // work vectors, the claim/parity state and a host-mapped timeout flag for standalone applies
+    DBuf<int32_t> tasks;
+    int ntask = 0;
+    struct Chain {
+        DBuf<unsigned char> work;   // 4 x n words of the precision
+        DBuf<unsigned char> state;  // IluChainState
+        int* h_flag = nullptr;      // pinned, mapped: set by a wait that gave up
+        int* d_flag = nullptr;
+        int grid = 0;
+    } chain[2];                     // [0] double, [1] float
+    IluStruct() = default;
+    IluStruct(const IluStruct&) = delete;
+    IluStruct& operator=(const IluStruct&) = delete;
+    ~IluStruct() {
+        for (auto& c : chain)
+            if (c.h_flag) cudaFreeHost(c.h_flag);
+    }
 };
 
 struct SolverBase {

@@ -27,6 +27,14 @@ class LinearGmresCudaError(VFVChemError):
     code = 4
 
 
+class DeviceWaitTimeout(VFVChemError):
+    """A bounded device wait gave up (status 5); the context stays usable. No reference
+    counterpart: the reference's CPU solver has no device waits. Like any solve error it is
+    recoverable by the caller (transient_adaptive.rs:190-205 retries a failed solve)."""
+
+    code = 5
+
+
 class LinearGmresNonPositiveThreads(LinearGmresBadInput):
     """``LinearGmresNonPositiveThreads { num_thread }`` (linear_gmres.rs:26-28)."""
 
@@ -43,7 +51,8 @@ class LinearGmresNonPositiveMaxOuter(LinearGmresBadInput):
     """``LinearGmresNonPositiveMaxOuter { max_outer }`` (linear_gmres.rs:35-37)."""
 
 
-_BY_CODE = {1: LinearGmresDidNotConverge, 2: LinearGmresNonFinite, 3: LinearGmresBadInput, 4: LinearGmresCudaError}
+_BY_CODE = {1: LinearGmresDidNotConverge, 2: LinearGmresNonFinite, 3: LinearGmresBadInput, 4: LinearGmresCudaError,
+            5: DeviceWaitTimeout}
 
 
 def raise_for(code: int, message: str) -> None:
