@@ -213,10 +213,17 @@ vfv_pattern* vfv_transport_pattern(vfv_transport* t);
 int vfv_transport_info(const vfv_transport* t, int64_t* n_tot, int64_t* nnz, int32_t* nmesh, int64_t* row_ptr);
 /* matrix from the diffusivity D[n_tot] and velocity vel[3][n_tot] (host or device arrays) */
 int vfv_transport_assemble(vfv_ctx* ctx, vfv_transport* t, const double* D, const double* vel, int on_device);
-/* nsteps implicit-Euler steps from c0 (host, n_tot) to c_out (host); one batched GMRES per step,
- * converged when every mesh meets ||b_i - A_i c_i|| <= tol ||b_i||; iters[nsteps] may be NULL */
+/* nsteps implicit-Euler steps from c0 (host, n_tot) to c_out (host). Per step one batched GMRES in
+ * which every mesh has its own Krylov recurrence (its own dot products, Hessenberg matrix, Givens
+ * rotations and stopping test, as if it were solved alone: TransientBase::solve solves each system
+ * by itself, src/transient/transient_base.rs:83-109), converged when every mesh meets
+ * ||b_i - A_i c_i|| <= tol ||b_i||; a mesh that has converged is masked out of the orthogonalisation.
+ * The graph engine is used whatever opts->engine says. iters[nsteps] (may be NULL): Arnoldi steps of
+ * the batch per time step (a step counts while any mesh is active). */
 int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, const vfv_gmres_opts* opts, double* c_out,
                       int32_t* iters);
+/* Arnoldi steps of every mesh summed over the time steps of the last vfv_transport_run (steps[nmesh]) */
+int vfv_transport_mesh_steps(const vfv_transport* t, int64_t* steps);
 /* Transient adjoint (no reference counterpart): J = 0.5 ||c_nsteps - target||^2 and dJ/dD for the
  * uniform diffusivity D of the last vfv_transport_assemble. Forward states are checkpointed every
  * `every` steps and recomputed segment by segment during the backward sweep of transposed solves.

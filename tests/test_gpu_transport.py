@@ -115,3 +115,30 @@ def test_transient_adjoint_dJdD_matches_finite_differences(gpu_ctx, batch):
     # the checkpoint interval changes only the schedule, not the result
     _, g2 = tr.adjoint_D(c0, 25, target, every=7, opts=opts)
     assert abs(g2 - g) <= 1e-9 * abs(g)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mesh_in_a_batch_iterates_as_if_alone(gpu_ctx, precision):
+    """Every mesh of a batch has its own Krylov recurrence: a mesh solved inside a 16-mesh batch
+    gives the iterate of the same mesh solved alone (to 1e-12; the arithmetic is the same), and
+    its Arnoldi steps are its own."""
+    from vfvchem_vfvm3d_b200 import GmresOptions, Mesh, TransientTransportGpu
+    from vfvchem_vfvm3d_b200 import _lib as L
+    from vfvchem_vfvm3d_b200.problems import transport_fields
+    ns = [5, 9, 6, 7, 5, 8, 6, 10, 5, 7, 9, 6, 8, 5, 7, 6]
+    meshes = Mesh.jitter_cubes(ns, [101 + i for i in range(16)])
+    vel, c0 = transport_fields(meshes)
+    opts = GmresOptions(tol=1e-10, restart=20, max_outer=200, precond=L.PRECOND_ILU0, precision=precision,
+                        inner_rtol=1e-6 if precision else 0.0)
+    tr = TransientTransportGpu(meshes, DT, ctx=gpu_ctx)
+    tr.assemble(1e-3, vel)
+    c_b, _ = tr.run(c0, 3, opts)
+    steps_b = tr.mesh_steps()
+    assert steps_b.shape == (16,) and np.all(steps_b > 0)
+    for i in (0, 7, 13):
+        r0, r1 = tr.row_ptr[i], tr.row_ptr[i + 1]
+        alone = TransientTransportGpu([meshes[i]], DT, ctx=gpu_ctx)
+        alone.assemble(1e-3, vel[:, r0:r1])
+        c_a, its_a = alone.run(c0[r0:r1], 3, opts)
+        assert np.linalg.norm(c_b[r0:r1] - c_a) <= 1e-12 * np.linalg.norm(c_a)
+        assert steps_b[i] == alone.mesh_steps()[0] == int(np.sum(its_a))

@@ -98,6 +98,7 @@ SIGNATURES = [
     ("vfv_transport_info", C.c_int, [_P, _I64P, _I64P, _I32P, _I64P]),
     ("vfv_transport_assemble", C.c_int, [_P, _P, _P, _P, C.c_int]),
     ("vfv_transport_run", C.c_int, [_P, _P, _DP, C.c_int, C.POINTER(GmresOpts), _DP, _I32P]),
+    ("vfv_transport_mesh_steps", C.c_int, [_P, _I64P]),
     ("vfv_transport_adjoint_D", C.c_int, [_P, _P, _DP, C.c_int, C.c_int, _DP, C.POINTER(GmresOpts), _DP, _DP, _I32P]),
     ("vfv_flow_pattern_host", C.c_int, [_P, C.c_int64, _I64P, _I64P, _I32P, _I32P]),
     ("vfv_flow_create", C.c_int, [_P, _P, _DP, _DP, _DP, _DP, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]),

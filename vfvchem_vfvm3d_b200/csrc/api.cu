@@ -12,6 +12,7 @@
 #include "kernels/ilu0.cuh"
 #include "kernels/gmres_cycle.cuh"
 #include "kernels/krylov.cuh"
+#include "kernels/krylov_batch.cuh"
 #include "kernels/ns.cuh"
 #include "host/ns_setup.hpp"
 #include "host/sort.hpp"
@@ -59,6 +60,28 @@ void launch_spmv(cudaStream_t s, int lanes, int64_t n, const int32_t* rp, const 
             break;
         default:
             k_spmv<TV, TX, TY, TA, 4><<<grid_for(n * 4), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
+    }
+}
+
+// SpMV of a batched solve: the step's scale 1/beta_j looked up per row from its mesh
+template <typename TV, typename TX, typename TY, typename TA>
+void launch_spmv_seg(cudaStream_t s, int lanes, int64_t n, const int32_t* rp, const int32_t* ci, const TV* val, const TX* x, TY* y,
+                     const double* inv_beta, int stride, int j, const int64_t* mesh_row, int nm, const DevStatus* st) {
+    switch (lanes) {
+        case 2:
+            k_spmv_seg<TV, TX, TY, TA, 2><<<grid_for(n * 2), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
+            break;
+        case 8:
+            k_spmv_seg<TV, TX, TY, TA, 8><<<grid_for(n * 8), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
+            break;
+        case 16:
+            k_spmv_seg<TV, TX, TY, TA, 16><<<grid_for(n * 16), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
+            break;
+        case 32:
+            k_spmv_seg<TV, TX, TY, TA, 32><<<grid_for(n * 32), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
+            break;
+        default:
+            k_spmv_seg<TV, TX, TY, TA, 4><<<grid_for(n * 4), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
     }
 }
 
@@ -479,7 +502,6 @@ struct Gmres : SolverBase {
     int nblk = 0, mega_grid = 0, mega_chunk = 0;
     DBuf<T> V, z, z2, zc, valK;
     DBuf<unsigned> bar;
-    DBuf<double> blk_buf;  // per-block residual / rhs norms of a batched solve
     DBuf<unsigned long long> trace;  // per-phase timestamps of the last cycle (VFV_TRACE_CYCLE=1)
     DBuf<double> part, hacc, coef, H, cs, sn, g, beta, inv_beta, y, dinv, scal, x, b;
     DBuf<double> binv64;  // block-Jacobi inverses [16][n/4]
@@ -501,6 +523,15 @@ struct Gmres : SolverBase {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int ilu_prio = 0;  // greatest stream priority: the sweeps' blocks go first when SM slots free up
     bool ilu_chain = true;  // ILU(0) sweeps as one k_ilu0_chain launch (false: one launch per level)
+    // batch of independent meshes (block-diagonal system), one Krylov recurrence per mesh
+    int nm = 0;
+    DBuf<int64_t> b_mesh_row, b_tile_row, b_rtile_row;
+    DBuf<int32_t> b_tile_mesh, b_mesh_tile, b_rtile_mesh, b_mesh_rtile;
+    DBuf<double> b_part, b_rpart, b_hacc, b_coef, b_H, b_cs, b_sn, b_g, b_beta, b_inv_beta, b_y, b_tol;
+    DBuf<MeshStat> b_ms;
+    DBuf<unsigned> b_counter;
+    BatchDev B{};
+    std::vector<MeshStat> mesh_stat;  // per-mesh state after the last solve
     long long wait_polls = kDefaultWaitPolls;  // bounded device waits of this solve (vfv_gmres_opts::wait_limit)
     ~Gmres() override {
         if (exec) cudaGraphExecDestroy(exec);
@@ -618,6 +649,84 @@ struct Gmres : SolverBase {
                 if (rc) return rc;
             }
         }
+        return VFV_OK;
+    }
+
+    // Tiles of the batched kernels from the mesh row ranges: vector tiles of kBlk * kRows rows and
+    // residual tiles of kBlk / kSpG rows, each starting at its mesh's first row.
+    int init_batch(vfv_ctx* ctx, const std::vector<int64_t>& rows) {
+        nm = (int)rows.size() - 1;
+        std::vector<int64_t> tr, rr;
+        std::vector<int32_t> tm, mt(nm + 1), rm, mr(nm + 1);
+        const int64_t tv = (int64_t)kBlk * kRows, tres = kBlk / kSpG;
+        for (int q = 0; q < nm; ++q) {
+            mt[q] = (int32_t)tm.size();
+            mr[q] = (int32_t)rm.size();
+            for (int64_t r = rows[q]; r < rows[q + 1]; r += tv) {
+                tr.push_back(r);
+                tm.push_back(q);
+            }
+            for (int64_t r = rows[q]; r < rows[q + 1]; r += tres) {
+                rr.push_back(r);
+                rm.push_back(q);
+            }
+        }
+        mt[nm] = (int32_t)tm.size();
+        mr[nm] = (int32_t)rm.size();
+        tr.push_back(rows[nm]);
+        rr.push_back(rows[nm]);
+        cudaStream_t s = ctx->stream;
+        CK(b_mesh_row.upload(rows.data(), rows.size(), s));
+        CK(b_tile_row.upload(tr.data(), tr.size(), s));
+        CK(b_tile_mesh.upload(tm.data(), tm.size(), s));
+        CK(b_mesh_tile.upload(mt.data(), mt.size(), s));
+        CK(b_rtile_row.upload(rr.data(), rr.size(), s));
+        CK(b_rtile_mesh.upload(rm.data(), rm.size(), s));
+        CK(b_mesh_rtile.upload(mr.data(), mr.size(), s));
+        const int ntile = (int)tm.size(), nrtile = (int)rm.size();
+        CK(b_part.alloc((size_t)kMaxBasis * ntile));
+        CK(b_rpart.alloc(nrtile));
+        CK(b_hacc.alloc((size_t)nm * kMaxBasis));
+        CK(b_coef.alloc((size_t)nm * kMaxBasis));
+        CK(b_H.alloc((size_t)nm * m * (m + 1)));
+        CK(b_cs.alloc((size_t)nm * m));
+        CK(b_sn.alloc((size_t)nm * m));
+        CK(b_g.alloc((size_t)nm * (m + 1)));
+        CK(b_beta.alloc((size_t)nm * (m + 1)));
+        CK(b_inv_beta.alloc((size_t)nm * (m + 1)));
+        CK(b_y.alloc((size_t)nm * m));
+        CK(b_tol.alloc(nm));
+        CK(b_ms.alloc(nm));
+        CK(b_counter.alloc(4));
+        CK(cudaMemset(b_counter.p, 0, 4 * sizeof(unsigned)));
+        B.nm = nm;
+        B.m = m;
+        B.ldv = ldv;
+        B.mesh_row = b_mesh_row.p;
+        B.tile_row = b_tile_row.p;
+        B.tile_mesh = b_tile_mesh.p;
+        B.mesh_tile = b_mesh_tile.p;
+        B.rtile_row = b_rtile_row.p;
+        B.rtile_mesh = b_rtile_mesh.p;
+        B.mesh_rtile = b_mesh_rtile.p;
+        B.ntile = ntile;
+        B.nrtile = nrtile;
+        B.part = b_part.p;
+        B.rpart = b_rpart.p;
+        B.hacc = b_hacc.p;
+        B.coef = b_coef.p;
+        B.H = b_H.p;
+        B.cs = b_cs.p;
+        B.sn = b_sn.p;
+        B.g = b_g.p;
+        B.beta = b_beta.p;
+        B.inv_beta = b_inv_beta.p;
+        B.y = b_y.p;
+        B.tol_abs = b_tol.p;
+        B.ms = b_ms.p;
+        B.counter = b_counter.p;
+        B.st = st.p;
+        B.scal = scal.p;
         return VFV_OK;
     }
 
@@ -760,6 +869,23 @@ struct Gmres : SolverBase {
         const T* vk = krylov_vals(p);
         const int lanes = p->spmv_lanes[sizeof(T) == 8 ? 0 : 1];
         T* w = V.p + (int64_t)(j + 1) * ldv;
+        if (nm > 0) {  // one recurrence per mesh of a batch
+            const T* uj = V.p + (int64_t)j * ldv;
+            const T* in = uj;
+            if (precond == VFV_PRECOND_ILU0) {
+                apply_ilu(s, uj, z.p, st.p);
+                in = z.p;
+            }
+            launch_spmv_seg<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, in, w, b_inv_beta.p, m + 1, j, b_mesh_row.p, nm, st.p);
+            const int fb = grid_for((int64_t)nm * (j + 1) * 32);
+            k_bmdot<T><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, j + 1);
+            k_bdots_finish<true><<<fb, 256, 0, s>>>(B, j + 1);
+            k_bupdate<T, false><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, w, j + 1);
+            k_bdots_finish<false><<<fb, 256, 0, s>>>(B, j + 1);
+            k_bupdate<T, true><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, w, j + 1);
+            k_bstep_finish<<<nm, kBlk, 0, s>>>(B, j);
+            return;
+        }
         if (engine == VFV_ENGINE_OVERLAP) {
             launch_spmv<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, Zb.p + (int64_t)j * ldv, abuf.p, inv_beta.p + j, st.p);
             cudaEventRecord(ev_fork, s);
@@ -795,8 +921,23 @@ struct Gmres : SolverBase {
     void enqueue_epilogue(cudaStream_t s, vfv_pattern* p) {
         constexpr int G = kSpG;
         const int sp_blocks = grid_for(n * G);
-        k_backsolve<<<1, 32, 0, s>>>(K);
         const int vb = grid_for(n);
+        if (nm > 0) {
+            k_bbacksolve<<<grid_for(nm, 128), 128, 0, s>>>(B);
+            if (precond == VFV_PRECOND_ILU0) {
+                k_bcombine<T, 2><<<B.ntile, kBlk, 0, s>>>(B, V.p, x.p, nullptr, z.p);
+                apply_ilu(s, z.p, z.p, nullptr);
+                k_add_to_x<T><<<vb, 256, 0, s>>>(n, x.p, z.p);
+            } else if (precond == VFV_PRECOND_JACOBI) {
+                k_bcombine<T, 1><<<B.ntile, kBlk, 0, s>>>(B, V.p, x.p, dinv.p, nullptr);
+            } else {
+                k_bcombine<T, 0><<<B.ntile, kBlk, 0, s>>>(B, V.p, x.p, nullptr, nullptr);
+            }
+            k_bresidual<T, G><<<B.nrtile, kBlk, 0, s>>>(B, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+            k_bresid_finish<<<nm, kBlk, 0, s>>>(B);
+            return;
+        }
+        k_backsolve<<<1, 32, 0, s>>>(K);
         if (engine == VFV_ENGINE_OVERLAP) {
             k_combine<T, 0><<<vb, kBlk, 0, s>>>(K, Zb.p, x.p, nullptr, nullptr);
         } else if (precond == VFV_PRECOND_ILU0) {
@@ -913,11 +1054,10 @@ struct Gmres : SolverBase {
         return cudaSuccess;
     }
 
-    // nblk > 0: block-diagonal system with block row ranges blk_d[0..nblk] (device); converged
-    // when every block meets ||b_i - A_i x_i|| <= tol ||b_i|| (the device stops a cycle early only on
-    // ||r|| <= tol min_i ||b_i||, which implies it for every block).
+    // A batched solver (nm > 0, a block-diagonal system of independent meshes) runs one Krylov
+    // recurrence per mesh and stops when every mesh meets ||b_i - A_i x_i|| <= tol ||b_i||.
     int solve(vfv_ctx* ctx, vfv_pattern* p, const double* d_b, const double* d_x0, double* d_x, const vfv_gmres_opts& o,
-              vfv_solve_info* info, int nblk = 0, const int64_t* blk_d = nullptr) {
+              vfv_solve_info* info) {
         cudaStream_t s = ctx->stream;
         constexpr int G = kSpG;
         const bool mixed = !std::is_same<T, double>::value;
@@ -952,49 +1092,49 @@ struct Gmres : SolverBase {
             if (bad) return set_err(ctx, VFV_NONFINITE, "block-Jacobi(4): singular diagonal block");
             bj_version = p->version;
         }
-        // ||b|| and the absolute tolerance
-        const int nb = std::min(grid_for(n), 1024);
-        k_norm2<<<nb, kBlk, 0, s>>>(n, b.p, part.p, counter.p + 4, scal.p + 2);
-        ctx->launches += 1;
-        CK(cudaMemcpyAsync(ctx->h_scalar, scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        CK(cudaGetLastError());
-        const double bnorm = std::sqrt(ctx->h_scalar[0]);
-        if (info) {
-            info->bnorm = bnorm;
-            info->levels = ilu ? ilu->nlev : 0;
-        }
-        if (!std::isfinite(bnorm)) return set_err(ctx, VFV_NONFINITE, "right-hand side is not finite");
-        if (bnorm == 0.0) {
-            CK(cudaMemsetAsync(d_x, 0, n * sizeof(double), s));
-            CK(cudaStreamSynchronize(s));
-            if (info) {
-                info->status = VFV_OK;
-                info->iters = info->cycles = 0;
-                info->relres = 0.0;
-            }
-            return VFV_OK;
-        }
-        double tol_abs = o.tol * bnorm;
-        std::vector<double> blk_b2, blk_r2;
-        if (nblk > 0) {
-            if ((int64_t)blk_buf.n < 2 * (int64_t)nblk) CK(blk_buf.alloc(2 * (size_t)nblk));
-            k_block_resid2<<<nblk, kBlk, 0, s>>>(p->rp.p, p->ci.p, p->val.p, x.p, b.p, blk_d, blk_buf.p, blk_buf.p + nblk);
+        double bnorm = 0.0, tol_abs = 0.0;
+        if (nm > 0) {
+            // per-mesh ||b_i||, tolerances and first residuals (meshes with b_i = 0 get x_i = 0)
+            const double hs[2] = {0.0, mixed ? std::max(0.0, o.inner_rtol) : 0.0};
+            CK(cudaMemcpyAsync(scal.p, hs, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+            CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
+            k_bnorm<<<nm, kBlk, 0, s>>>(B, b.p, o.tol);
+            k_bzero_x<<<grid_for(n), 256, 0, s>>>(B, x.p);
+            k_bresidual<T, G><<<B.nrtile, kBlk, 0, s>>>(B, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+            k_bresid_finish<<<nm, kBlk, 0, s>>>(B);
+            ctx->launches += 4;
+            if (info) info->levels = ilu ? ilu->nlev : 0;
+        } else {
+            // ||b|| and the absolute tolerance
+            const int nb = std::min(grid_for(n), 1024);
+            k_norm2<<<nb, kBlk, 0, s>>>(n, b.p, part.p, counter.p + 4, scal.p + 2);
             ctx->launches += 1;
-            blk_b2.resize(nblk);
-            blk_r2.resize(nblk);
-            CK(cudaMemcpyAsync(blk_b2.data(), blk_buf.p + nblk, nblk * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(ctx->h_scalar, scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
-            double bmin = 1e300;
-            for (double v : blk_b2)
-                if (v > 0.0) bmin = std::min(bmin, std::sqrt(v));
-            tol_abs = o.tol * (bmin < 1e300 ? bmin : bnorm);
+            CK(cudaGetLastError());
+            bnorm = std::sqrt(ctx->h_scalar[0]);
+            if (info) {
+                info->bnorm = bnorm;
+                info->levels = ilu ? ilu->nlev : 0;
+            }
+            if (!std::isfinite(bnorm)) return set_err(ctx, VFV_NONFINITE, "right-hand side is not finite");
+            if (bnorm == 0.0) {
+                CK(cudaMemsetAsync(d_x, 0, n * sizeof(double), s));
+                CK(cudaStreamSynchronize(s));
+                if (info) {
+                    info->status = VFV_OK;
+                    info->iters = info->cycles = 0;
+                    info->relres = 0.0;
+                }
+                return VFV_OK;
+            }
+            tol_abs = o.tol * bnorm;
+            const double hs[2] = {tol_abs, mixed ? std::max(0.0, o.inner_rtol) : 0.0};
+            CK(cudaMemcpyAsync(scal.p, hs, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+            CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
+            k_residual<T, G><<<grid_for(n * G), kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
+            ctx->launches += 1;
         }
-        const double hs[2] = {tol_abs, mixed ? std::max(0.0, o.inner_rtol) : 0.0};
-        CK(cudaMemcpyAsync(scal.p, hs, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
-        CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
-        k_residual<T, G><<<grid_for(n * G), kBlk, 0, s>>>(K, p->rp.p, p->ci.p, p->val.p, x.p, b.p, V.p);
-        ctx->launches += 1;
         if (engine != VFV_ENGINE_PERSISTENT && !exec) {
             cudaGraph_t graph = nullptr;
             cudaError_t e = cudaErrorUnknown;
@@ -1053,15 +1193,6 @@ struct Gmres : SolverBase {
                 break;
             }
             if (hst.converged) break;
-            if (nblk > 0 && cycles > 0) {
-                k_block_resid2<<<nblk, kBlk, 0, s>>>(p->rp.p, p->ci.p, p->val.p, x.p, b.p, blk_d, blk_buf.p, nullptr);
-                ctx->launches += 1;
-                CK(cudaMemcpyAsync(blk_r2.data(), blk_buf.p, nblk * sizeof(double), cudaMemcpyDeviceToHost, s));
-                CK(cudaStreamSynchronize(s));
-                bool all = true;
-                for (int i = 0; i < nblk && all; ++i) all = blk_r2[i] <= o.tol * o.tol * blk_b2[i];
-                if (all) break;
-            }
             if (cycles >= o.max_outer) {
                 rc = VFV_NOT_CONVERGED;
                 break;
@@ -1083,25 +1214,37 @@ struct Gmres : SolverBase {
         CK(cudaGetLastError());
         if (trace.p) dump_trace(ctx, cycles);
         if (const char* e = getenv("VFV_PROFILE_STEP")) {
-            if (e[0] == '1' && engine == VFV_ENGINE_GRAPH) profile_step(ctx, p);
+            if (e[0] == '1' && engine == VFV_ENGINE_GRAPH && nm == 0) profile_step(ctx, p);
         }
 
         CK(cudaMemcpyAsync(d_x, x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        double relres = bnorm > 0.0 ? hst.beta0 / bnorm : 0.0;
+        if (nm > 0) {  // the batch's relative residual is its worst mesh's
+            mesh_stat.resize(nm);
+            CK(cudaMemcpyAsync(mesh_stat.data(), b_ms.p, nm * sizeof(MeshStat), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            relres = 0.0;
+            for (const MeshStat& M : mesh_stat) {
+                bnorm = std::max(bnorm, M.bnorm);
+                if (M.bnorm > 0.0) relres = std::max(relres, M.beta0 / M.bnorm);
+            }
+            if (info) info->bnorm = bnorm;
+        }
         CK(cudaStreamSynchronize(s));
         if (const char* e = getenv("VFV_TRACE_SOLVE")) {  // diagnostics: one line per solve
             if (e[0] == '1')
-                fprintf(stderr, "[vfv solve] n=%lld %s cycles=%d iters=%d relres=%.3e bnorm=%.3e tol_abs=%.3e nblk=%d\n", (long long)n,
-                        mixed ? "mixed" : "fp64", cycles, hst.total_steps, hst.beta0 / bnorm, bnorm, tol_abs, nblk);
+                fprintf(stderr, "[vfv solve] n=%lld %s cycles=%d iters=%d relres=%.3e bnorm=%.3e tol_abs=%.3e meshes=%d\n", (long long)n,
+                        mixed ? "mixed" : "fp64", cycles, hst.total_steps, relres, bnorm, tol_abs, nm);
         }
         if (info) {
             info->status = rc;
             info->iters = hst.total_steps;
             info->cycles = cycles;
-            info->relres = hst.beta0 / bnorm;
+            info->relres = relres;
         }
         if (rc == VFV_NOT_CONVERGED)
             return set_err(ctx, rc, "GMRES did not converge in " + std::to_string(o.max_outer) + " restart cycles (relres " +
-                                        std::to_string(hst.beta0 / bnorm) + ")");
+                                        std::to_string(relres) + ")");
         if (rc == VFV_NONFINITE) return set_err(ctx, rc, "GMRES: non-finite residual");
         if (rc == VFV_TIMEOUT) return set_err(ctx, rc, "GMRES: a bounded device wait gave up (grid barrier or ILU(0) sweep)");
         return VFV_OK;
@@ -1129,26 +1272,50 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
 }
 
 int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info,
-              int nblk, const int64_t* blk_d) {
-    const auto key = std::make_tuple(o->precision, o->precond, o->precond == VFV_PRECOND_ILU0 ? o->ilu_order : 0, o->restart, o->engine);
+              bool batched) {
+    vfv_gmres_opts oo = *o;
+    batched = batched && p->blocks.size() > 2;
+    if (batched) {
+        if (oo.precond == VFV_PRECOND_BJ4) return set_err(ctx, VFV_BAD_INPUT, "block-Jacobi(4) is not offered for batches of meshes");
+        oo.engine = VFV_ENGINE_GRAPH;  // the per-mesh recurrences run on the graph engine
+    }
+    const auto key = std::make_tuple(oo.precision, oo.precond, oo.precond == VFV_PRECOND_ILU0 ? oo.ilu_order : 0, oo.restart,
+                                     oo.engine + (batched ? 16 : 0));
     auto it = p->solvers.find(key);
     if (it == p->solvers.end()) {
         std::unique_ptr<SolverBase> sb;
         int rc;
-        if (o->precision == VFV_MIXED) {
+        if (oo.precision == VFV_MIXED) {
             auto g = std::make_unique<Gmres<float>>();
-            rc = g->init(ctx, p, o->restart, o->precond, o->ilu_order, o->engine);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine);
+            if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         } else {
             auto g = std::make_unique<Gmres<double>>();
-            rc = g->init(ctx, p, o->restart, o->precond, o->ilu_order, o->engine);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine);
+            if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         }
         if (rc) return rc;
         it = p->solvers.emplace(key, std::move(sb)).first;
     }
-    if (o->precision == VFV_MIXED) return static_cast<Gmres<float>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info, nblk, blk_d);
-    return static_cast<Gmres<double>*>(it->second.get())->solve(ctx, p, b, x0, x, *o, info, nblk, blk_d);
+    if (oo.precision == VFV_MIXED) return static_cast<Gmres<float>*>(it->second.get())->solve(ctx, p, b, x0, x, oo, info);
+    return static_cast<Gmres<double>*>(it->second.get())->solve(ctx, p, b, x0, x, oo, info);
+}
+
+// Per-mesh Arnoldi steps of the last batched solve of this pattern with these options (meshes in
+// block order); false when no such solve exists.
+bool batch_mesh_steps(const vfv_pattern* p, const vfv_gmres_opts* o, std::vector<int32_t>& steps) {
+    const auto key = std::make_tuple(o->precision, o->precond, o->precond == VFV_PRECOND_ILU0 ? o->ilu_order : 0, o->restart,
+                                     VFV_ENGINE_GRAPH + 16);
+    auto it = p->solvers.find(key);
+    if (it == p->solvers.end()) return false;
+    const std::vector<MeshStat>* ms = nullptr;
+    if (o->precision == VFV_MIXED) ms = &static_cast<Gmres<float>*>(it->second.get())->mesh_stat;
+    else ms = &static_cast<Gmres<double>*>(it->second.get())->mesh_stat;
+    steps.resize(ms->size());
+    for (size_t i = 0; i < ms->size(); ++i) steps[i] = (*ms)[i].total_steps;
+    return !ms->empty();
 }
 
 namespace {

@@ -132,9 +132,13 @@ struct vfv_mesh {
     Dual d;
 };
 
-// GMRES solve on device arrays (the solver of vfv_solve): cached per pattern and options.
+// GMRES solve on device arrays (the solver of vfv_solve): cached per pattern and options. batched:
+// the pattern's diagonal blocks (p->blocks) are independent meshes, each with its own Krylov
+// recurrence and stopping test.
 int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info,
-              int nblk = 0, const int64_t* blk_d = nullptr);
+              bool batched = false);
+// per-mesh Arnoldi steps of the last batched solve with these options
+bool batch_mesh_steps(const vfv_pattern* p, const vfv_gmres_opts* o, std::vector<int32_t>& steps);
 // argument checks of the reference's LinearGmres constructor and solve options
 int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o);
 // transpose of a pattern (tmap: slot in A of every entry of A^T) and the gather of A's values into it

@@ -458,33 +458,6 @@ __global__ void __launch_bounds__(kBlk) k_norm2(int64_t n, const double* __restr
     }
 }
 
-// Per-block ||b - A x||^2 (and ||b||^2 when b2 != null) for a block-diagonal system: one CTA per
-// block of rows [blk[i], blk[i+1]), deterministic. Used for the per-mesh stopping rule of a batch.
-__global__ void __launch_bounds__(256) k_block_resid2(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                     const double* __restrict__ val, const double* __restrict__ x,
-                                                     const double* __restrict__ b, const int64_t* __restrict__ blk, double* r2,
-                                                     double* b2) {
-    __shared__ double red[kBlk / 32];
-    const int64_t r0 = blk[blockIdx.x], r1 = blk[blockIdx.x + 1];
-    double sr = 0.0, sb = 0.0;
-    for (int64_t row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
-        double s = 0.0;
-        for (int32_t k = rp[row]; k < rp[row + 1]; ++k) s += val[k] * x[ci[k]];
-        const double r = b[row] - s;
-        sr += r * r;
-        sb += b[row] * b[row];
-    }
-    sr = block_sum(sr, red);
-    if (b2) {
-        __syncthreads();
-        sb = block_sum(sb, red);
-    }
-    if (threadIdx.x == 0) {
-        r2[blockIdx.x] = sr;
-        if (b2) b2[blockIdx.x] = sb;
-    }
-}
-
 // ---------------------------------------------------------------- matrix preparation
 // dinv[i] = 1 / a_ii (diag_pos[i] = slot of the diagonal, -1 if absent -> 1)
 __global__ void k_jacobi_inv(int64_t n, const int32_t* __restrict__ diag_pos, const double* __restrict__ val, double* __restrict__ dinv) {

@@ -25,6 +25,7 @@ struct vfv_transport {
     DBuf<int32_t> tmap;
     DBuf<double> adj;        // checkpoints, one segment of states, two adjoint vectors, rhs, zero, partials, terms
     DBuf<unsigned> adj_counter;
+    std::vector<int64_t> run_mesh_steps;  // Arnoldi steps per mesh summed over the last vfv_transport_run
     TransportDev dev() const {
         TransportDev T{};
         T.n = n;
@@ -182,17 +183,30 @@ int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nste
     CK(cudaMemcpyAsync(t->c0.p, c0, n * sizeof(double), cudaMemcpyHostToDevice, s));
     double* cur = t->c0.p;
     double* nxt = t->c1.p;
+    t->run_mesh_steps.assign(t->nmesh, 0);
+    std::vector<int32_t> ms;
     for (int k = 0; k < nsteps; ++k) {
         launch_transport_rhs(s, n, t->cvol.p, t->dt, cur, t->b.p);
         ctx->launches += 1;
         vfv_solve_info info{};
-        rc = solve_dev(ctx, t->pat, t->b.p, cur, nxt, opts, &info, t->nmesh, t->d_row_ptr.p);
+        rc = solve_dev(ctx, t->pat, t->b.p, cur, nxt, opts, &info, true);
         if (rc) return rc;
         if (iters) iters[k] = info.iters;
+        if (t->nmesh > 1 && batch_mesh_steps(t->pat, opts, ms))
+            for (int i = 0; i < t->nmesh; ++i) t->run_mesh_steps[i] += ms[i];
+        else if (t->nmesh == 1)
+            t->run_mesh_steps[0] += info.iters;
         std::swap(cur, nxt);
     }
     CK(cudaMemcpyAsync(c_out, cur, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    return VFV_OK;
+}
+
+int vfv_transport_mesh_steps(const vfv_transport* t, int64_t* steps) {
+    if (!t || !steps) return set_err(nullptr, VFV_BAD_INPUT, "NULL argument");
+    if ((int)t->run_mesh_steps.size() != t->nmesh) return set_err(nullptr, VFV_BAD_INPUT, "no vfv_transport_run yet");
+    std::memcpy(steps, t->run_mesh_steps.data(), t->nmesh * sizeof(int64_t));
     return VFV_OK;
 }
 
@@ -236,7 +250,7 @@ int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, in
     auto step = [&](const double* cin, double* cout) -> int {
         launch_transport_rhs(s, n, t->cvol.p, t->dt, cin, t->b.p);
         vfv_solve_info info{};
-        return solve_dev(ctx, t->pat, t->b.p, cin, cout, opts, &info, t->nmesh, t->d_row_ptr.p);
+        return solve_dev(ctx, t->pat, t->b.p, cin, cout, opts, &info, true);
     };
     // forward sweep, keeping checkpoints
     CK(cudaMemcpyAsync(t->c0.p, ck, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -260,7 +274,7 @@ int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, in
     if (J) *J = 0.5 * jsum;
     CK(cudaMemcpyAsync(rhs, hc.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
     vfv_solve_info info{};
-    if ((rc = solve_dev(ctx, t->pat_t, rhs, zero, lam, opts, &info, t->nmesh, t->d_row_ptr.p))) return rc;
+    if ((rc = solve_dev(ctx, t->pat_t, rhs, zero, lam, opts, &info, true))) return rc;
     if (adj_iters) adj_iters[nsteps - 1] = info.iters;
     // backward sweep over the segments, last first
     for (int k = nsteps - 1; k >= 0; --k) {
@@ -277,7 +291,7 @@ int vfv_transport_adjoint_D(vfv_ctx* ctx, vfv_transport* t, const double* c0, in
         launch_transport_dAdD_dot(s, T, lam, c_k1, part, t->adj_counter.p, terms + k);
         if (k > 0) {
             launch_transport_rhs(s, n, t->cvol.p, t->dt, lam, rhs);  // M^T lam = -vol lam / dt
-            if ((rc = solve_dev(ctx, t->pat_t, rhs, lam, lam2, opts, &info, t->nmesh, t->d_row_ptr.p))) return rc;
+            if ((rc = solve_dev(ctx, t->pat_t, rhs, lam, lam2, opts, &info, true))) return rc;
             if (adj_iters) adj_iters[k - 1] = info.iters;
             std::swap(lam, lam2);
         }

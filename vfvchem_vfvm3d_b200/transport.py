@@ -1,8 +1,10 @@
 """Batched transient advection-diffusion over many independent meshes.
 
 The meshes are concatenated into one block-diagonal system (``vfv_transport``); every kernel of
-the assembly and of the GMRES runs over all meshes at once, and each time step's solve stops when
-every mesh meets its own relative-residual tolerance. Operators per row, in push order:
+the assembly and of the GMRES runs over all meshes at once, while every mesh keeps its own Krylov
+recurrence (dot products, Hessenberg matrix, Givens rotations, stopping test), so each mesh is
+solved as if alone — the reference solves each system by itself (src/transient/transient_base.rs:83-109);
+a time step's solve ends when every mesh meets its own relative-residual tolerance. Operators per row, in push order:
 ``OpSclDomTimeUnity`` (src/operator/core/opscl_dom_timeunity.rs:32-58), ``OpSclDomDiffusion``
 (opscl_dom_diff.rs:40-91), ``OpSclDomAdvection`` (power law, opscl_dom_adv.rs:49-125) with the face
 mass flux of ``flow_helper::update_flux`` (flow_helper.rs:72-179) at zero pressure/body force.
@@ -50,6 +52,12 @@ class TransientTransportGpu:
         _check(self.ctx.handle, L.load().vfv_transport_run(self.ctx.handle, self._h, L.dptr(c0), int(nsteps), C.byref(o), L.dptr(out),
                                                           L.ptr(its, C.c_int32)))
         return out, its[:nsteps]
+
+    def mesh_steps(self) -> np.ndarray:
+        """Arnoldi steps of every mesh summed over the time steps of the last :meth:`run`."""
+        out = np.empty(self.nmesh, np.int64)
+        _check(self.ctx.handle, L.load().vfv_transport_mesh_steps(self._h, L.ptr(out, C.c_int64)))
+        return out
 
     def adjoint_D(self, c0, nsteps: int, target, every: int = 10, opts: GmresOptions | None = None, return_iters: bool = False):
         """(J, dJ/dD) for J = 0.5 ||c_nsteps - target||^2, checkpointing every `every` steps; with
