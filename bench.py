@@ -513,11 +513,18 @@ def main():
 
 
 def reference_heat_system(n):
-    """The workload's system for the reference arm, built on the host."""
-    from vfvchem_vfvm3d_b200.problems import steady_heat
-    prob = steady_heat(n, hetero=True)
-    rp, ci, va, b = oracle_heat_system(prob)
-    return rp, ci, va, b, prob.T0.copy(), "product host mesh + oracle assembly"
+    """The workload's system for the reference arm, built by the oracle alone: its jittered-cube
+    vertex set, its Bowyer-Watson Delaunay (delaunay.rs restated), its Voronoi dual (geom_tet.rs
+    restated) and its push-order assembly (steady_heat.rs); no product code runs in this process."""
+    import oracle
+    from oracle import mesh as om
+    from vfvchem_vfvm3d_b200.problems import HEAT_BND_KIND, HEAT_BND_ORDER, heat_fields
+    pos, node_bnd, n_pts = om.jitter_cube(n, 42, 0.25)
+    d = om.dual(pos, om.delaunay(pos), n_pts)
+    k, q, s, T0, bc = heat_fields(node_bnd, hetero=True)
+    r, c, v, b = oracle.heat_triplets(d, n_pts, node_bnd, HEAT_BND_ORDER, HEAT_BND_KIND, k, q, s, T0, bc)
+    rp, ci, va = oracle.csr_from_triplets(node_bnd.size, r, c, v)
+    return rp, ci, va, b, T0, "oracle mesh (jittered cube, Delaunay, dual) + oracle assembly"
 
 
 def run_reference(args, R):

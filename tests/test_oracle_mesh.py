@@ -1,0 +1,86 @@
+"""The mesh-stage oracle (oracle/mesh_oracle.c) against the product's host mesh code and against
+independent facts (CPU only).
+
+The oracle restates the reference's Bowyer-Watson insertion (src/base/delaunay.rs:6-170) and the
+dual of Tetrahedron::update_tet (src/base/geom_tet.rs:101-293) in C with exact predicates. The
+product builds the same tetrahedra (the Delaunay tetrahedralisation of points in general position
+is unique) in a different order (its insertion order and tetrahedron storage differ), so sums over
+tetrahedra agree to round-off, not bit for bit, and per-vertex boundary sub-faces agree as sets.
+"""
+import numpy as np
+import pytest
+from scipy.spatial import Delaunay
+
+from oracle import geom_tet
+from oracle import mesh as om
+
+
+def _tetset(t):
+    return set(map(tuple, np.sort(np.asarray(t), axis=1)))
+
+
+def test_jitter_cube_equals_product_vertices(lib_built):
+    from vfvchem_vfvm3d_b200 import Mesh
+    pos, bnd, npts = om.jitter_cube(9, 42, 0.25)
+    m = Mesh.jitter_cube(9, 42, 0.25)
+    ppos, pnb, _ = m.export()
+    assert npts == m.n_pts
+    assert np.array_equal(pos, ppos) and np.array_equal(bnd[npts:], pnb) and np.all(bnd[:npts] == -1)
+    assert np.array_equal(np.ldexp(pos, 18), np.rint(np.ldexp(pos, 18)))  # on the 2^-18 lattice
+
+
+@pytest.mark.parametrize("n", [5, 8, 12])
+def test_delaunay_equals_qhull_and_product(lib_built, n):
+    from vfvchem_vfvm3d_b200 import Mesh
+    pos, _, _ = om.jitter_cube(n, 100 + n, 0.25)
+    tets = om.delaunay(pos)
+    p = [pos[tets[:, i]] for i in range(4)]
+    det = np.einsum("ij,ij->i", p[0] - p[3], np.cross(p[1] - p[3], p[2] - p[3]))
+    assert np.all(det > 0) and abs(det.sum() / 6.0 - 1.0) < 1e-12
+    st = np.sort(Delaunay(pos).simplices, axis=1)
+    a, b, c, d = (pos[st[:, i]] for i in range(4))
+    st = st[np.abs(np.einsum("ij,ij->i", a - d, np.cross(b - d, c - d))) > 1e-15]
+    assert _tetset(tets) == _tetset(st)
+    _, _, ptets = Mesh.jitter_cube(n, 100 + n, 0.25).export()
+    assert _tetset(tets) == _tetset(ptets)
+
+
+def test_delaunay_rejects_duplicates():
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 0, 0]], float)
+    with pytest.raises(ValueError):
+        om.delaunay(pos)
+
+
+@pytest.mark.parametrize("n", [6, 10])
+def test_dual_agrees_with_product_and_numpy_restatement(lib_built, n):
+    from vfvchem_vfvm3d_b200 import Mesh
+    pos, _, npts = om.jitter_cube(n, 42, 0.25)
+    tets = om.delaunay(pos)
+    d = om.dual(pos, tets, npts)
+    nd = geom_tet.build_dual(pos, tets, npts)  # numpy restatement on the oracle's own tetrahedra and order
+    for k in ["nbr_ptr", "nbr_idx", "bnd_ptr", "bnd_j", "bnd_k"]:
+        assert np.array_equal(d[k].astype(np.int64), np.asarray(nd[k]).astype(np.int64)), k
+    for k in ["dist", "area", "norm", "skew", "grad_wgt", "cvol", "cskew", "bnd_area", "bnd_norm", "bnd_wgt"]:
+        scale = max(np.max(np.abs(nd[k])), 1e-300)
+        assert np.max(np.abs(d[k] - nd[k])) <= 1e-12 * scale, k
+    pd = Mesh.jitter_cube(n, 42, 0.25).dual()
+    for k in ["nbr_ptr", "nbr_idx", "bnd_ptr"]:
+        assert np.array_equal(d[k].astype(np.int64), pd[k].astype(np.int64)), k
+    for k in ["dist", "norm", "grad_wgt", "area", "cvol", "cskew"]:
+        assert np.max(np.abs(d[k] - pd[k])) <= 1e-12 * np.max(np.abs(pd[k])), k
+    # skew is a ratio with the face area: compare it on faces that carry area
+    big = np.abs(pd["area"]) > 1e-6 * pd["dist"] ** 2
+    assert np.max(np.abs(d["skew"][:, big] - pd["skew"][:, big])) <= 1e-10 * np.max(np.abs(pd["skew"]))
+    # boundary sub-faces: the same (j, k, area) per vertex, listed in each code's triangle order
+    for v in range(n ** 3):
+        a0, a1, b0, b1 = d["bnd_ptr"][v], d["bnd_ptr"][v + 1], pd["bnd_ptr"][v], pd["bnd_ptr"][v + 1]
+        sa = sorted(zip(d["bnd_j"][a0:a1], d["bnd_k"][a0:a1]))
+        sb = sorted(zip(pd["bnd_j"][b0:b1], pd["bnd_k"][b0:b1]))
+        assert sa == sb
+    # control volumes tile the unit cube and close: sum over faces of A n = 0 for interior points
+    assert abs(d["cvol"].sum() - 1.0) < 1e-12
+    v = np.repeat(np.arange(n ** 3), np.diff(d["nbr_ptr"]))
+    an = np.zeros((3, n ** 3))
+    for c in range(3):
+        np.add.at(an[c], v, d["area"] * d["norm"][c])
+    assert np.max(np.abs(an[:, :npts])) < 1e-12

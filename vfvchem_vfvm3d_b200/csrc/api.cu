@@ -13,6 +13,7 @@
 #include "kernels/gmres_cycle.cuh"
 #include "kernels/krylov.cuh"
 #include "kernels/krylov_batch.cuh"
+#include "kernels/krylov_staged.cuh"
 #include "kernels/ns.cuh"
 #include "host/ns_setup.hpp"
 #include "host/sort.hpp"
@@ -500,6 +501,8 @@ struct Gmres : SolverBase {
     int64_t n = 0, ldv = 0;
     int m = 0, precond = 0, ilu_order = 0, engine = 0;
     int nblk = 0, mega_grid = 0, mega_chunk = 0;
+    int nblk_v = 0;       // blocks of the register multi-vector kernels (kBlk * kRows rows each)
+    bool staged = true;   // Gram-Schmidt passes with the basis tile in shared memory (kStR-row tiles)
     DBuf<T> V, z, z2, zc, valK;
     DBuf<unsigned> bar;
     DBuf<unsigned long long> trace;  // per-phase timestamps of the last cycle (VFV_TRACE_CYCLE=1)
@@ -547,7 +550,18 @@ struct Gmres : SolverBase {
         ilu_order = ilu_order_;
         engine = engine_;
         ldv = (n + 63) / 64 * 64;
-        nblk = (int)((n + kBlk * kRows - 1) / (kBlk * kRows));
+        if (const char* e = getenv("VFV_ORTHO_REGS")) staged = e[0] != '1';
+        nblk_v = (int)((n + kBlk * kRows - 1) / (kBlk * kRows));
+        nblk = staged ? (int)((n + kStR - 1) / kStR) : nblk_v;  // partial dots per vector
+        if (staged) {
+            const int smax = (m + 1) * kStR * (int)sizeof(T);
+            CK(cudaFuncSetAttribute(k_mdot_s<T, SingleMap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+            CK(cudaFuncSetAttribute(k_update_s<T, SingleMap, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+            CK(cudaFuncSetAttribute(k_update_s<T, SingleMap, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+            CK(cudaFuncSetAttribute(k_mdot_s<T, BatchMap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+            CK(cudaFuncSetAttribute(k_update_s<T, BatchMap, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+            CK(cudaFuncSetAttribute(k_update_s<T, BatchMap, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+        }
         const int64_t res_blocks = (n * kSpG + kBlk - 1) / kBlk;
         CK(V.alloc((size_t)(m + 1) * ldv));
         CK(cudaMemset(V.p, 0, sizeof(T) * (size_t)(m + 1) * ldv));
@@ -658,7 +672,7 @@ struct Gmres : SolverBase {
         nm = (int)rows.size() - 1;
         std::vector<int64_t> tr, rr;
         std::vector<int32_t> tm, mt(nm + 1), rm, mr(nm + 1);
-        const int64_t tv = (int64_t)kBlk * kRows, tres = kBlk / kSpG;
+        const int64_t tv = staged ? (int64_t)kStR : (int64_t)kBlk * kRows, tres = kBlk / kSpG;
         for (int q = 0; q < nm; ++q) {
             mt[q] = (int32_t)tm.size();
             mr[q] = (int32_t)rm.size();
@@ -750,6 +764,27 @@ struct Gmres : SolverBase {
         else return ilu->lu32.p;
     }
 
+    // The CGS2 passes of Arnoldi step j on w = A M^-1 u_j (in `win`; the result goes to `w`, which
+    // may be the same vector): first-pass dots, update + second-pass dots, update + norm + Givens.
+    void enqueue_ortho(cudaStream_t s, const T* win, T* w, int j) {
+        const int nv = j + 1, fb = grid_for((int64_t)nv * 32);
+        if (staged) {
+            const SingleMap M{n, st.p};
+            const size_t sm = (size_t)nv * kStR * sizeof(T);
+            k_mdot_s<T, SingleMap><<<nblk, kStR, sm, s>>>(M, V.p, ldv, win, nv, part.p, nblk);
+            k_dots_finish<true><<<fb, 256, 0, s>>>(K, nv);
+            k_update_s<T, SingleMap, false, false><<<nblk, kStR, sm, s>>>(M, K, V.p, ldv, win, w, nv, coef.p, part.p, nblk, j);
+            k_dots_finish<false><<<fb, 256, 0, s>>>(K, nv);
+            k_update_s<T, SingleMap, true, true><<<nblk, kStR, sm, s>>>(M, K, V.p, ldv, w, w, nv, coef.p, part.p, nblk, j);
+            return;
+        }
+        k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, win, nv);
+        k_dots_finish<true><<<fb, 256, 0, s>>>(K, nv);
+        k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, win, w, nv, j);
+        k_dots_finish<false><<<fb, 256, 0, s>>>(K, nv);
+        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, nv, j);
+    }
+
     // phase timestamps of the last cycle, averaged over its steps (diagnostics, VFV_TRACE_CYCLE=1)
     void dump_trace(vfv_ctx* ctx, int cycles) {
         std::vector<unsigned long long> h((size_t)(m + 2) * 8);
@@ -795,19 +830,13 @@ struct Gmres : SolverBase {
         cudaEventRecord(ev[1], s);
         launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
         cudaEventRecord(ev[2], s);
-        k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
-        k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
+        enqueue_ortho(s, w, w, j);
         cudaEventRecord(ev[3], s);
-        k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
-        k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-        cudaEventRecord(ev[4], s);
-        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
-        cudaEventRecord(ev[5], s);
-        cudaEventSynchronize(ev[5]);
-        float t[5];
-        for (int q = 0; q < 5; ++q) cudaEventElapsedTime(&t[q], ev[q], ev[q + 1]);
-        fprintf(stderr, "[vfv step profile] %s j=%d (us): ilu %.1f spmv %.1f mdot %.1f update+dot %.1f update+norm %.1f\n",
-                sizeof(T) == 4 ? "fp32" : "fp64", j, t[0] * 1e3, t[1] * 1e3, t[2] * 1e3, t[3] * 1e3, t[4] * 1e3);
+        cudaEventSynchronize(ev[3]);
+        float t[3];
+        for (int q = 0; q < 3; ++q) cudaEventElapsedTime(&t[q], ev[q], ev[q + 1]);
+        fprintf(stderr, "[vfv step profile] %s j=%d (us): ilu %.1f spmv %.1f cgs2 passes %.1f (%s)\n", sizeof(T) == 4 ? "fp32" : "fp64",
+                j, t[0] * 1e3, t[1] * 1e3, t[2] * 1e3, staged ? "staged tiles" : "register tiles");
         for (auto& e : ev) cudaEventDestroy(e);
     }
 
@@ -877,12 +906,23 @@ struct Gmres : SolverBase {
                 in = z.p;
             }
             launch_spmv_seg<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, in, w, b_inv_beta.p, m + 1, j, b_mesh_row.p, nm, st.p);
-            const int fb = grid_for((int64_t)nm * (j + 1) * 32);
-            k_bmdot<T><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, j + 1);
-            k_bdots_finish<true><<<fb, 256, 0, s>>>(B, j + 1);
-            k_bupdate<T, false><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, w, j + 1);
-            k_bdots_finish<false><<<fb, 256, 0, s>>>(B, j + 1);
-            k_bupdate<T, true><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, w, j + 1);
+            const int nv = j + 1, fb = grid_for((int64_t)nm * nv * 32);
+            if (staged) {
+                const BatchMap M{b_tile_row.p, b_tile_mesh.p, b_ms.p, st.p};
+                const size_t sm = (size_t)nv * kStR * sizeof(T);
+                k_mdot_s<T, BatchMap><<<B.ntile, kStR, sm, s>>>(M, V.p, ldv, w, nv, b_part.p, B.ntile);
+                k_bdots_finish<true><<<fb, 256, 0, s>>>(B, nv);
+                k_update_s<T, BatchMap, false, false><<<B.ntile, kStR, sm, s>>>(M, K, V.p, ldv, w, w, nv, b_coef.p, b_part.p, B.ntile, j);
+                k_bdots_finish<false><<<fb, 256, 0, s>>>(B, nv);
+                k_update_s<T, BatchMap, true, false><<<B.ntile, kStR, sm, s>>>(M, K, V.p, ldv, w, w, nv, b_coef.p, b_part.p, B.ntile, j);
+                k_bstep_finish<<<nm, kStR, 0, s>>>(B, j);  // reduces the tile norms like the last block of k_update_s
+                return;
+            }
+            k_bmdot<T><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, nv);
+            k_bdots_finish<true><<<fb, 256, 0, s>>>(B, nv);
+            k_bupdate<T, false><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, w, nv);
+            k_bdots_finish<false><<<fb, 256, 0, s>>>(B, nv);
+            k_bupdate<T, true><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, w, nv);
             k_bstep_finish<<<nm, kBlk, 0, s>>>(B, j);
             return;
         }
@@ -892,13 +932,9 @@ struct Gmres : SolverBase {
             cudaStreamWaitEvent(s2, ev_fork, 0);
             apply_ilu(s2, abuf.p, qbuf.p, st.p, ilu_prio, true);
             cudaEventRecord(ev_join, s2);
-            k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, abuf.p, j + 1);
-            k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-            k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, abuf.p, w, j + 1, j);
-            k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-            k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
+            enqueue_ortho(s, abuf.p, w, j);
             cudaStreamWaitEvent(s, ev_join, 0);
-            k_zupdate<T><<<nblk, kBlk, 0, s>>>(K, Zb.p, qbuf.p, j + 1, j);
+            k_zupdate<T><<<nblk_v, kBlk, 0, s>>>(K, Zb.p, qbuf.p, j + 1, j);
             return;
         }
         const T* uj = V.p + (int64_t)j * ldv;
@@ -911,11 +947,7 @@ struct Gmres : SolverBase {
             in = z.p;
         }
         launch_spmv<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
-        k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, j + 1);
-        k_dots_finish<true><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-        k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
-        k_dots_finish<false><<<grid_for((int64_t)(j + 1) * 32), 256, 0, s>>>(K, j + 1);
-        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, j + 1, j);
+        enqueue_ortho(s, w, w, j);
     }
 
     void enqueue_epilogue(cudaStream_t s, vfv_pattern* p) {

@@ -264,6 +264,48 @@ __global__ void __launch_bounds__(256) k_dots_finish(KrylovDev K, int nvec) {
     }
 }
 
+// Completes Arnoldi step j from ||w||^2 (tot): Hessenberg column, norms, the rotation of the new
+// column by the previous Givens rotations and a new one, the residual estimate and the stopping
+// test. One thread.
+__device__ __forceinline__ void finish_column(KrylovDev K, int j, double tot) {
+    const int m1 = K.m + 1;
+    double* col = K.H + (int64_t)j * m1;
+    const double bnext = sqrt(tot);
+    for (int i = 0; i <= j; ++i) col[i] = K.hacc[i];
+    col[j + 1] = bnext;
+    K.beta[j + 1] = bnext;
+    K.inv_beta[j + 1] = 1.0 / bnext;
+    for (int i = 0; i < j; ++i) {
+        const double a = col[i], bb = col[i + 1];
+        col[i] = K.cs[i] * a + K.sn[i] * bb;
+        col[i + 1] = -K.sn[i] * a + K.cs[i] * bb;
+    }
+    const double a = col[j], bb = col[j + 1];
+    const double rr = hypot(a, bb);
+    double c = 1.0, sgn = 0.0;
+    if (rr > 0.0) {
+        c = a / rr;
+        sgn = bb / rr;
+    }
+    K.cs[j] = c;
+    K.sn[j] = sgn;
+    col[j] = rr;
+    col[j + 1] = 0.0;
+    const double gj = K.g[j];
+    K.g[j] = c * gj;
+    K.g[j + 1] = -sgn * gj;
+    const double est = fabs(K.g[j + 1]);
+    DevStatus* st = K.st;
+    st->steps = j + 1;
+    st->total_steps += 1;
+    st->resid_est = est;
+    const bool fin = isfinite(est) && isfinite(bnext) && isfinite(rr);
+    if (!fin) st->nonfinite = 1;
+    const double floor_abs = K.scal[1] * st->beta0;
+    const bool stop = !fin || rr == 0.0 || bnext == 0.0 || est <= K.scal[0] || est <= floor_abs || j + 1 >= K.m;
+    if (stop) st->done = 1;
+}
+
 // ---------------------------------------------------------------- update + second pass
 // w <- win - sum_i coef_i u_i (win == w except in the overlapped engine). Then, with FINAL == false, the partials of the second CGS pass
 // d'_i = <u_i, w> (k_dots_finish<false> adds d'_i/beta_i into hacc and sets coef); with
@@ -334,42 +376,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, con
         const double tot = reduce_partials(K.part, gridDim.x, red2);
         if (threadIdx.x == 0) {
             K.counter[3] = 0u;
-            const int m1 = K.m + 1;
-            double* col = K.H + (int64_t)j * m1;
-            const double bnext = sqrt(tot);
-            for (int i = 0; i <= j; ++i) col[i] = K.hacc[i];
-            col[j + 1] = bnext;
-            K.beta[j + 1] = bnext;
-            K.inv_beta[j + 1] = 1.0 / bnext;
-            for (int i = 0; i < j; ++i) {
-                const double a = col[i], bb = col[i + 1];
-                col[i] = K.cs[i] * a + K.sn[i] * bb;
-                col[i + 1] = -K.sn[i] * a + K.cs[i] * bb;
-            }
-            const double a = col[j], bb = col[j + 1];
-            const double rr = hypot(a, bb);
-            double c = 1.0, sgn = 0.0;
-            if (rr > 0.0) {
-                c = a / rr;
-                sgn = bb / rr;
-            }
-            K.cs[j] = c;
-            K.sn[j] = sgn;
-            col[j] = rr;
-            col[j + 1] = 0.0;
-            const double gj = K.g[j];
-            K.g[j] = c * gj;
-            K.g[j + 1] = -sgn * gj;
-            const double est = fabs(K.g[j + 1]);
-            DevStatus* st = K.st;
-            st->steps = j + 1;
-            st->total_steps += 1;
-            st->resid_est = est;
-            const bool fin = isfinite(est) && isfinite(bnext) && isfinite(rr);
-            if (!fin) st->nonfinite = 1;
-            const double floor_abs = K.scal[1] * st->beta0;
-            const bool stop = !fin || rr == 0.0 || bnext == 0.0 || est <= K.scal[0] || est <= floor_abs || j + 1 >= K.m;
-            if (stop) st->done = 1;
+            finish_column(K, j, tot);
         }
     }
 }

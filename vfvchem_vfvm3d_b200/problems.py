@@ -37,13 +37,10 @@ class HeatProblem:
         return self.mesh.n_tot
 
 
-def steady_heat(n: int, hetero: bool = False, mesh_seed: int = 42, field_seed: int = 7, flux_top: float = 0.0,
-                prod: float = 0.0) -> HeatProblem:
-    mesh = Mesh.jitter_cube(n, mesh_seed, 0.25)
-    N = mesh.n_tot
-    _, nb, _ = mesh.export()
-    node_bnd = np.full(N, -1, np.int32)
-    node_bnd[mesh.n_pts:] = nb
+def heat_fields(node_bnd: np.ndarray, hetero: bool = False, field_seed: int = 7, flux_top: float = 0.0, prod: float = 0.0):
+    """(k, q, s, T0, bc_val) of the cube heat problem for a vertex set with boundary ids node_bnd
+    (-1 for points); numpy only."""
+    N = node_bnd.size
     if hetero:
         rng = np.random.default_rng(field_seed)
         k = np.exp(rng.standard_normal(N))
@@ -57,6 +54,17 @@ def steady_heat(n: int, hetero: bool = False, mesh_seed: int = 42, field_seed: i
     bc[node_bnd == 5] = flux_top     # optional outward flux on z = 1
     T0 = np.zeros(N)
     T0[node_bnd == 1] = 1.0           # initial_dirichlet (steady_base.rs:53-57)
+    return k, q, s, T0, bc
+
+
+def steady_heat(n: int, hetero: bool = False, mesh_seed: int = 42, field_seed: int = 7, flux_top: float = 0.0,
+                prod: float = 0.0) -> HeatProblem:
+    mesh = Mesh.jitter_cube(n, mesh_seed, 0.25)
+    N = mesh.n_tot
+    _, nb, _ = mesh.export()
+    node_bnd = np.full(N, -1, np.int32)
+    node_bnd[mesh.n_pts:] = nb
+    k, q, s, T0, bc = heat_fields(node_bnd, hetero, field_seed, flux_top, prod)
     return HeatProblem(mesh, k, q, s, T0, bc, node_bnd)
 
 
