@@ -162,7 +162,10 @@ int vfv_ilu0_ordering(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int32_t* perm
 
 /* ---- mesh (host, once per mesh): jittered unit cube, Delaunay, Voronoi dual */
 int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out);
-/* a mesh from given vertices (points first, then nodes with a boundary id each) */
+/* a mesh from given vertices (points first, then nodes with a boundary id each). The Delaunay
+ * predicates are exact integer arithmetic on the 2^-18 lattice: every coordinate must be a finite
+ * multiple of 2^-18 and the bounding box at most 1.75 on each axis (scale the domain into it);
+ * other input is refused with VFV_BAD_INPUT rather than rounded. */
 int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out);
 void vfv_mesh_destroy(vfv_mesh* m);
 /* count meshes at once (built in parallel on the host): out[i] = jitter cube of n[i]^3 points, seeds[i] */

@@ -63,6 +63,16 @@ def test_mesh_rejects_bad_input(lib_built):
     pos = np.zeros((4, 3))
     with pytest.raises(VFVChemError):  # coincident vertices
         Mesh.from_vertices(pos, 0, np.zeros(4, np.int32))
+    ref = Mesh.jitter_cube(4, 5, 0.25)
+    vpos, vbnd, _ = ref.export()
+    m = Mesh.from_vertices(vpos, ref.n_pts, vbnd)  # on the 2^-18 lattice, inside the exact range
+    assert m.n_tet == ref.n_tet
+    off = vpos.copy()
+    off[0, 0] += 2.0 ** -20  # an interior point between lattice points: refused, not rounded
+    with pytest.raises(VFVChemError, match="multiples of 2"):
+        Mesh.from_vertices(off, ref.n_pts, vbnd)
+    with pytest.raises(VFVChemError, match="bounding box"):  # the exact integer predicates would overflow
+        Mesh.from_vertices(vpos * 2.0, ref.n_pts, vbnd)
 
 
 def test_linear_gmres_constructor_checks():
