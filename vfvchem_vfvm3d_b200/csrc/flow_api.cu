@@ -22,6 +22,7 @@ struct vfv_flow {
     DBuf<int32_t> np, ni, bp, bj, bk, gcp, gcv, div_off, pst_off, sub_off, slot_loc;
     DBuf<double> dist, area, norm, skew, gw, cvol, cskew, barea, bnorm, bw, gcc;
     DBuf<double> den, visc, fce, bc_vel, gfix, gvel, rc, mom, flux, tv, b, x, xu;
+    DBuf<double> xo, rpart;  // previous Picard state and the partials of its scaled change (device)
     DBuf<int64_t> trip_ptr, slot_ptr;
     vfv_pattern* pat = nullptr;
     ~vfv_flow() {
@@ -87,40 +88,119 @@ __global__ void k_damp(int64_t n, double damp, double* __restrict__ x, const dou
     if (i < n) x[i] = (1.0 - damp) * x[i] + damp * xu[i];
 }
 
-// Picard change measure of scaled_residual (src/base/scaling.rs:113-136) for the pressure field
-// (scale: max(range p, rho_max |u|max^2), round-off dead band 1e-11 max|p|) and the velocity field
-// (scale: max |u|); the larger of the two. NaN if the new state is not finite.
-double flow_scaled_residual(int64_t n, double rho_max, const std::vector<double>& xo, const std::vector<double>& xn) {
-    for (double v : xn)
-        if (!std::isfinite(v)) return std::nan("");
-    const double floor_ = 1e-30;
-    double vmax = 0.0;
-    for (const std::vector<double>* x : {&xo, &xn})
-        for (int64_t i = 0; i < n; ++i) {
-            const double a = (*x)[i], b = (*x)[n + i], c = (*x)[2 * n + i];
-            vmax = std::max(vmax, std::sqrt(a * a + b * b + c * c));
+// Picard change measure of scaled_residual (src/base/scaling.rs:113-136), on the device: for the
+// pressure field the scale is max(range p, rho_max |u|max^2) with a round-off dead band of
+// 1e-11 max|p|, for the velocity field max |u| (ranges and maxima over the old and the new state);
+// the measure is the larger of the two RMS changes over their scales, NaN if the new state is not
+// finite. Four small kernels: per-block extrema, their reduction, per-block sums of squared
+// changes, their reduction into out[0]. Extrema are exact in any order; the sums are summed in a
+// fixed block order.
+constexpr int kResBlocks = 296;  // two per SM
+struct ResPart { double vmax, pmin, pmax, pabs, sp, sv; int32_t nonfinite, pad; };
+
+__global__ void __launch_bounds__(256) k_res_extrema(int64_t n, const double* __restrict__ xo, const double* __restrict__ xn,
+                                                    ResPart* part) {
+    __shared__ double sv[4][8];
+    __shared__ int snf;
+    if (threadIdx.x == 0) snf = 0;
+    __syncthreads();
+    double vmax = 0.0, pmin = 1e308, pmax = -1e308, pabs = 0.0;
+    int nf = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int st = 0; st < 2; ++st) {
+            const double* x = st ? xn : xo;
+            const double a = x[i], b = x[n + i], c = x[2 * n + i], p = x[3 * n + i];
+            vmax = fmax(vmax, sqrt(a * a + b * b + c * c));
+            pmin = fmin(pmin, p);
+            pmax = fmax(pmax, p);
+            pabs = fmax(pabs, fabs(p));
+            if (st && !(isfinite(a) && isfinite(b) && isfinite(c) && isfinite(p))) nf = 1;
         }
-    double pmin = 1e308, pmax = -1e308, pabs = 0.0;
-    for (const std::vector<double>* x : {&xo, &xn})
-        for (int64_t i = 3 * n; i < 4 * n; ++i) {
-            pmin = std::min(pmin, (*x)[i]);
-            pmax = std::max(pmax, (*x)[i]);
-            pabs = std::max(pabs, std::fabs((*x)[i]));
+    }
+    if (nf) snf = 1;
+    for (int o = 16; o > 0; o >>= 1) {
+        vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        pmin = fmin(pmin, __shfl_xor_sync(0xffffffffu, pmin, o));
+        pmax = fmax(pmax, __shfl_xor_sync(0xffffffffu, pmax, o));
+        pabs = fmax(pabs, __shfl_xor_sync(0xffffffffu, pabs, o));
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        sv[0][wid] = vmax;
+        sv[1][wid] = pmin;
+        sv[2][wid] = pmax;
+        sv[3][wid] = pabs;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ResPart r{};
+        r.vmax = sv[0][0];
+        r.pmin = sv[1][0];
+        r.pmax = sv[2][0];
+        r.pabs = sv[3][0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            r.vmax = fmax(r.vmax, sv[0][w]);
+            r.pmin = fmin(r.pmin, sv[1][w]);
+            r.pmax = fmax(r.pmax, sv[2][w]);
+            r.pabs = fmax(r.pabs, sv[3][w]);
         }
-    const double dead = 1e-11 * pabs;
+        r.nonfinite = snf;
+        part[blockIdx.x] = r;
+    }
+}
+
+// part[nb] <- the reduced extrema (one thread)
+__global__ void k_res_extrema_finish(int nb, ResPart* part) {
+    ResPart g = part[0];
+    for (int b = 1; b < nb; ++b) {
+        const ResPart& r = part[b];
+        g.vmax = fmax(g.vmax, r.vmax);
+        g.pmin = fmin(g.pmin, r.pmin);
+        g.pmax = fmax(g.pmax, r.pmax);
+        g.pabs = fmax(g.pabs, r.pabs);
+        g.nonfinite |= r.nonfinite;
+    }
+    part[nb] = g;
+}
+
+__global__ void __launch_bounds__(256) k_res_sums(int64_t n, const double* __restrict__ xo, const double* __restrict__ xn, ResPart* part,
+                                                 int nb) {
+    __shared__ double red[8];
+    const double dead = 1e-11 * part[nb].pabs;
     double sp = 0.0, sv = 0.0;
-    for (int64_t i = 3 * n; i < 4 * n; ++i) {
-        const double d = std::max(std::fabs(xn[i] - xo[i]) - dead, 0.0);
-        sp += d * d;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double dp = fmax(fabs(xn[3 * n + i] - xo[3 * n + i]) - dead, 0.0);
+        sp += dp * dp;
+        for (int c = 0; c < 3; ++c) {
+            const double d = fabs(xn[c * n + i] - xo[c * n + i]);
+            sv += d * d;
+        }
     }
-    for (int64_t i = 0; i < 3 * n; ++i) {
-        const double d = std::fabs(xn[i] - xo[i]);
-        sv += d * d;
+    sp = block_sum(sp, red);
+    __syncthreads();
+    sv = block_sum(sv, red);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x].sp = sp;
+        part[blockIdx.x].sv = sv;
     }
-    const double nn = (double)std::max<int64_t>(n, 1);
-    const double rp = std::sqrt(sp / nn) / std::max(std::max(pmax - pmin, rho_max * vmax * vmax), floor_);
-    const double rv = std::sqrt(sv / nn) / std::max(vmax, floor_);
-    return std::max(rp, rv);
+}
+
+__global__ void k_res_finish(int64_t n, int nb, double rho_max, const ResPart* part, double* out) {
+    const ResPart g = part[nb];
+    double sp = 0.0, sv = 0.0;
+    for (int b = 0; b < nb; ++b) {
+        sp += part[b].sp;
+        sv += part[b].sv;
+    }
+    if (g.nonfinite) {
+        out[0] = nan("");
+        return;
+    }
+    const double floor_ = 1e-30;
+    const double nn = (double)(n > 1 ? n : 1);
+    const double rp = sqrt(sp / nn) / fmax(fmax(g.pmax - g.pmin, rho_max * g.vmax * g.vmax), floor_);
+    const double rv = sqrt(sv / nn) / fmax(g.vmax, floor_);
+    out[0] = fmax(rp, rv);
 }
 
 int flow_assemble(vfv_ctx* ctx, vfv_flow* f, const double* xs) {
@@ -282,8 +362,14 @@ int vfv_flow_picard(vfv_ctx* ctx, vfv_flow* f, double* x, int max_iter, double t
     if (rc) return rc;
     cudaStream_t s = ctx->stream;
     const int64_t N4 = 4 * f->n;
+    if (!f->xo.p) {
+        CK(f->xo.alloc(N4));
+        CK(f->rpart.alloc(sizeof(ResPart) / sizeof(double) * (kResBlocks + 1) + 1));
+    }
     CK(cudaMemcpyAsync(f->x.p, x, N4 * sizeof(double), cudaMemcpyHostToDevice, s));
-    std::vector<double> xo(x, x + N4), xn(N4);
+    CK(cudaMemcpyAsync(f->xo.p, f->x.p, N4 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ResPart* rpart = reinterpret_cast<ResPart*>(f->rpart.p);
+    double* rout = f->rpart.p + sizeof(ResPart) / sizeof(double) * (kResBlocks + 1);
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -303,12 +389,16 @@ int vfv_flow_picard(vfv_ctx* ctx, vfv_flow* f, double* x, int max_iter, double t
         if (lin_iters) lin_iters[it] = info.iters;
         if (rc) break;
         k_damp<<<grid_for(N4), 256, 0, s>>>(N4, damp, f->x.p, f->xu.p);
-        ctx->launches += 1;
-        CK(cudaMemcpyAsync(xn.data(), f->x.p, N4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        k_res_extrema<<<kResBlocks, 256, 0, s>>>(f->n, f->xo.p, f->x.p, rpart);
+        k_res_extrema_finish<<<1, 1, 0, s>>>(kResBlocks, rpart);
+        k_res_sums<<<kResBlocks, 256, 0, s>>>(f->n, f->xo.p, f->x.p, rpart, kResBlocks);
+        k_res_finish<<<1, 1, 0, s>>>(f->n, kResBlocks, f->rho_max, rpart, rout);
+        CK(cudaMemcpyAsync(f->xo.p, f->x.p, N4 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        ctx->launches += 5;
+        CK(cudaMemcpyAsync(ctx->h_scalar, rout, sizeof(double), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        const double r = flow_scaled_residual(f->n, f->rho_max, xo, xn);
+        const double r = ctx->h_scalar[0];
         if (res) res[it] = r;
-        xo.swap(xn);
         if (!std::isfinite(r)) {
             rc = set_err(ctx, VFV_NONFINITE, "Picard: non-finite residual (SteadyNonFiniteResidual)");
             ++it;
@@ -318,7 +408,8 @@ int vfv_flow_picard(vfv_ctx* ctx, vfv_flow* f, double* x, int max_iter, double t
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    std::copy(xo.begin(), xo.end(), x);
+    CK(cudaMemcpyAsync(x, f->x.p, N4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     if (iters_done) *iters_done = it;
     if (solve_seconds) *solve_seconds = tsolve;
     if (rc) return rc;
