@@ -133,11 +133,14 @@ int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double*
 /* y = A x with float values/vectors (the mixed-precision inner SpMV); the float copy of the
  * values is made on first use and refreshed by every vfv_values_* call */
 int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y);
-/* Autotuner: measures the pattern's SpMV with 2, 4, 8, 16 and 32 lanes per row (double and float values)
- * and keeps the fastest for every later SpMV and solver of this pattern; call before its first
- * solve. Returns the chosen lanes (either pointer may be NULL). */
+/* Autotuner: measures the pattern's SpMV in each of its shapes (2 to 32 lanes per row, 1 to 8 strides
+ * of indices and values loaded per lane before the gathers; double and float values) and keeps the
+ * fastest for every later SpMV and solver of this pattern; call before its first solve. Returns the
+ * chosen lanes (either pointer may be NULL). */
 int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t* lanes32);
-/* Sets the SpMV lanes per row by hand (2, 4, 8, 16 or 32 each); VFV_BAD_INPUT otherwise. */
+/* the SpMV shape in use: lanes per row and strides per lane, double and float (pointers may be NULL) */
+int vfv_pattern_spmv_shape(const vfv_pattern* p, int32_t* lanes64, int32_t* strides64, int32_t* lanes32, int32_t* strides32);
+/* Sets the SpMV lanes per row by hand (2, 4, 8, 16 or 32 each, 4 strides per lane); VFV_BAD_INPUT otherwise. */
 int vfv_pattern_set_spmv_lanes(vfv_ctx* ctx, vfv_pattern* p, int32_t lanes64, int32_t lanes32);
 /* z = M^-1 r for the ILU(0) preconditioner of the pattern's current values (device arrays, double) */
 int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels);

@@ -77,6 +77,7 @@ SIGNATURES = [
     ("vfv_ilu0_apply_device_f32", C.c_int, [_P, _P, C.c_int, _P, _P, _P, _I32P]),
     ("vfv_pattern_autotune", C.c_int, [_P, _P, _I32P, _I32P]),
     ("vfv_pattern_set_spmv_lanes", C.c_int, [_P, _P, C.c_int32, C.c_int32]),
+    ("vfv_pattern_spmv_shape", C.c_int, [_P, _I32P, _I32P, _I32P, _I32P]),
     ("vfv_ilu0_ordering", C.c_int, [_P, _P, C.c_int, _I32P, _I32P, _I32P]),
     ("vfv_ilu0_apply_device_noalloc", C.c_int, [_P, _P, C.c_int, _P, _P, _I32P]),
     ("vfv_mesh_jitter_cube", C.c_int, [C.c_int, C.c_uint64, C.c_double, _PP]),

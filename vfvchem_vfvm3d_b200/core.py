@@ -209,6 +209,12 @@ class Pattern:
         _check(self.ctx.handle, L.load().vfv_pattern_autotune(self.ctx.handle, self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def spmv_shape(self):
+        """((lanes, strides) double, (lanes, strides) float) of the SpMV in use."""
+        a, b, c, d = (C.c_int32() for _ in range(4))
+        _check(self.ctx.handle, L.load().vfv_pattern_spmv_shape(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return (a.value, b.value), (c.value, d.value)
+
     def set_spmv_lanes(self, lanes64: int, lanes32: int) -> None:
         _check(self.ctx.handle, L.load().vfv_pattern_set_spmv_lanes(self.ctx.handle, self._h, int(lanes64), int(lanes32)))
 

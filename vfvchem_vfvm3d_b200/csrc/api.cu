@@ -13,7 +13,6 @@
 #include "kernels/gmres_cycle.cuh"
 #include "kernels/krylov.cuh"
 #include "kernels/krylov_batch.cuh"
-#include "kernels/krylov_staged.cuh"
 #include "kernels/ns.cuh"
 #include "host/ns_setup.hpp"
 #include "host/sort.hpp"
@@ -42,47 +41,44 @@ std::string& vfv_thread_error() {
 // ================================================================ GMRES driver
 namespace {
 
-// SpMV with the lanes-per-row the pattern was tuned for (2, 4, 8, 16 or 32)
+// SpMV shapes: G lanes per row, each lane loading its first S strides of the row (indices and
+// values) before any gather. The autotuner picks one per pattern and precision; (G, 4) exists for
+// every G (the shape vfv_pattern_set_spmv_lanes selects).
+#define VFV_SPMV_SHAPES(X) X(2, 4) X(2, 8) X(4, 4) X(4, 6) X(4, 8) X(8, 2) X(8, 3) X(8, 4) X(16, 1) X(16, 2) X(16, 4) X(32, 1) X(32, 4)
+constexpr int kSpmvShapes[][2] = {
+#define VFV_SHAPE_ENTRY(G, S) {G, S},
+    VFV_SPMV_SHAPES(VFV_SHAPE_ENTRY)
+#undef VFV_SHAPE_ENTRY
+};
+
 template <typename TV, typename TX, typename TY, typename TA>
-void launch_spmv(cudaStream_t s, int lanes, int64_t n, const int32_t* rp, const int32_t* ci, const TV* val, const TX* x, TY* y,
-                 const double* scale, const DevStatus* st) {
-    switch (lanes) {
-        case 2:
-            k_spmv<TV, TX, TY, TA, 2><<<grid_for(n * 2), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
-            break;
-        case 8:
-            k_spmv<TV, TX, TY, TA, 8><<<grid_for(n * 8), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
-            break;
-        case 16:
-            k_spmv<TV, TX, TY, TA, 16><<<grid_for(n * 16), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
-            break;
-        case 32:
-            k_spmv<TV, TX, TY, TA, 32><<<grid_for(n * 32), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
-            break;
+void launch_spmv(cudaStream_t s, int lanes, int strides, int64_t n, const int32_t* rp, const int32_t* ci, const TV* val, const TX* x,
+                 TY* y, const double* scale, const DevStatus* st) {
+    switch (lanes * 16 + strides) {
+#define VFV_SHAPE_CASE(G, S)                                                                                  \
+    case G * 16 + S:                                                                                          \
+        k_spmv<TV, TX, TY, TA, G, S><<<grid_for(n * G), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);         \
+        return;
+        VFV_SPMV_SHAPES(VFV_SHAPE_CASE)
+#undef VFV_SHAPE_CASE
         default:
-            k_spmv<TV, TX, TY, TA, 4><<<grid_for(n * 4), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
+            k_spmv<TV, TX, TY, TA, 4, 4><<<grid_for(n * 4), kBlk, 0, s>>>(n, rp, ci, val, x, y, scale, st);
     }
 }
 
 // SpMV of a batched solve: the step's scale 1/beta_j looked up per row from its mesh
 template <typename TV, typename TX, typename TY, typename TA>
-void launch_spmv_seg(cudaStream_t s, int lanes, int64_t n, const int32_t* rp, const int32_t* ci, const TV* val, const TX* x, TY* y,
-                     const double* inv_beta, int stride, int j, const int64_t* mesh_row, int nm, const DevStatus* st) {
-    switch (lanes) {
-        case 2:
-            k_spmv_seg<TV, TX, TY, TA, 2><<<grid_for(n * 2), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
-            break;
-        case 8:
-            k_spmv_seg<TV, TX, TY, TA, 8><<<grid_for(n * 8), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
-            break;
-        case 16:
-            k_spmv_seg<TV, TX, TY, TA, 16><<<grid_for(n * 16), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
-            break;
-        case 32:
-            k_spmv_seg<TV, TX, TY, TA, 32><<<grid_for(n * 32), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
-            break;
+void launch_spmv_seg(cudaStream_t s, int lanes, int strides, int64_t n, const int32_t* rp, const int32_t* ci, const TV* val, const TX* x,
+                     TY* y, const double* inv_beta, int stride, int j, const int64_t* mesh_row, int nm, const DevStatus* st) {
+    switch (lanes * 16 + strides) {
+#define VFV_SHAPE_CASE(G, S)                                                                                                         \
+    case G * 16 + S:                                                                                                                 \
+        k_spmv_seg<TV, TX, TY, TA, G, S><<<grid_for(n * G), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st); \
+        return;
+        VFV_SPMV_SHAPES(VFV_SHAPE_CASE)
+#undef VFV_SHAPE_CASE
         default:
-            k_spmv_seg<TV, TX, TY, TA, 4><<<grid_for(n * 4), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
+            k_spmv_seg<TV, TX, TY, TA, 4, 4><<<grid_for(n * 4), kBlk, 0, s>>>(n, rp, ci, val, x, y, inv_beta, stride, j, mesh_row, nm, st);
     }
 }
 
@@ -419,37 +415,44 @@ constexpr int chain_slot() {
     return std::is_same<T, double>::value ? 0 : 1;
 }
 
-// Work vectors refilled with the sentinel, claim/parity state cleared, poll limit set: the state
-// of a fresh chain (at set-up, and after a wait gave up, which leaves it undefined).
+// Claim counter, completion counters and abort flag cleared, poll limit set: the state of a fresh
+// chain (at set-up, and after a wait gave up, which leaves it undefined).
 template <typename T>
-int chain_reset(vfv_ctx* ctx, IluStruct& S, int64_t n, long long polls) {
+int chain_reset(vfv_ctx* ctx, IluStruct& S, long long polls) {
     IluStruct::Chain& C = S.chain[chain_slot<T>()];
     cudaStream_t s = ctx->stream;
     IluChainState h{};
     h.poll_limit = polls > 0 ? polls : kDefaultWaitPolls;
-    CK(cudaMemsetAsync(C.work.p, 0xFF, C.work.n, s));
+    CK(cudaMemsetAsync(C.state.p, 0, C.state.n, s));
     CK(cudaMemcpyAsync(C.state.p, &h, sizeof(h), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
     *C.h_flag = 0;
     return VFV_OK;
 }
 
-// Task table (row ranges of at most kChainThreads rows inside one level) and the chain state of
-// precision T; once per ILU structure and precision.
+// Task table (row ranges of at most kChainThreads rows inside one level, their levels, tasks per
+// level) and the chain state of precision T, with a work vector of n entries for standalone
+// applies; once per ILU structure and precision.
 template <typename T>
 int chain_setup(vfv_ctx* ctx, IluStruct& S, int64_t n) {
     IluStruct::Chain& C = S.chain[chain_slot<T>()];
     if (C.grid > 0) return VFV_OK;
     if (!S.tasks.p) {
-        std::vector<int32_t> tk;
+        std::vector<int32_t> tk, tl, ln(S.nlev, 0);
         for (int l = 0; l < S.nlev; ++l)
-            for (int32_t r = S.lev_ptr[l]; r < S.lev_ptr[l + 1]; r += kChainThreads) tk.push_back(r);
+            for (int32_t r = S.lev_ptr[l]; r < S.lev_ptr[l + 1]; r += kChainThreads) {
+                tk.push_back(r);
+                tl.push_back(l);
+                ln[l]++;
+            }
         tk.push_back(S.lev_ptr[S.nlev]);
-        S.ntask = (int)tk.size() - 1;
+        S.ntask = (int)tl.size();
         CK(S.tasks.upload(tk.data(), tk.size(), ctx->stream));
+        CK(S.task_lev.upload(tl.data(), tl.size(), ctx->stream));
+        CK(S.lev_ntask.upload(ln.data(), ln.size(), ctx->stream));
     }
-    CK(C.work.alloc((size_t)4 * n * sizeof(T)));
-    CK(C.state.alloc(sizeof(IluChainState)));
+    CK(C.work.alloc((size_t)n * sizeof(T)));
+    CK(C.state.alloc(sizeof(IluChainState) + 2 * (size_t)S.nlev * sizeof(unsigned)));
     CK(cudaHostAlloc((void**)&C.h_flag, sizeof(int), cudaHostAllocMapped));
     *C.h_flag = 0;
     CK(cudaHostGetDevicePointer((void**)&C.d_flag, C.h_flag, 0));
@@ -457,7 +460,7 @@ int chain_setup(vfv_ctx* ctx, IluStruct& S, int64_t n) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu0_chain<T>, kChainThreads, 0));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     C.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * sms, 2 * (int64_t)S.ntask));
-    return chain_reset<T>(ctx, S, n, 0);
+    return chain_reset<T>(ctx, S, 0);
 }
 
 // poll limit of the chain's bounded waits for the launches that follow (enqueued on the stream)
@@ -469,10 +472,11 @@ int chain_set_polls(vfv_ctx* ctx, IluStruct& S, long long polls) {
     return VFV_OK;
 }
 
-// z = (LU)^-1 r in one launch (k_ilu0_chain). `timeout_flag` receives 1 if a bounded wait gave up.
+// z = (LU)^-1 r in one launch (k_ilu0_chain); t is a work vector of n entries that aliases neither
+// r nor z. `timeout_flag` receives 1 if a bounded wait gave up.
 template <typename T>
-cudaError_t ilu_apply_chain(cudaStream_t s, IluStruct& S, int64_t n, const T* lu, const T* in, T* out, const DevStatus* st,
-                            int* timeout_flag, int prio = 0, bool use_prio = false) {
+cudaError_t ilu_apply_chain(cudaStream_t s, IluStruct& S, const T* lu, const T* in, T* t, T* out, const DevStatus* st, int* timeout_flag,
+                            int prio = 0, bool use_prio = false) {
     IluStruct::Chain& C = S.chain[chain_slot<T>()];
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)C.grid);
@@ -485,10 +489,10 @@ cudaError_t ilu_apply_chain(cudaStream_t s, IluStruct& S, int64_t n, const T* lu
         cfg.attrs = attr;
         cfg.numAttrs = 1;
     }
-    using U = typename ChainWord<T>::U;
-    return cudaLaunchKernelEx(&cfg, k_ilu0_chain<T>, (int32_t)S.ntask, (const int32_t*)S.tasks.p, (const int32_t*)S.rp.p,
-                              (const int32_t*)S.ci.p, (const int32_t*)S.dg.p, lu, (const int32_t*)S.perm.p, n, in, out,
-                              reinterpret_cast<U*>(C.work.p), reinterpret_cast<IluChainState*>(C.state.p), timeout_flag, st);
+    return cudaLaunchKernelEx(&cfg, k_ilu0_chain<T>, (int32_t)S.ntask, (int32_t)S.nlev, (const int32_t*)S.tasks.p,
+                              (const int32_t*)S.task_lev.p, (const int32_t*)S.lev_ntask.p, (const int32_t*)S.rp.p, (const int32_t*)S.ci.p,
+                              (const int32_t*)S.dg.p, lu, (const int32_t*)S.perm.p, in, t, out,
+                              reinterpret_cast<IluChainState*>(C.state.p), timeout_flag, st);
 }
 
 constexpr int kStepsPerIf = 4;  // Arnoldi steps per IF node of a cycle graph
@@ -501,8 +505,7 @@ struct Gmres : SolverBase {
     int64_t n = 0, ldv = 0;
     int m = 0, precond = 0, ilu_order = 0, engine = 0;
     int nblk = 0, mega_grid = 0, mega_chunk = 0;
-    int nblk_v = 0;       // blocks of the register multi-vector kernels (kBlk * kRows rows each)
-    bool staged = true;   // Gram-Schmidt passes with the basis tile in shared memory (kStR-row tiles)
+    int nblk_v = 0;       // blocks of the multi-vector kernels (kBlk * kRows rows each)
     DBuf<T> V, z, z2, zc, valK;
     DBuf<unsigned> bar;
     DBuf<unsigned long long> trace;  // per-phase timestamps of the last cycle (VFV_TRACE_CYCLE=1)
@@ -550,18 +553,8 @@ struct Gmres : SolverBase {
         ilu_order = ilu_order_;
         engine = engine_;
         ldv = (n + 63) / 64 * 64;
-        if (const char* e = getenv("VFV_ORTHO_REGS")) staged = e[0] != '1';
         nblk_v = (int)((n + kBlk * kRows - 1) / (kBlk * kRows));
-        nblk = staged ? (int)((n + kStR - 1) / kStR) : nblk_v;  // partial dots per vector
-        if (staged) {
-            const int smax = (m + 1) * kStR * (int)sizeof(T);
-            CK(cudaFuncSetAttribute(k_mdot_s<T, SingleMap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-            CK(cudaFuncSetAttribute(k_update_s<T, SingleMap, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-            CK(cudaFuncSetAttribute(k_update_s<T, SingleMap, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-            CK(cudaFuncSetAttribute(k_mdot_s<T, BatchMap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-            CK(cudaFuncSetAttribute(k_update_s<T, BatchMap, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-            CK(cudaFuncSetAttribute(k_update_s<T, BatchMap, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-        }
+        nblk = nblk_v;  // partial dots per vector
         const int64_t res_blocks = (n * kSpG + kBlk - 1) / kBlk;
         CK(V.alloc((size_t)(m + 1) * ldv));
         CK(cudaMemset(V.p, 0, sizeof(T) * (size_t)(m + 1) * ldv));
@@ -672,7 +665,7 @@ struct Gmres : SolverBase {
         nm = (int)rows.size() - 1;
         std::vector<int64_t> tr, rr;
         std::vector<int32_t> tm, mt(nm + 1), rm, mr(nm + 1);
-        const int64_t tv = staged ? (int64_t)kStR : (int64_t)kBlk * kRows, tres = kBlk / kSpG;
+        const int64_t tv = (int64_t)kBlk * kRows, tres = kBlk / kSpG;
         for (int q = 0; q < nm; ++q) {
             mt[q] = (int32_t)tm.size();
             mr[q] = (int32_t)rm.size();
@@ -747,7 +740,7 @@ struct Gmres : SolverBase {
     // z = M^-1 r for the ILU(0) preconditioner; `in` and `out` may alias. st: early exit once the
     // solve is done (null: always run).
     void apply_ilu(cudaStream_t s, const T* in, T* out, const DevStatus* stp, int prio = 0, bool use_prio = false) {
-        if (ilu_chain) ilu_apply_chain<T>(s, *ilu, n, lu_vals(), in, out, stp, &st.p->timeout, prio, use_prio);
+        if (ilu_chain) ilu_apply_chain<T>(s, *ilu, lu_vals(), in, z2.p, out, stp, &st.p->timeout, prio, use_prio);
         else ilu_apply_levels<T>(s, *ilu, lu_vals(), in, z2.p, out, stp, prio, use_prio);
     }
 
@@ -768,16 +761,6 @@ struct Gmres : SolverBase {
     // may be the same vector): first-pass dots, update + second-pass dots, update + norm + Givens.
     void enqueue_ortho(cudaStream_t s, const T* win, T* w, int j) {
         const int nv = j + 1, fb = grid_for((int64_t)nv * 32);
-        if (staged) {
-            const SingleMap M{n, st.p};
-            const size_t sm = (size_t)nv * kStR * sizeof(T);
-            k_mdot_s<T, SingleMap><<<nblk, kStR, sm, s>>>(M, V.p, ldv, win, nv, part.p, nblk);
-            k_dots_finish<true><<<fb, 256, 0, s>>>(K, nv);
-            k_update_s<T, SingleMap, false, false><<<nblk, kStR, sm, s>>>(M, K, V.p, ldv, win, w, nv, coef.p, part.p, nblk, j);
-            k_dots_finish<false><<<fb, 256, 0, s>>>(K, nv);
-            k_update_s<T, SingleMap, true, true><<<nblk, kStR, sm, s>>>(M, K, V.p, ldv, w, w, nv, coef.p, part.p, nblk, j);
-            return;
-        }
         k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, win, nv);
         k_dots_finish<true><<<fb, 256, 0, s>>>(K, nv);
         k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, win, w, nv, j);
@@ -828,15 +811,15 @@ struct Gmres : SolverBase {
             in = z.p;
         }
         cudaEventRecord(ev[1], s);
-        launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
+        launch_spmv<T, T, T, T>(s, p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], p->spmv_strides[sizeof(T) == 8 ? 0 : 1], n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
         cudaEventRecord(ev[2], s);
         enqueue_ortho(s, w, w, j);
         cudaEventRecord(ev[3], s);
         cudaEventSynchronize(ev[3]);
         float t[3];
         for (int q = 0; q < 3; ++q) cudaEventElapsedTime(&t[q], ev[q], ev[q + 1]);
-        fprintf(stderr, "[vfv step profile] %s j=%d (us): ilu %.1f spmv %.1f cgs2 passes %.1f (%s)\n", sizeof(T) == 4 ? "fp32" : "fp64",
-                j, t[0] * 1e3, t[1] * 1e3, t[2] * 1e3, staged ? "staged tiles" : "register tiles");
+        fprintf(stderr, "[vfv step profile] %s j=%d (us): ilu %.1f spmv %.1f cgs2 passes %.1f\n", sizeof(T) == 4 ? "fp32" : "fp64", j,
+                t[0] * 1e3, t[1] * 1e3, t[2] * 1e3);
         for (auto& e : ev) cudaEventDestroy(e);
     }
 
@@ -896,7 +879,7 @@ struct Gmres : SolverBase {
 
     void enqueue_step(cudaStream_t s, vfv_pattern* p, int j) {
         const T* vk = krylov_vals(p);
-        const int lanes = p->spmv_lanes[sizeof(T) == 8 ? 0 : 1];
+        const int lanes = p->spmv_lanes[sizeof(T) == 8 ? 0 : 1], strides = p->spmv_strides[sizeof(T) == 8 ? 0 : 1];
         T* w = V.p + (int64_t)(j + 1) * ldv;
         if (nm > 0) {  // one recurrence per mesh of a batch
             const T* uj = V.p + (int64_t)j * ldv;
@@ -905,19 +888,8 @@ struct Gmres : SolverBase {
                 apply_ilu(s, uj, z.p, st.p);
                 in = z.p;
             }
-            launch_spmv_seg<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, in, w, b_inv_beta.p, m + 1, j, b_mesh_row.p, nm, st.p);
+            launch_spmv_seg<T, T, T, T>(s, lanes, strides, n, p->rp.p, p->ci.p, vk, in, w, b_inv_beta.p, m + 1, j, b_mesh_row.p, nm, st.p);
             const int nv = j + 1, fb = grid_for((int64_t)nm * nv * 32);
-            if (staged) {
-                const BatchMap M{b_tile_row.p, b_tile_mesh.p, b_ms.p, st.p};
-                const size_t sm = (size_t)nv * kStR * sizeof(T);
-                k_mdot_s<T, BatchMap><<<B.ntile, kStR, sm, s>>>(M, V.p, ldv, w, nv, b_part.p, B.ntile);
-                k_bdots_finish<true><<<fb, 256, 0, s>>>(B, nv);
-                k_update_s<T, BatchMap, false, false><<<B.ntile, kStR, sm, s>>>(M, K, V.p, ldv, w, w, nv, b_coef.p, b_part.p, B.ntile, j);
-                k_bdots_finish<false><<<fb, 256, 0, s>>>(B, nv);
-                k_update_s<T, BatchMap, true, false><<<B.ntile, kStR, sm, s>>>(M, K, V.p, ldv, w, w, nv, b_coef.p, b_part.p, B.ntile, j);
-                k_bstep_finish<<<nm, kStR, 0, s>>>(B, j);  // reduces the tile norms like the last block of k_update_s
-                return;
-            }
             k_bmdot<T><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, nv);
             k_bdots_finish<true><<<fb, 256, 0, s>>>(B, nv);
             k_bupdate<T, false><<<B.ntile, kBlk, 0, s>>>(B, V.p, w, w, nv);
@@ -927,7 +899,7 @@ struct Gmres : SolverBase {
             return;
         }
         if (engine == VFV_ENGINE_OVERLAP) {
-            launch_spmv<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, Zb.p + (int64_t)j * ldv, abuf.p, inv_beta.p + j, st.p);
+            launch_spmv<T, T, T, T>(s, lanes, strides, n, p->rp.p, p->ci.p, vk, Zb.p + (int64_t)j * ldv, abuf.p, inv_beta.p + j, st.p);
             cudaEventRecord(ev_fork, s);
             cudaStreamWaitEvent(s2, ev_fork, 0);
             apply_ilu(s2, abuf.p, qbuf.p, st.p, ilu_prio, true);
@@ -946,7 +918,7 @@ struct Gmres : SolverBase {
             k_bj4_apply<T><<<grid_for(n / 4), 256, 0, s>>>(n / 4, bj_vals(), uj, z.p, st.p);
             in = z.p;
         }
-        launch_spmv<T, T, T, T>(s, lanes, n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
+        launch_spmv<T, T, T, T>(s, lanes, strides, n, p->rp.p, p->ci.p, vk, in, w, inv_beta.p + j, st.p);
         enqueue_ortho(s, w, w, j);
     }
 
@@ -1215,7 +1187,7 @@ struct Gmres : SolverBase {
                 if (bar.p) CK(cudaMemsetAsync(bar.p, 0, 2 * kGenOffset * sizeof(unsigned), s));
                 CK(cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s));
                 if (ilu && ilu_chain) {
-                    int rc2 = chain_reset<T>(ctx, *ilu, n, wait_polls);
+                    int rc2 = chain_reset<T>(ctx, *ilu, wait_polls);
                     if (rc2) return rc2;
                 }
                 break;
@@ -1612,7 +1584,7 @@ int vfv_solve(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
 
 int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double* y) {
     if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
-    launch_spmv<double, double, double, double>(ctx->stream, p->spmv_lanes[0], p->n, p->rp.p, p->ci.p, p->val.p, x, y, nullptr, nullptr);
+    launch_spmv<double, double, double, double>(ctx->stream, p->spmv_lanes[0], p->spmv_strides[0], p->n, p->rp.p, p->ci.p, p->val.p, x, y, nullptr, nullptr);
     ctx->launches += 1;
     CK(cudaGetLastError());
     return VFV_OK;
@@ -1625,7 +1597,7 @@ int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y) 
         k_cast<double, float><<<grid_for(p->nnz), 256, 0, ctx->stream>>>(p->nnz, p->val.p, p->val32.p);
         p->version32 = p->version;
     }
-    launch_spmv<float, float, float, float>(ctx->stream, p->spmv_lanes[1], p->n, p->rp.p, p->ci.p, p->val32.p, x, y, nullptr, nullptr);
+    launch_spmv<float, float, float, float>(ctx->stream, p->spmv_lanes[1], p->spmv_strides[1], p->n, p->rp.p, p->ci.p, p->val32.p, x, y, nullptr, nullptr);
     ctx->launches += 1;
     CK(cudaGetLastError());
     return VFV_OK;
@@ -1661,7 +1633,7 @@ int chain_check_flag(vfv_ctx* ctx, IluStruct& S, int64_t n) {
     IluStruct::Chain& C = S.chain[chain_slot<T>()];
     if (!*(volatile int*)C.h_flag) return VFV_OK;
     CK(cudaStreamSynchronize(ctx->stream));
-    int rc = chain_reset<T>(ctx, S, n, 0);
+    int rc = chain_reset<T>(ctx, S, 0);
     if (rc) return rc;
     return set_err(ctx, VFV_TIMEOUT, "ILU(0) sweeps: a bounded device wait gave up");
 }
@@ -1676,7 +1648,8 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
     if (rc) return rc;
     rc = chain_check_flag<double>(ctx, *S, p->n);
     if (rc) return rc;
-    CK(ilu_apply_chain<double>(ctx->stream, *S, p->n, S->lu64.p, r, z, nullptr, S->chain[0].d_flag));
+    CK(ilu_apply_chain<double>(ctx->stream, *S, S->lu64.p, r, reinterpret_cast<double*>(S->chain[0].work.p), z, nullptr,
+                               S->chain[0].d_flag));
     ctx->launches += 1;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
@@ -1689,7 +1662,7 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
 // z = M^-1 r with the float copy of the factor: the kernel the mixed-precision solver runs.
 // Enqueued on the context's stream with no synchronisation, so calls after the first (which builds
 // the factor and the sweep state) allocate nothing and can be timed back to back. A bounded wait
-// that gave up is reported by the next call on the pattern. t is unused (kept for the ABI).
+// that gave up is reported by the next call on the pattern.
 int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const float* r, float* t, float* z, int32_t* levels) {
     if (!ctx || !p || !r || !t || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (t == r || t == z) return set_err(ctx, VFV_BAD_INPUT, "the work vector aliases r or z");
@@ -1698,7 +1671,7 @@ int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const
     if (rc) return rc;
     rc = chain_check_flag<float>(ctx, *S, p->n);
     if (rc) return rc;
-    CK(ilu_apply_chain<float>(ctx->stream, *S, p->n, S->lu32.p, r, z, nullptr, S->chain[1].d_flag));
+    CK(ilu_apply_chain<float>(ctx->stream, *S, S->lu32.p, r, t, z, nullptr, S->chain[1].d_flag));
     ctx->launches += 1;
     CK(cudaGetLastError());
     if (levels) *levels = S->nlev;
@@ -1764,9 +1737,10 @@ int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, c
     return VFV_OK;
 }
 
-// Autotuner: times the SpMV of this pattern (its current values) with 2, 4, 8, 16 and 32 lanes per
-// row in double and in float (short rows of a scalar problem favour few lanes, the 2-ring rows of
-// the coupled flow system a warp per row), keeps the fastest of each for every later SpMV and solver of the pattern.
+// Autotuner: times the SpMV of this pattern (its current values) in every shape of kSpmvShapes
+// (2 to 32 lanes per row, 1 to 8 strides loaded per lane before the gathers) in double and in float
+// (short rows of a scalar problem favour few lanes, the 2-ring rows of the coupled flow system a
+// warp per row), keeps the fastest of each for every later SpMV and solver of the pattern.
 // Must run before the pattern's first solve (solvers capture their kernels once).
 int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t* lanes32) {
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
@@ -1785,35 +1759,48 @@ int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    const int cand[5] = {2, 4, 8, 16, 32};
+    const int nshape = (int)(sizeof(kSpmvShapes) / sizeof(kSpmvShapes[0]));
     for (int prec = 0; prec < 2; ++prec) {
         float best = 1e30f;
-        int best_g = kSpG;
-        for (int g : cand) {
-            auto run = [&] {
-                if (prec == 0) launch_spmv<double, double, double, double>(s, g, n, p->rp.p, p->ci.p, p->val.p, x.p, y.p, nullptr, nullptr);
-                else launch_spmv<float, float, float, float>(s, g, n, p->rp.p, p->ci.p, v32.p, x32.p, y32.p, nullptr, nullptr);
-            };
-            for (int w = 0; w < 3; ++w) run();
-            CK(cudaEventRecord(e0, s));
-            for (int r = 0; r < 10; ++r) run();
-            CK(cudaEventRecord(e1, s));
-            CK(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) {
-                best = ms;
-                best_g = g;
+        int best_g = kSpG, best_s = 4;
+        for (int round = 0; round < 2; ++round)  // two rounds: a shape's time is its better one
+            for (int c = 0; c < nshape; ++c) {
+                const int g = kSpmvShapes[c][0], st = kSpmvShapes[c][1];
+                auto run = [&] {
+                    if (prec == 0) launch_spmv<double, double, double, double>(s, g, st, n, p->rp.p, p->ci.p, p->val.p, x.p, y.p, nullptr, nullptr);
+                    else launch_spmv<float, float, float, float>(s, g, st, n, p->rp.p, p->ci.p, v32.p, x32.p, y32.p, nullptr, nullptr);
+                };
+                for (int w = 0; w < 3; ++w) run();
+                CK(cudaEventRecord(e0, s));
+                for (int r = 0; r < 10; ++r) run();
+                CK(cudaEventRecord(e1, s));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) {
+                    best = ms;
+                    best_g = g;
+                    best_s = st;
+                }
             }
-        }
         p->spmv_lanes[prec] = best_g;
+        p->spmv_strides[prec] = best_s;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->launches += 2 * 5 * 13 + 1;
+    ctx->launches += 2 * 2 * nshape * 13 + 1;
     CK(cudaGetLastError());
     if (lanes64) *lanes64 = p->spmv_lanes[0];
     if (lanes32) *lanes32 = p->spmv_lanes[1];
+    return VFV_OK;
+}
+
+int vfv_pattern_spmv_shape(const vfv_pattern* p, int32_t* lanes64, int32_t* strides64, int32_t* lanes32, int32_t* strides32) {
+    if (!p) return set_err(nullptr, VFV_BAD_INPUT, "pattern is NULL");
+    if (lanes64) *lanes64 = p->spmv_lanes[0];
+    if (strides64) *strides64 = p->spmv_strides[0];
+    if (lanes32) *lanes32 = p->spmv_lanes[1];
+    if (strides32) *strides32 = p->spmv_strides[1];
     return VFV_OK;
 }
 
@@ -1823,6 +1810,7 @@ int vfv_pattern_set_spmv_lanes(vfv_ctx* ctx, vfv_pattern* p, int32_t lanes64, in
     if (!ok(lanes64) || !ok(lanes32)) return set_err(ctx, VFV_BAD_INPUT, "SpMV lanes per row must be 2, 4, 8, 16 or 32");
     p->spmv_lanes[0] = lanes64;
     p->spmv_lanes[1] = lanes32;
+    p->spmv_strides[0] = p->spmv_strides[1] = 4;
     return VFV_OK;
 }
 

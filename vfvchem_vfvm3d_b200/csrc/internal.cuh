@@ -85,13 +85,14 @@ struct IluStruct {
     DBuf<int> bad;
     uint64_t version64 = ~0ull, version32 = ~0ull;
 
-    // single-launch sweeps (k_ilu0_chain): row tasks inside levels, and per precision the four
-    // work vectors, the claim/parity state and a host-mapped timeout flag for standalone applies
-    DBuf<int32_t> tasks;
+    // single-launch sweeps (k_ilu0_chain): row tasks inside levels (row starts, levels, tasks per
+    // level), and per precision a work vector for standalone applies, the claim and completion
+    // counters and a host-mapped timeout flag for standalone applies
+    DBuf<int32_t> tasks, task_lev, lev_ntask;
     int ntask = 0;
     struct Chain {
-        DBuf<unsigned char> work;   // 4 x n words of the precision
-        DBuf<unsigned char> state;  // IluChainState
+        DBuf<unsigned char> work;   // n entries of the precision (standalone applies)
+        DBuf<unsigned char> state;  // IluChainState + 2 nlev completion counters
         int* h_flag = nullptr;      // pinned, mapped: set by a wait that gave up
         int* d_flag = nullptr;
         int grid = 0;
@@ -112,7 +113,8 @@ struct SolverBase {
 struct vfv_pattern {
     vfv_ctx* ctx = nullptr;
     int64_t n = 0, nnz = 0, ntrip = 0;
-    int spmv_lanes[2] = {4, 4};  // lanes per row of the SpMV for double / float values (autotuned; kSpG by default)
+    int spmv_lanes[2] = {4, 4};    // lanes per row of the SpMV for double / float values (autotuned; kSpG by default)
+    int spmv_strides[2] = {4, 4};  // strides each lane loads before its gathers (autotuned with the lanes)
     std::vector<int32_t> h_rp, h_ci;
     DBuf<int32_t> rp, ci, diag_pos;
     DBuf<double> val;

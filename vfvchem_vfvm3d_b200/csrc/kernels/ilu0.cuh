@@ -129,75 +129,43 @@ namespace vfv {
 
 // ---------------------------------------------------------------- both sweeps in one launch
 // The level-per-launch sweeps above pay a launch and a drain per level (20 per apply on the
-// 10^6-row heat matrix, ~5 µs each), while a level moves only ~8 MB. Here one launch runs both
-// sweeps as a dataflow over row tasks: a task is at most kChainThreads rows of one level, lower
-// tasks in level order followed by upper tasks in reverse level order, and CTAs claim tasks from a
-// global counter in that order. A thread owns one row: it loads the row's indices and factor
-// values, then gathers the solved values it needs, waiting (bounded) for each one that is not
-// solved yet. Solved values double as the ready flags: the work vectors start filled with a
-// sentinel bit pattern (all ones, a NaN no arithmetic produces), a relaxed load that returns
-// anything else is the final value, and a stored result that happens to equal the sentinel is
-// replaced by the canonical NaN.
+// 10^6-row heat matrix). Here one launch runs both sweeps: a task is at most kChainThreads rows of
+// one level; CTAs claim tasks from a global counter, lower tasks in level order, then upper tasks
+// in reverse level order. Each level has a completion counter; a task first loads everything that
+// does not depend on the sweep (its rows' indices, factor values, right-hand side), then one thread
+// of the CTA waits (bounded, with backoff) until the level it depends on has all its tasks counted,
+// and then the rows gather their solved neighbours from L2 (ld.global.cg: solved values are written
+// during the launch, so no L1 copy may be used). One polling thread per CTA keeps the waiting cheap.
 //
-// Progress: a task waits only on tasks claimed before it (its lower entries are rows of earlier
-// levels, its upper entries rows of later levels, whose upper tasks come first, and the upper task
-// of row i needs the lower result of row i). The smallest unfinished claim therefore has every
-// input solved and finishes, so the sweeps complete for any number of resident CTAs (no cooperative
-// launch needed; kernels on other streams may share the GPU). Every wait is bounded anyway: past
-// the poll limit (or 2 s) the waiting thread raises `abort`, records the timeout and every CTA
-// leaves.
+// Progress: a task waits only on levels whose tasks were all claimed before it (lower level l on
+// lower level l-1; upper level L-1 on lower level L-1, which completes after every lower level;
+// upper level l on upper level l+1), so the smallest unfinished claim always has its inputs and
+// finishes, whatever number of CTAs is resident (no cooperative launch; kernels on other streams
+// may share the GPU). Every wait is bounded anyway: past the poll limit (or 2 s) the waiting thread
+// raises `abort`, records the timeout, and every CTA leaves. The last CTA to leave zeroes the
+// counters for the next launch.
 //
-// Work vectors: two pairs (t = lower results, u = upper results, permuted numbering) used by
-// alternate launches; a launch refills the other pair with the sentinel as it goes (row i resets
-// its own entries), so no separate clearing pass is needed. The last CTA to leave resets the claim
-// counter and flips the parity for the next launch.
-//
-// Results are bit-identical to k_ilu0_level: each row sums its entries in the same order.
+// Results are bit-identical to k_ilu0_level: same work vector use (t in place) and the same
+// summation order per row.
 constexpr int kChainThreads = 128;
 
 struct IluChainState {
-    unsigned claim;      // next task index
+    unsigned claim;        // next task index
     unsigned pad0[31];
-    unsigned exited;     // CTAs that have left this launch
+    unsigned exited;       // CTAs that have left this launch
     unsigned pad1[31];
-    unsigned parity;     // work-vector pair of the next launch
-    unsigned abort;      // a bounded wait gave up: every CTA leaves at its next check
+    unsigned abort;        // a bounded wait gave up: every CTA leaves at its next check
+    unsigned pad2;
     long long poll_limit;  // polls before a wait gives up (set by the host)
-    unsigned pad2[28];
+    unsigned pad3[28];
+    // followed by 2 * nlev completion counters: [phase * nlev + level], phase 0 lower, 1 upper
 };
 
-template <typename T> struct ChainWord;
-template <> struct ChainWord<float> {
-    using U = uint32_t;
-    static constexpr U kSentinel = 0xFFFFFFFFu;
-    static constexpr U kCanonNaN = 0x7FFFFFFFu;
-};
-template <> struct ChainWord<double> {
-    using U = unsigned long long;
-    static constexpr U kSentinel = 0xFFFFFFFFFFFFFFFFull;
-    static constexpr U kCanonNaN = 0x7FF8000000000000ull;
-};
-
-__device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t* p) {
-    uint32_t v;
-    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p));
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
 }
-__device__ __forceinline__ unsigned long long ld_relaxed_gpu(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
-    return v;
-}
-__device__ __forceinline__ void st_relaxed_gpu(uint32_t* p, uint32_t v) {
-    asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void st_relaxed_gpu(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ float word_to(uint32_t b) { return __uint_as_float(b); }
-__device__ __forceinline__ double word_to(unsigned long long b) { return __longlong_as_double((long long)b); }
-__device__ __forceinline__ uint32_t to_word(float v) { return __float_as_uint(v); }
-__device__ __forceinline__ unsigned long long to_word(double v) { return (unsigned long long)__double_as_longlong(v); }
 
 __device__ __forceinline__ unsigned long long chain_clock_ns() {
     unsigned long long t;
@@ -205,160 +173,122 @@ __device__ __forceinline__ unsigned long long chain_clock_ns() {
     return t;
 }
 
-// Slow path of a gather: poll until the word is solved and return it. Returns the sentinel itself
-// (after raising abort and the timeout flag) when the poll limit or 2 s pass, or when another
-// thread has aborted.
-template <typename U>
-__device__ __noinline__ U chain_wait(const U* p, U sentinel, IluChainState* cs, int* timeout_flag, long long poll_limit) {
+// Waits until *cnt reaches target (one thread). False when the poll limit or 2 s pass (after
+// raising abort and the timeout flag) or when another CTA has aborted.
+__device__ __noinline__ bool chain_wait_count(const unsigned* cnt, unsigned target, IluChainState* cs, int* timeout_flag,
+                                              long long poll_limit) {
+    if (ld_relaxed_u32(cnt) >= target) return true;
     const unsigned long long t0 = chain_clock_ns();
+    unsigned sleep = 32;
     for (long long it = 1;; ++it) {
-        __nanosleep(64);
-        const U b = ld_relaxed_gpu(p);
-        if (b != sentinel) return b;
-        if ((it & 63) == 0 && *(volatile unsigned*)&cs->abort) return sentinel;
-        if (it >= poll_limit || ((it & 1023) == 0 && chain_clock_ns() - t0 > 2000000000ull)) {
+        __nanosleep(sleep);
+        if (sleep < 1024) sleep <<= 1;
+        if (ld_relaxed_u32(cnt) >= target) return true;
+        if ((it & 15) == 0 && ld_relaxed_u32(&cs->abort)) return false;
+        if (it >= poll_limit || ((it & 255) == 0 && chain_clock_ns() - t0 > 2000000000ull)) {
             *(volatile unsigned*)&cs->abort = 1u;
             *(volatile int*)timeout_flag = 1;
-            return sentinel;
+            return false;
         }
     }
-}
-
-// s += sum over entries [kb, ke) of lu[k] * x[ci[k]], gathering x from the work vector `xw`
-// (waiting for unsolved rows). The first K entries were loaded into c/v before any wait.
-template <typename T, int K>
-__device__ __forceinline__ bool chain_gather(const int32_t* c, const T* v, int32_t kb, int32_t ke, const int32_t* __restrict__ ci,
-                                             const T* __restrict__ lu, const typename ChainWord<T>::U* xw, T& s, IluChainState* cs,
-                                             int* timeout_flag, long long poll_limit) {
-    using W = ChainWord<T>;
-    using U = typename W::U;
-    constexpr int G = 4;  // gathers in flight before the first use
-#pragma unroll
-    for (int q0 = 0; q0 < K; q0 += G) {
-        U raw[G];
-#pragma unroll
-        for (int g = 0; g < G; ++g) raw[g] = c[q0 + g] >= 0 ? ld_relaxed_gpu(xw + c[q0 + g]) : U(0);
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-            if (c[q0 + g] < 0) continue;
-            U b = raw[g];
-            if (b == W::kSentinel) {
-                b = chain_wait(xw + c[q0 + g], W::kSentinel, cs, timeout_flag, poll_limit);
-                if (b == W::kSentinel) return false;
-            }
-            s += v[q0 + g] * word_to(b);
-        }
-    }
-    for (int32_t k = kb + K; k < ke; ++k) {
-        const int32_t col = __ldg(ci + k);
-        U b = ld_relaxed_gpu(xw + col);
-        if (b == W::kSentinel) {
-            b = chain_wait(xw + col, W::kSentinel, cs, timeout_flag, poll_limit);
-            if (b == W::kSentinel) return false;
-        }
-        s += __ldg(lu + k) * word_to(b);
-    }
-    return true;
 }
 
 template <typename T> struct ChainCfg;
 template <> struct ChainCfg<float> { static constexpr int K = 16, kMinBlocks = 8; };
-template <> struct ChainCfg<double> { static constexpr int K = 12, kMinBlocks = 6; };
+template <> struct ChainCfg<double> { static constexpr int K = 16, kMinBlocks = 6; };
 
-// z = (LU)^-1 r over the permuted factor; tasks[ntask + 1] = row starts of the tasks (each inside
-// one level); work = 4 vectors of n words (t0, t1, u0, u1). `in` and `out` may alias: only row i
-// reads in[perm[i]], before the upper task of row i writes out[perm[i]].
+// z = (LU)^-1 r over the permuted factor. tasks[ntask + 1]: row starts of the tasks (each inside
+// one level); task_lev[ntask]: their levels; lev_ntask[nlev]: tasks per level. t is the work vector
+// (n entries, may not alias r or z; r and z may alias: only row i reads r[perm[i]], before the
+// upper task of row i writes z[perm[i]]).
 template <typename T>
 __global__ void __launch_bounds__(kChainThreads, ChainCfg<T>::kMinBlocks)
-    k_ilu0_chain(int32_t ntask, const int32_t* __restrict__ tasks, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                 const int32_t* __restrict__ dg, const T* __restrict__ lu, const int32_t* __restrict__ perm, int64_t n, const T* in,
-                 T* out, typename ChainWord<T>::U* work, IluChainState* cs, int* timeout_flag, const DevStatus* __restrict__ st) {
-    using W = ChainWord<T>;
-    using U = typename W::U;
+    k_ilu0_chain(int32_t ntask, int32_t nlev, const int32_t* __restrict__ tasks, const int32_t* __restrict__ task_lev,
+                 const int32_t* __restrict__ lev_ntask, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                 const int32_t* __restrict__ dg, const T* __restrict__ lu, const int32_t* __restrict__ perm, const T* in, T* t, T* out,
+                 IluChainState* cs, int* timeout_flag, const DevStatus* __restrict__ st) {
     constexpr int K = ChainCfg<T>::K;
+    unsigned* done = reinterpret_cast<unsigned*>(cs + 1);
     const long long poll_limit = cs->poll_limit;
     const int total = 2 * ntask;
     __shared__ int s_task[2];
-    __shared__ unsigned s_par;
-    __shared__ int s_abort;
+    __shared__ int s_go;
     if (threadIdx.x == 0) {
         // A CTA that finds the solve already done (or an earlier launch aborted) claims nothing but
         // still counts itself out below. `done` may be set by a kernel running concurrently on
         // another stream, so CTAs can disagree; the CTAs that do claim keep claiming until every
-        // task is taken, so a launch either completes every row or (no claims at all) none.
-        const bool ab = *(volatile unsigned*)&cs->abort != 0u;
-        const bool skip = ab || (st && *(volatile const int32_t*)&st->done);
-        s_par = *(volatile unsigned*)&cs->parity;
+        // task is taken, so a launch completes every row or (no claims at all) none.
+        const bool skip = ld_relaxed_u32(&cs->abort) != 0u || (st && *(volatile const int32_t*)&st->done);
         s_task[0] = skip ? total : (int)atomicAdd(&cs->claim, 1u);
-        s_abort = ab ? 1 : 0;
     }
     __syncthreads();
-    const unsigned par = s_par & 1u;
-    U* tcur = work + (int64_t)par * n;
-    U* tnxt = work + (int64_t)(1u - par) * n;
-    U* ucur = work + (int64_t)(2u + par) * n;
-    U* unxt = work + (int64_t)(3u - par) * n;
     int cur = 0;
-    bool ok = true;
     for (;;) {
         const int task = s_task[cur];
-        if (task >= total || s_abort) break;
+        if (task >= total) break;
         if (threadIdx.x == 0) s_task[cur ^ 1] = (int)atomicAdd(&cs->claim, 1u);  // next claim, in flight during this task
         const bool lower = task < ntask;
         const int tk = lower ? task : total - 1 - task;
+        const int lev = __ldg(task_lev + tk);
         const int32_t r0 = __ldg(tasks + tk), r1 = __ldg(tasks + tk + 1);
         const int32_t i = r0 + (int32_t)threadIdx.x;
-        if (i < r1 && ok) {
-            const int32_t d = __ldg(dg + i);
-            const int32_t kb = lower ? __ldg(rp + i) : d + 1;
-            const int32_t ke = lower ? d : __ldg(rp + i + 1);
-            const int32_t pi = __ldg(perm + i);
-            int32_t c[K];
-            T v[K];
+        const bool row = i < r1;
+        int32_t kb = 0, ke = 0, d = 0, pi = 0;
+        int32_t c[K];
+        T v[K];
+        T rhs = T(0), diag = T(1);
+        if (row) {
+            d = __ldg(dg + i);
+            kb = lower ? __ldg(rp + i) : d + 1;
+            ke = lower ? d : __ldg(rp + i + 1);
+            pi = __ldg(perm + i);
+            if (lower) rhs = in[pi];
+            else diag = __ldg(lu + d);
 #pragma unroll
             for (int q = 0; q < K; ++q) {
                 c[q] = kb + q < ke ? __ldg(ci + kb + q) : -1;
                 v[q] = kb + q < ke ? __ldg(lu + kb + q) : T(0);
             }
+        }
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            if (lower && lev > 0) ok = chain_wait_count(done + lev - 1, (unsigned)__ldg(lev_ntask + lev - 1), cs, timeout_flag, poll_limit);
+            else if (!lower && lev == nlev - 1) ok = chain_wait_count(done + lev, (unsigned)__ldg(lev_ntask + lev), cs, timeout_flag, poll_limit);
+            else if (!lower) ok = chain_wait_count(done + nlev + lev + 1, (unsigned)__ldg(lev_ntask + lev + 1), cs, timeout_flag, poll_limit);
+            s_go = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_go) break;
+        if (row) {
+            if (!lower) rhs = __ldcg(t + i);
             T s = T(0);
+#pragma unroll
+            for (int q = 0; q < K; ++q)
+                if (c[q] >= 0) s += v[q] * __ldcg(t + c[q]);
+            for (int32_t k = kb + K; k < ke; ++k) s += __ldg(lu + k) * __ldcg(t + __ldg(ci + k));
             if (lower) {
-                const T rhs = in[pi];
-                tnxt[i] = W::kSentinel;  // the next launch's pair: nobody reads it during this one
-                unxt[i] = W::kSentinel;
-                ok = chain_gather<T, K>(c, v, kb, ke, ci, lu, tcur, s, cs, timeout_flag, poll_limit);
-                if (ok) {
-                    U r = to_word(rhs - s);
-                    if (r == W::kSentinel) r = W::kCanonNaN;
-                    st_relaxed_gpu(tcur + i, r);
-                }
+                t[i] = rhs - s;
             } else {
-                const T diag = __ldg(lu + d);
-                U rb = ld_relaxed_gpu(tcur + i);
-                if (rb == W::kSentinel) rb = chain_wait(tcur + i, W::kSentinel, cs, timeout_flag, poll_limit);
-                ok = rb != W::kSentinel;
-                if (ok) ok = chain_gather<T, K>(c, v, kb, ke, ci, lu, ucur, s, cs, timeout_flag, poll_limit);
-                if (ok) {
-                    const T x = (word_to(rb) - s) / diag;
-                    U r = to_word(x);
-                    if (r == W::kSentinel) r = W::kCanonNaN;
-                    st_relaxed_gpu(ucur + i, r);
-                    out[pi] = x;
-                }
+                const T x = (rhs - s) / diag;
+                t[i] = x;
+                out[pi] = x;
             }
         }
-        if (threadIdx.x == 0 && *(volatile unsigned*)&cs->abort) s_abort = 1;
-        __syncthreads();
+        __syncthreads();  // this task's rows are stored (and s_task[cur ^ 1] is visible)
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(done + (lower ? 0 : nlev) + lev, 1u);
+        }
         cur ^= 1;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         const unsigned e = atomicAdd(&cs->exited, 1u);
-        if (e == gridDim.x - 1) {  // every CTA has stopped claiming: reset for the next launch
-            const unsigned claimed = *(volatile unsigned*)&cs->claim;
+        if (e == gridDim.x - 1) {  // every CTA has stopped claiming and counting: reset for the next launch
             cs->claim = 0u;
             cs->exited = 0u;
-            if (claimed > 0u) cs->parity = par ^ 1u;  // every row ran and refilled the other pair
+            for (int l = 0; l < 2 * nlev; ++l) done[l] = 0u;
             __threadfence();
         }
     }

@@ -70,7 +70,7 @@ __device__ __forceinline__ int mesh_of_row(const int64_t* __restrict__ mesh_row,
 }
 
 // y = (A x) * inv_beta[mesh(row)][j]: the single-system SpMV with the step's scale looked up per row.
-template <typename TV, typename TX, typename TY, typename TA, int G>
+template <typename TV, typename TX, typename TY, typename TA, int G, int S = 4>
 __global__ void __launch_bounds__(kBlk) k_spmv_seg(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                                   const TV* __restrict__ val, const TX* __restrict__ x, TY* __restrict__ y,
                                                   const double* __restrict__ inv_beta, int stride, int j,
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kBlk) k_spmv_seg(int64_t n, const int32_t* __r
     const int lane = threadIdx.x & (G - 1);
     const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     TA s = TA(0);
-    if (row < n) s = row_dot<TV, TX, TA, G>(rp, ci, val, x, row, lane);
+    if (row < n) s = row_dot<TV, TX, TA, G, S>(rp, ci, val, x, row, lane);
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, G);
     if (lane == 0 && row < n) {
