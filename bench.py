@@ -341,7 +341,8 @@ def main():
     heat.assemble_device(k_d.data_ptr(), q_d.data_ptr(), s_d.data_ptr(), T_d.data_ptr(), bc_d.data_ptr())
     ctx.synchronize()
     pat = heat.pattern
-    lanes64, lanes32 = pat.autotune()  # SpMV lanes per row, measured before the solvers capture their graphs
+    pat.autotune()  # SpMV shape (lanes per row, strides per lane), measured before the solvers capture their graphs
+    (lanes64, strides64), (lanes32, strides32) = pat.spmv_shape()
     n, nnz = pat.n, pat.nnz
     b_d = torch.tensor(heat.assemble(prob.k, prob.q, prob.s, prob.T0, prob.bc_val), device=dev)
     x_d = torch.empty_like(b_d)
@@ -493,9 +494,9 @@ def main():
                      "traffic": ILU_TRAFFIC_N100 if args.n == 100 else None,
                      "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                      "algorithmic_bytes_per_apply": bytes_ilu32, "apply_us": ilu_s * 1e6},
-        "roofline_spmv": {"bound": "hbm", "kernel": f"k_spmv<double> (CSR, {lanes64} lanes/row)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
+        "roofline_spmv": {"bound": "hbm", "kernel": f"k_spmv<double> (CSR, {lanes64} lanes/row, {strides64} strides/lane)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
                           "frac": gbs64 / peak, "peak_kind": peak_kind,
-                          "traffic": SPMV_TRAFFIC_N100_4LANES if (args.n == 100 and lanes64 == 4) else None,
+                          "traffic": SPMV_TRAFFIC_N100_4LANES if (args.n == 100 and (lanes64, strides64) == (4, 4)) else None,
                           "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                           "algorithmic_bytes_per_launch": bytes64},
         "cpu_baseline": cpu,
@@ -503,7 +504,7 @@ def main():
         "gpu_launches": int(launches_mx),
         "clocks": clocks,
         "ref_solution": ref_info,
-        "spmv_fp64_gbs": gbs64, "spmv_fp32_gbs": gbs32, "spmv_fp64_ms": sp64 * 1e3, "spmv_fp32_ms": sp32 * 1e3,
+        "spmv_fp64_gbs": gbs64, "spmv_fp32_gbs": gbs32, "spmv_shape_f32": [lanes32, strides32], "spmv_fp64_ms": sp64 * 1e3, "spmv_fp32_ms": sp32 * 1e3,
         "assembly_ms": asm_s * 1e3, "mesh_setup_s": t_mesh,
         "extras": extras,
     }
