@@ -26,57 +26,47 @@ __device__ __forceinline__ unsigned group_mask(int G) {
     return base << (lane & ~(G - 1));
 }
 
-// grad_f[v] = sum_loc w[v][loc] * (f[n] - f[v]) for up to 4 fields at once.
-// out layout: [field][3][n]
+// grad_f[v] = sum_loc w[v][loc] * (f[n] - f[v]) for NF <= 4 fields at once; out layout [field][3][n].
+// A row's 16 lanes compute the terms of 16 faces at a time into shared memory; then lane
+// 3 f + c adds component (f, c) of those terms in face order (the reference's summation order),
+// so the 3 NF running sums proceed in parallel instead of through 3 NF shuffles per face.
+template <int NF>
 __global__ void __launch_bounds__(256) k_grad_lsq(int64_t n, const int32_t* __restrict__ np, const int32_t* __restrict__ ni,
-                                                 const double* __restrict__ gw, int64_t n_dir, int nf,
-                                                 const double* __restrict__ f0, const double* __restrict__ f1,
-                                                 const double* __restrict__ f2, const double* __restrict__ f3,
-                                                 double* __restrict__ out) {
+                                                 const double* __restrict__ gw, int64_t n_dir, const double* __restrict__ f0,
+                                                 const double* __restrict__ f1, const double* __restrict__ f2,
+                                                 const double* __restrict__ f3, double* __restrict__ out) {
+    __shared__ double term[256 / kAG][3 * NF][kAG + 1];  // [row of the block][component][face of the chunk]
     const int lane = threadIdx.x & (kAG - 1);
+    const int rib = threadIdx.x / kAG;  // row in block
     const int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kAG;
     if (v >= n) return;  // whole groups leave together
     const unsigned mask = group_mask(kAG);
     const double* F[4] = {f0, f1, f2, f3};
-    double fv[4], acc[4][3];
+    double fv[NF];
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-        fv[f] = f < nf ? F[f][v] : 0.0;
-        acc[f][0] = acc[f][1] = acc[f][2] = 0.0;
-    }
+    for (int f = 0; f < NF; ++f) fv[f] = F[f][v];
+    double acc = 0.0;  // lane 3 f + c < 3 NF: component (f, c)
     const int32_t b = np[v], e = np[v + 1];
     for (int32_t c0 = b; c0 < e; c0 += kAG) {
         const int32_t i = c0 + lane;
-        double p[4][3];
         if (i < e) {
             const int32_t nb = ni[i];
             const double wx = gw[i], wy = gw[n_dir + i], wz = gw[2 * n_dir + i];
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                const double dlt = f < nf ? F[f][nb] - fv[f] : 0.0;
-                p[f][0] = wx * dlt;
-                p[f][1] = wy * dlt;
-                p[f][2] = wz * dlt;
+            for (int f = 0; f < NF; ++f) {
+                const double dlt = F[f][nb] - fv[f];
+                term[rib][3 * f][lane] = wx * dlt;
+                term[rib][3 * f + 1][lane] = wy * dlt;
+                term[rib][3 * f + 2][lane] = wz * dlt;
             }
-        } else {
-#pragma unroll
-            for (int f = 0; f < 4; ++f) p[f][0] = p[f][1] = p[f][2] = 0.0;
         }
+        __syncwarp(mask);
         const int cnt = min(kAG, (int)(e - c0));
-        for (int q = 0; q < cnt; ++q) {
-#pragma unroll
-            for (int f = 0; f < 4; ++f)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const double t = __shfl_sync(mask, p[f][c], q, kAG);
-                    acc[f][c] += t;
-                }
-        }
+        if (lane < 3 * NF)
+            for (int q = 0; q < cnt; ++q) acc += term[rib][lane][q];
+        __syncwarp(mask);
     }
-    if (lane == 0) {
-        for (int f = 0; f < nf; ++f)
-            for (int c = 0; c < 3; ++c) out[((int64_t)f * 3 + c) * n + v] = acc[f][c];
-    }
+    if (lane < 3 * NF) out[(int64_t)lane * n + v] = acc;  // lane = 3 f + c: out[(f * 3 + c) n + v]
 }
 
 __global__ void __launch_bounds__(256) k_assemble_heat(HeatDev H) {
@@ -303,8 +293,15 @@ void launch_grad(cudaStream_t s, int64_t n, const int32_t* np, const int32_t* ni
                  const double* const* f, double* out) {
     const int64_t threads = n * kAG;
     const int blocks = (int)((threads + 255) / 256);
-    k_grad_lsq<<<blocks, 256, 0, s>>>(n, np, ni, gw, n_dir, nf, f[0], nf > 1 ? f[1] : nullptr, nf > 2 ? f[2] : nullptr,
-                                       nf > 3 ? f[3] : nullptr, out);
+    const double* g1 = nf > 1 ? f[1] : nullptr;
+    const double* g2 = nf > 2 ? f[2] : nullptr;
+    const double* g3 = nf > 3 ? f[3] : nullptr;
+    switch (nf) {
+        case 1: k_grad_lsq<1><<<blocks, 256, 0, s>>>(n, np, ni, gw, n_dir, f[0], g1, g2, g3, out); break;
+        case 2: k_grad_lsq<2><<<blocks, 256, 0, s>>>(n, np, ni, gw, n_dir, f[0], g1, g2, g3, out); break;
+        case 3: k_grad_lsq<3><<<blocks, 256, 0, s>>>(n, np, ni, gw, n_dir, f[0], g1, g2, g3, out); break;
+        default: k_grad_lsq<4><<<blocks, 256, 0, s>>>(n, np, ni, gw, n_dir, f[0], g1, g2, g3, out); break;
+    }
 }
 
 void launch_assemble_heat(cudaStream_t s, const HeatDev& H) {
