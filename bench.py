@@ -185,7 +185,7 @@ def extras_transport(ctx, count):
     from vfvchem_vfvm3d_b200 import _lib as L
     from vfvchem_vfvm3d_b200.problems import transport_batch, transport_fields
     t0 = time.perf_counter()
-    tb = transport_batch(count)
+    tb = transport_batch(count, dual_ctx=ctx)  # Delaunay on the host, Voronoi duals on the device
     vel, c0 = transport_fields(tb.meshes)
     t_mesh = time.perf_counter() - t0
     tr = TransientTransportGpu(tb.meshes, tb.dt, ctx=ctx)
@@ -203,7 +203,8 @@ def extras_transport(ctx, count):
     t_adj = time.perf_counter() - t0
     return {"meshes": count, "rows": tr.n, "nnz": tr.nnz, "steps": tb.steps, "run_s": t_run, "step_ms": t_run / tb.steps * 1e3,
             "iters_per_step": float(np.mean(its)), "adjoint_dJdD_s": t_adj, "adjoint_iters_per_solve": float(np.mean(aits)), "J": J, "dJdD": dJdD, "spmv_lanes_f64_f32": list(lanes),
-            "mesh_setup_s": t_mesh,
+            "mesh_setup_s": t_mesh, "per_mesh_steps_mean": float(np.mean(tr.mesh_steps())),
+            "per_mesh_steps_min_max": [int(np.min(tr.mesh_steps())), int(np.max(tr.mesh_steps()))],
             "workload": f"{count} jittered cubes, N_i log-uniform in [2000, 50000], D=1e-3, u=(sin pi y, sin pi z, sin pi x), dt=1e-2; "
                         "GMRES(30)+ILU(0) mixed to 1e-10 relres per mesh and step; host arrays in/out"}
 

@@ -171,6 +171,12 @@ int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out);
  * other input is refused with VFV_BAD_INPUT rather than rounded. */
 int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out);
 void vfv_mesh_destroy(vfv_mesh* m);
+/* Recomputes the mesh's Voronoi dual from its tetrahedra on the device of ctx (Tetrahedron::update_tet,
+ * src/base/geom_tet.rs:122-293: face pieces, sorted-edge sums, control volumes, boundary sub-faces,
+ * least-squares weights); the result equals the host dual bit for bit and replaces it. */
+int vfv_mesh_dual_device(vfv_ctx* ctx, vfv_mesh* m);
+/* vfv_mesh_jitter_cubes with the duals built on the device (Delaunay on the host, meshes in parallel) */
+int vfv_mesh_jitter_cubes_device_dual(vfv_ctx* ctx, int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out);
 /* count meshes at once (built in parallel on the host): out[i] = jitter cube of n[i]^3 points, seeds[i] */
 int vfv_mesh_jitter_cubes(int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out);
 /* counts: vertices split, tetrahedra, directed faces (2 x Voronoi faces), boundary sub-faces */

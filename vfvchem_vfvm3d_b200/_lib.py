@@ -83,6 +83,8 @@ SIGNATURES = [
     ("vfv_mesh_jitter_cube", C.c_int, [C.c_int, C.c_uint64, C.c_double, _PP]),
     ("vfv_mesh_from_vertices", C.c_int, [C.c_int64, C.c_int64, _DP, _I32P, _PP]),
     ("vfv_mesh_destroy", None, [_P]),
+    ("vfv_mesh_dual_device", C.c_int, [_P, _P]),
+    ("vfv_mesh_jitter_cubes_device_dual", C.c_int, [_P, C.c_int, _I32P, _U64P, C.c_double, C.POINTER(C.c_void_p)]),
     ("vfv_mesh_jitter_cubes", C.c_int, [C.c_int, _I32P, _U64P, C.c_double, C.POINTER(C.c_void_p)]),
     ("vfv_mesh_info", C.c_int, [_P, _I64P, _I64P, _I64P, _I64P, _I64P]),
     ("vfv_mesh_export", C.c_int, [_P, _DP, _I32P, _I32P]),

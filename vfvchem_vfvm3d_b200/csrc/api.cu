@@ -426,7 +426,6 @@ int chain_reset(vfv_ctx* ctx, IluStruct& S, long long polls) {
     CK(cudaMemsetAsync(C.state.p, 0, C.state.n, s));
     CK(cudaMemcpyAsync(C.state.p, &h, sizeof(h), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
-    *C.h_flag = 0;
     return VFV_OK;
 }
 
@@ -453,9 +452,6 @@ int chain_setup(vfv_ctx* ctx, IluStruct& S, int64_t n) {
     }
     CK(C.work.alloc((size_t)n * sizeof(T)));
     CK(C.state.alloc(sizeof(IluChainState) + 2 * (size_t)S.nlev * sizeof(unsigned)));
-    CK(cudaHostAlloc((void**)&C.h_flag, sizeof(int), cudaHostAllocMapped));
-    *C.h_flag = 0;
-    CK(cudaHostGetDevicePointer((void**)&C.d_flag, C.h_flag, 0));
     int per_sm = 0, sms = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu0_chain<T>, kChainThreads, 0));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
@@ -528,7 +524,7 @@ struct Gmres : SolverBase {
     cudaStream_t s2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int ilu_prio = 0;  // greatest stream priority: the sweeps' blocks go first when SM slots free up
-    bool ilu_chain = true;  // ILU(0) sweeps as one k_ilu0_chain launch (false: one launch per level)
+    bool ilu_chain = false;  // ILU(0) sweeps as one k_ilu0_chain launch (VFV_ILU_CHAIN=1) instead of one launch per level
     // batch of independent meshes (block-diagonal system), one Krylov recurrence per mesh
     int nm = 0;
     DBuf<int64_t> b_mesh_row, b_tile_row, b_rtile_row;
@@ -650,7 +646,7 @@ struct Gmres : SolverBase {
                 it = p->ilu.emplace(ilu_order, std::move(S)).first;
             }
             ilu = it->second.get();
-            if (const char* e = getenv("VFV_ILU_LEVELS")) ilu_chain = e[0] != '1';
+            if (const char* e = getenv("VFV_ILU_CHAIN")) ilu_chain = e[0] == '1';
             if (ilu_chain) {
                 int rc = chain_setup<T>(ctx, *ilu, n);
                 if (rc) return rc;
@@ -1607,7 +1603,7 @@ int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y) 
 
 namespace {
 // Finds or builds the ILU(0) structure of an ordering, refreshes its numeric factor and sets up the
-// single-launch sweeps of precision T.
+// sweep state of precision T (its work vector serves the standalone double apply).
 template <typename T>
 int ilu_for_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, IluStruct** out) {
     if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
@@ -1627,16 +1623,6 @@ int ilu_for_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, IluStruct** out) 
     return VFV_OK;
 }
 
-// A chain wait of an earlier standalone apply gave up: restore the chain and report it.
-template <typename T>
-int chain_check_flag(vfv_ctx* ctx, IluStruct& S, int64_t n) {
-    IluStruct::Chain& C = S.chain[chain_slot<T>()];
-    if (!*(volatile int*)C.h_flag) return VFV_OK;
-    CK(cudaStreamSynchronize(ctx->stream));
-    int rc = chain_reset<T>(ctx, S, 0);
-    if (rc) return rc;
-    return set_err(ctx, VFV_TIMEOUT, "ILU(0) sweeps: a bounded device wait gave up");
-}
 }  // namespace
 
 extern "C" {
@@ -1646,33 +1632,25 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
     IluStruct* S = nullptr;
     int rc = ilu_for_apply<double>(ctx, p, ilu_order, &S);
     if (rc) return rc;
-    rc = chain_check_flag<double>(ctx, *S, p->n);
-    if (rc) return rc;
-    CK(ilu_apply_chain<double>(ctx->stream, *S, S->lu64.p, r, reinterpret_cast<double*>(S->chain[0].work.p), z, nullptr,
-                               S->chain[0].d_flag));
-    ctx->launches += 1;
+    ilu_apply_levels<double>(ctx->stream, *S, S->lu64.p, r, reinterpret_cast<double*>(S->chain[0].work.p), z, nullptr);
+    ctx->launches += 2 * S->nlev;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
-    rc = chain_check_flag<double>(ctx, *S, p->n);
-    if (rc) return rc;
     if (levels) *levels = S->nlev;
     return VFV_OK;
 }
 
-// z = M^-1 r with the float copy of the factor: the kernel the mixed-precision solver runs.
+// z = M^-1 r with the float copy of the factor: the level sweeps the mixed-precision solver runs.
 // Enqueued on the context's stream with no synchronisation, so calls after the first (which builds
-// the factor and the sweep state) allocate nothing and can be timed back to back. A bounded wait
-// that gave up is reported by the next call on the pattern.
+// the factor) allocate nothing and can be timed back to back.
 int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const float* r, float* t, float* z, int32_t* levels) {
     if (!ctx || !p || !r || !t || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (t == r || t == z) return set_err(ctx, VFV_BAD_INPUT, "the work vector aliases r or z");
     IluStruct* S = nullptr;
     int rc = ilu_for_apply<float>(ctx, p, ilu_order, &S);
     if (rc) return rc;
-    rc = chain_check_flag<float>(ctx, *S, p->n);
-    if (rc) return rc;
-    CK(ilu_apply_chain<float>(ctx->stream, *S, S->lu32.p, r, t, z, nullptr, S->chain[1].d_flag));
-    ctx->launches += 1;
+    ilu_apply_levels<float>(ctx->stream, *S, S->lu32.p, r, t, z, nullptr);
+    ctx->launches += 2 * S->nlev;
     CK(cudaGetLastError());
     if (levels) *levels = S->nlev;
     return VFV_OK;

@@ -482,6 +482,80 @@ inline void face_pieces(const Mesh& mesh, const int32_t* tv, V3 c_t, int e, doub
 
 }  // namespace
 
+// Boundary sub-faces (geom_tet.rs:208-259) of the faces flagged in bface[4 t + k] (the face
+// opposite local vertex k of tetrahedron t is a boundary face), visited in (tetrahedron, face)
+// order; fills d.bnd_* and d.bnd_sum. Returns "" on success.
+std::string boundary_subfaces(const Mesh& mesh, const std::vector<uint8_t>& bface, Dual& d) {
+    const int64_t N = mesh.n_tot(), T = mesh.n_tet();
+    const int32_t* tet = mesh.tets.data();
+    auto P = [&](int64_t v) { return V3{mesh.pos[3 * v], mesh.pos[3 * v + 1], mesh.pos[3 * v + 2]}; };
+    static const int FO[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};  // counterclockwise from outside
+    std::vector<int32_t> surf;
+    for (int64_t t = 0; t < T; ++t)
+        for (int k = 0; k < 4; ++k)
+            if (bface[4 * t + k]) surf.insert(surf.end(), {tet[4 * t + FO[k][0]], tet[4 * t + FO[k][1]], tet[4 * t + FO[k][2]]});
+    for (int32_t v : surf)
+        if (v < mesh.n_pts) return "dual: a boundary face joins an interior point";
+    // ---- boundary sub-faces (geom_tet.rs:208-259)
+    const int64_t S = (int64_t)surf.size() / 3;
+    d.bnd_ptr.assign(N + 1, 0);
+    for (int64_t s = 0; s < S; ++s)
+        for (int l = 0; l < 3; ++l) d.bnd_ptr[surf[3 * s + l] + 1]++;
+    for (int64_t v = 0; v < N; ++v) d.bnd_ptr[v + 1] += d.bnd_ptr[v];
+    const int64_t B = d.bnd_ptr[N];
+    d.bnd_j.assign(B, 0);
+    d.bnd_k.assign(B, 0);
+    d.bnd_area.assign(B, 0.0);
+    d.bnd_norm.assign(3 * B, 0.0);
+    d.bnd_wgt.assign(3 * B, 0.0);
+    d.bnd_sum.assign(N, 0.0);
+    std::vector<int64_t> bcur(d.bnd_ptr.begin(), d.bnd_ptr.end() - 1);
+    for (int64_t s = 0; s < S; ++s) {
+        const int32_t* tt = &surf[3 * s];
+        const V3 p0 = P(tt[0]), p1 = P(tt[1]), p2 = P(tt[2]);
+        V3 nrm = cross3(sub3(p1, p0), sub3(p2, p0));
+        nrm = scale3(1.0 / len3(nrm), nrm);
+        const V3 c = circumcircle3(p0, p1, p2);
+        const double sq[3] = {dot3(sub3(p2, p1), sub3(p2, p1)), dot3(sub3(p0, p2), sub3(p0, p2)), dot3(sub3(p1, p0), sub3(p1, p0))};
+        const double lraw[3] = {sq[0] * (sq[1] + sq[2] - sq[0]), sq[1] * (sq[2] + sq[0] - sq[1]), sq[2] * (sq[0] + sq[1] - sq[2])};
+        const double lsum = lraw[0] + lraw[1] + lraw[2];
+        const double lam[3] = {lraw[0] / lsum, lraw[1] / lsum, lraw[2] / lsum};
+        for (int loc = 0; loc < 3; ++loc) {
+            const int32_t vi = tt[loc], vj = tt[(loc + 1) % 3], vk = tt[(loc + 2) % 3];
+            const V3 pi = P(vi), pj = P(vj), pk = P(vk);
+            double ar[2];
+            for (int side = 0; side < 2; ++side) {
+                const V3 pa = side == 0 ? pj : pk, pb = side == 0 ? pk : pj;
+                const V3 m = scale3(0.5, add3(pi, pa));
+                const V3 e = sub3(pa, pi);
+                const double len = len3(e);
+                const V3 u = sub3(sub3(pb, m), scale3(dot3(sub3(pb, m), e) / (len * len), e));
+                ar[side] = 0.25 * len * dot3(sub3(c, m), scale3(1.0 / len3(u), u));
+            }
+            const double asum = ar[0] + ar[1];
+            const double l0 = lam[loc], l1 = lam[(loc + 1) % 3], l2 = lam[(loc + 2) % 3];
+            const V3 cj{(1.5 + l0) / 3.0, (0.5 + l1) / 3.0, l2 / 3.0};
+            const V3 ck{(1.5 + l0) / 3.0, l1 / 3.0, (0.5 + l2) / 3.0};
+            const V3 w = (std::fabs(asum) > 1e-12 * len3(sub3(pj, pi)) * len3(sub3(pk, pi)))
+                             ? scale3(1.0 / asum, add3(scale3(ar[0], cj), scale3(ar[1], ck)))
+                             : V3{1.0, 0.0, 0.0};
+            const int64_t ib = bcur[vi]++;
+            d.bnd_sum[vi] += asum;
+            d.bnd_j[ib] = vj;
+            d.bnd_k[ib] = vk;
+            d.bnd_area[ib] = asum;
+            d.bnd_norm[ib] = nrm.x;
+            d.bnd_norm[B + ib] = nrm.y;
+            d.bnd_norm[2 * B + ib] = nrm.z;
+            d.bnd_wgt[ib] = w.x;
+            d.bnd_wgt[B + ib] = w.y;
+            d.bnd_wgt[2 * B + ib] = w.z;
+        }
+    }
+
+    return "";
+}
+
 // Every step is a data-parallel pass over tetrahedra, vertices or edges. Each sum runs in the
 // order of the serial tetrahedron loop of the reference (tetrahedron, then local edge, then side),
 // so the result does not depend on the thread count.
@@ -734,70 +808,8 @@ std::string build_dual(const Mesh& mesh, Dual& d, double piece_store_bytes) {
     pc_cent.reset();
     ctc.reset();
 
-    // ---- boundary faces in (tetrahedron, face) order
-    static const int FO[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};  // counterclockwise from outside
-    std::vector<int32_t> surf;
-    for (int64_t t = 0; t < T; ++t)
-        for (int k = 0; k < 4; ++k)
-            if (bface[4 * t + k]) surf.insert(surf.end(), {tet[4 * t + FO[k][0]], tet[4 * t + FO[k][1]], tet[4 * t + FO[k][2]]});
-    for (int32_t v : surf)
-        if (v < mesh.n_pts) return "dual: a boundary face joins an interior point";
-    // ---- boundary sub-faces (geom_tet.rs:208-259)
-    const int64_t S = (int64_t)surf.size() / 3;
-    d.bnd_ptr.assign(N + 1, 0);
-    for (int64_t s = 0; s < S; ++s)
-        for (int l = 0; l < 3; ++l) d.bnd_ptr[surf[3 * s + l] + 1]++;
-    for (int64_t v = 0; v < N; ++v) d.bnd_ptr[v + 1] += d.bnd_ptr[v];
-    const int64_t B = d.bnd_ptr[N];
-    d.bnd_j.assign(B, 0);
-    d.bnd_k.assign(B, 0);
-    d.bnd_area.assign(B, 0.0);
-    d.bnd_norm.assign(3 * B, 0.0);
-    d.bnd_wgt.assign(3 * B, 0.0);
-    d.bnd_sum.assign(N, 0.0);
-    std::vector<int64_t> bcur(d.bnd_ptr.begin(), d.bnd_ptr.end() - 1);
-    for (int64_t s = 0; s < S; ++s) {
-        const int32_t* tt = &surf[3 * s];
-        const V3 p0 = P(tt[0]), p1 = P(tt[1]), p2 = P(tt[2]);
-        V3 nrm = cross3(sub3(p1, p0), sub3(p2, p0));
-        nrm = scale3(1.0 / len3(nrm), nrm);
-        const V3 c = circumcircle3(p0, p1, p2);
-        const double sq[3] = {dot3(sub3(p2, p1), sub3(p2, p1)), dot3(sub3(p0, p2), sub3(p0, p2)), dot3(sub3(p1, p0), sub3(p1, p0))};
-        const double lraw[3] = {sq[0] * (sq[1] + sq[2] - sq[0]), sq[1] * (sq[2] + sq[0] - sq[1]), sq[2] * (sq[0] + sq[1] - sq[2])};
-        const double lsum = lraw[0] + lraw[1] + lraw[2];
-        const double lam[3] = {lraw[0] / lsum, lraw[1] / lsum, lraw[2] / lsum};
-        for (int loc = 0; loc < 3; ++loc) {
-            const int32_t vi = tt[loc], vj = tt[(loc + 1) % 3], vk = tt[(loc + 2) % 3];
-            const V3 pi = P(vi), pj = P(vj), pk = P(vk);
-            double ar[2];
-            for (int side = 0; side < 2; ++side) {
-                const V3 pa = side == 0 ? pj : pk, pb = side == 0 ? pk : pj;
-                const V3 m = scale3(0.5, add3(pi, pa));
-                const V3 e = sub3(pa, pi);
-                const double len = len3(e);
-                const V3 u = sub3(sub3(pb, m), scale3(dot3(sub3(pb, m), e) / (len * len), e));
-                ar[side] = 0.25 * len * dot3(sub3(c, m), scale3(1.0 / len3(u), u));
-            }
-            const double asum = ar[0] + ar[1];
-            const double l0 = lam[loc], l1 = lam[(loc + 1) % 3], l2 = lam[(loc + 2) % 3];
-            const V3 cj{(1.5 + l0) / 3.0, (0.5 + l1) / 3.0, l2 / 3.0};
-            const V3 ck{(1.5 + l0) / 3.0, l1 / 3.0, (0.5 + l2) / 3.0};
-            const V3 w = (std::fabs(asum) > 1e-12 * len3(sub3(pj, pi)) * len3(sub3(pk, pi)))
-                             ? scale3(1.0 / asum, add3(scale3(ar[0], cj), scale3(ar[1], ck)))
-                             : V3{1.0, 0.0, 0.0};
-            const int64_t ib = bcur[vi]++;
-            d.bnd_sum[vi] += asum;
-            d.bnd_j[ib] = vj;
-            d.bnd_k[ib] = vk;
-            d.bnd_area[ib] = asum;
-            d.bnd_norm[ib] = nrm.x;
-            d.bnd_norm[B + ib] = nrm.y;
-            d.bnd_norm[2 * B + ib] = nrm.z;
-            d.bnd_wgt[ib] = w.x;
-            d.bnd_wgt[B + ib] = w.y;
-            d.bnd_wgt[2 * B + ib] = w.z;
-        }
-    }
+    std::string e = boundary_subfaces(mesh, bface, d);
+    if (!e.empty()) return e;
 
     // ---- least-squares gradient weights (geom_tet.rs:261-293)
     d.gw.assign(3 * D, 0.0);

@@ -73,6 +73,10 @@ std::string delaunay(Mesh& mesh);
 constexpr double kDualPieceStoreBytes = 8.0 * 1024 * 1024 * 1024;
 std::string build_dual(const Mesh& mesh, Dual& dual, double piece_store_bytes = kDualPieceStoreBytes);
 
+// Boundary sub-faces of the faces flagged in bface (4 per tetrahedron); part of build_dual, shared
+// with the device dual. Returns "" on success.
+std::string boundary_subfaces(const Mesh& mesh, const std::vector<uint8_t>& bface, Dual& dual);
+
 // exact orientation / in-sphere signs on the quantised grid (exported for tests)
 int orient_sign(const double* a, const double* b, const double* c, const double* d);
 int insphere_sign(const double* a, const double* b, const double* c, const double* d, const double* e);

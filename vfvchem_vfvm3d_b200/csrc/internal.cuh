@@ -86,24 +86,15 @@ struct IluStruct {
     uint64_t version64 = ~0ull, version32 = ~0ull;
 
     // single-launch sweeps (k_ilu0_chain): row tasks inside levels (row starts, levels, tasks per
-    // level), and per precision a work vector for standalone applies, the claim and completion
-    // counters and a host-mapped timeout flag for standalone applies
+    // level), and per precision a work vector for standalone applies and the claim and completion
+    // counters
     DBuf<int32_t> tasks, task_lev, lev_ntask;
     int ntask = 0;
     struct Chain {
         DBuf<unsigned char> work;   // n entries of the precision (standalone applies)
         DBuf<unsigned char> state;  // IluChainState + 2 nlev completion counters
-        int* h_flag = nullptr;      // pinned, mapped: set by a wait that gave up
-        int* d_flag = nullptr;
         int grid = 0;
     } chain[2];                     // [0] double, [1] float
-    IluStruct() = default;
-    IluStruct(const IluStruct&) = delete;
-    IluStruct& operator=(const IluStruct&) = delete;
-    ~IluStruct() {
-        for (auto& c : chain)
-            if (c.h_flag) cudaFreeHost(c.h_flag);
-    }
 };
 
 struct SolverBase {
@@ -141,6 +132,11 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
               bool batched = false);
 // per-mesh Arnoldi steps of the last batched solve with these options
 bool batch_mesh_steps(const vfv_pattern* p, const vfv_gmres_opts* o, std::vector<int32_t>& steps);
+// the Voronoi dual of a mesh's tetrahedra computed on the device of ctx (same arrays, bit for bit,
+// as the host build_dual); "" on success (csrc/kernels/dual.cu)
+namespace vfv {
+std::string build_dual_device(vfv_ctx* ctx, const Mesh& mesh, Dual& d);
+}
 // argument checks of the reference's LinearGmres constructor and solve options
 int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o);
 // transpose of a pattern (tmap: slot in A of every entry of A^T) and the gather of A's values into it

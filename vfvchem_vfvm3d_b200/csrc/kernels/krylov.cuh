@@ -22,8 +22,8 @@ namespace vfv {
 
 constexpr int kBlk = 256;        // threads per block of the vector kernels
 constexpr int kRows = 4;         // rows per thread in the multi-vector kernels
-constexpr int kVecMinBlocks = 8; // <= 32 registers: 8 x 256 threads per SM, so the 977 blocks of a
-                                 // 10^6-row vector fit in one wave of 148 SMs (no tail wave)
+constexpr int kVecMinBlocks = 4; // <= 64 registers: room for the loads of kVecGroup basis vectors
+constexpr int kVecGroup = 4;     // basis vectors whose rows a thread loads before using any of them
 constexpr int kMaxBasis = 128;   // m + 1 <= kMaxBasis
 
 // Per-solve device workspace pointers used by the Krylov kernels.
@@ -193,6 +193,91 @@ __global__ void __launch_bounds__(kBlk) k_residual(KrylovDev K, const int32_t* _
     }
 }
 
+// ---------------------------------------------------------------- grouped multi-vector passes
+// A thread owns kRows rows (stride kBlk) of a block; rows past `end` read as zero. The basis rows
+// of kVecGroup vectors are loaded before any of them is used, so a thread keeps 16 loads in flight
+// instead of 4 between dependent warp reductions. Per vector and row the arithmetic (and its
+// order) is that of one vector at a time.
+
+// red[i][warp] = this warp's partial of <u_i, wr> for i < nvec
+template <typename T>
+__device__ __forceinline__ void group_dots(const T* __restrict__ V, int64_t ldv, int64_t base, int64_t end, const double* wr, int nvec,
+                                           double (*red)[kBlk / 32]) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const bool full = base + (kRows - 1) * kBlk < end;
+    int i = 0;
+    for (; i + kVecGroup <= nvec; i += kVecGroup) {
+        T x[kVecGroup][kRows];
+#pragma unroll
+        for (int q = 0; q < kVecGroup; ++q)
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) {
+                const int64_t row = base + r * kBlk;
+                x[q][r] = (full || row < end) ? V[(int64_t)(i + q) * ldv + row] : T(0);
+            }
+        double sq[kVecGroup];
+#pragma unroll
+        for (int q = 0; q < kVecGroup; ++q) {
+            sq[q] = 0.0;
+#pragma unroll
+            for (int r = 0; r < kRows; ++r)
+                if (full || base + r * kBlk < end) sq[q] += (double)x[q][r] * wr[r];
+        }
+#pragma unroll
+        for (int q = 0; q < kVecGroup; ++q) {
+            const double t = warp_sum(sq[q]);
+            if (lane == 0) red[i + q][wid] = t;
+        }
+    }
+    for (; i < nvec; ++i) {
+        const T* u = V + (int64_t)i * ldv;
+        double sv = 0.0;
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+            const int64_t row = base + r * kBlk;
+            if (row < end) sv += (double)u[row] * wr[r];
+        }
+        sv = warp_sum(sv);
+        if (lane == 0) red[i][wid] = sv;
+    }
+}
+
+// acc[r] = sum_i coef[i] u_i[row_r] for i < nvec, i in order
+template <typename T>
+__device__ __forceinline__ void group_combine(const T* __restrict__ V, int64_t ldv, int64_t base, int64_t end, const double* coef, int nvec,
+                                              double* acc) {
+    const bool full = base + (kRows - 1) * kBlk < end;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) acc[r] = 0.0;
+    int i = 0;
+    for (; i + kVecGroup <= nvec; i += kVecGroup) {
+        T x[kVecGroup][kRows];
+#pragma unroll
+        for (int q = 0; q < kVecGroup; ++q)
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) {
+                const int64_t row = base + r * kBlk;
+                x[q][r] = (full || row < end) ? V[(int64_t)(i + q) * ldv + row] : T(0);
+            }
+#pragma unroll
+        for (int q = 0; q < kVecGroup; ++q) {
+            const double c = coef[i + q];
+#pragma unroll
+            for (int r = 0; r < kRows; ++r)
+                if (full || base + r * kBlk < end) acc[r] += c * (double)x[q][r];
+        }
+    }
+    for (; i < nvec; ++i) {
+        const T* u = V + (int64_t)i * ldv;
+        const double c = coef[i];
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+            const int64_t row = base + r * kBlk;
+            if (row < end) acc[r] += c * (double)u[row];
+        }
+    }
+}
+
 // ---------------------------------------------------------------- multi-dot (first CGS pass)
 // Per-block partials of d_i = <u_i, w> for i < nvec (k_dots_finish<true> completes them).
 template <typename T>
@@ -208,17 +293,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_mdot(KrylovDev K, const
         const int64_t row = base + r * kBlk;
         wr[r] = row < K.n ? (double)w[row] : 0.0;
     }
-    for (int i = 0; i < nvec; ++i) {
-        const T* u = V + (int64_t)i * K.ldv;
-        double s = 0.0;
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            const int64_t row = base + r * kBlk;
-            if (row < K.n) s += (double)u[row] * wr[r];
-        }
-        s = warp_sum(s);
-        if (lane == 0) red[i][wid] = s;
-    }
+    group_dots(V, K.ldv, base, K.n, wr, nvec, red);
     __syncthreads();
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
         double s = 0.0;
@@ -322,20 +397,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, con
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * (kBlk * kRows) + threadIdx.x;
     double acc[kRows];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) acc[r] = 0.0;
-    // the second CGS pass (FINAL == false) keeps four basis vectors' loads in flight per thread;
-    // the last pass does better without (its occupancy is the limit)
-#pragma unroll(FINAL ? 1 : 4)
-    for (int i = 0; i < nvec; ++i) {
-        const T* u = V + (int64_t)i * K.ldv;
-        const double c = s_coef[i];
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            const int64_t row = base + r * kBlk;
-            if (row < K.n) acc[r] += c * (double)u[row];
-        }
-    }
+    group_combine(V, K.ldv, base, K.n, s_coef, nvec, acc);
     double wr[kRows];
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
@@ -349,17 +411,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, con
         }
     }
     if (!FINAL) {
-        for (int i = 0; i < nvec; ++i) {
-            const T* u = V + (int64_t)i * K.ldv;
-            double s = 0.0;
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const int64_t row = base + r * kBlk;
-                if (row < K.n) s += (double)u[row] * wr[r];
-            }
-            s = warp_sum(s);
-            if (lane == 0) red[i][wid] = s;
-        }
+        group_dots(V, K.ldv, base, K.n, wr, nvec, red);
         __syncthreads();
         for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
             double s = 0.0;
@@ -394,18 +446,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_zupdate(KrylovDev K, T*
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * (kBlk * kRows) + threadIdx.x;
     double acc[kRows];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) acc[r] = 0.0;
-#pragma unroll 4
-    for (int i = 0; i < nvec; ++i) {
-        const T* z = Z + (int64_t)i * K.ldv;
-        const double c = s_c[i];
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            const int64_t row = base + r * kBlk;
-            if (row < K.n) acc[r] += c * (double)z[row];
-        }
-    }
+    group_combine(Z, K.ldv, base, K.n, s_c, nvec, acc);
     T* out = Z + (int64_t)(j + 1) * K.ldv;
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {

@@ -218,17 +218,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_bmdot(BatchDev B, const
         const int64_t row = base + r * kBlk;
         wr[r] = row < end ? (double)w[row] : 0.0;
     }
-    for (int i = 0; i < nvec; ++i) {
-        const T* u = V + (int64_t)i * B.ldv;
-        double s = 0.0;
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            const int64_t row = base + r * kBlk;
-            if (row < end) s += (double)u[row] * wr[r];
-        }
-        s = warp_sum(s);
-        if (lane == 0) red[i][wid] = s;
-    }
+    group_dots(V, B.ldv, base, end, wr, nvec, red);
     __syncthreads();
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
         double s = 0.0;
@@ -289,18 +279,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_bupdate(BatchDev B, con
     __syncthreads();
     const int64_t base = B.tile_row[t] + threadIdx.x, end = B.tile_row[t + 1];
     double acc[kRows];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) acc[r] = 0.0;
-#pragma unroll(FINAL ? 1 : 4)
-    for (int i = 0; i < nvec; ++i) {
-        const T* u = V + (int64_t)i * B.ldv;
-        const double c = s_coef[i];
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            const int64_t row = base + r * kBlk;
-            if (row < end) acc[r] += c * (double)u[row];
-        }
-    }
+    group_combine(V, B.ldv, base, end, s_coef, nvec, acc);
     double wr[kRows];
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
@@ -314,17 +293,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_bupdate(BatchDev B, con
         }
     }
     if (!FINAL) {
-        for (int i = 0; i < nvec; ++i) {
-            const T* u = V + (int64_t)i * B.ldv;
-            double s = 0.0;
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const int64_t row = base + r * kBlk;
-                if (row < end) s += (double)u[row] * wr[r];
-            }
-            s = warp_sum(s);
-            if (lane == 0) red[i][wid] = s;
-        }
+        group_dots(V, B.ldv, base, end, wr, nvec, red);
         __syncthreads();
         for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
             double s = 0.0;

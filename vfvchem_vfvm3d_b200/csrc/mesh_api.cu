@@ -2,6 +2,7 @@
 // the Delaunay tetrahedra and the Voronoi dual (host code: csrc/host/mesh.cpp).
 #include "internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 
 #include <cstdlib>
@@ -71,6 +72,53 @@ int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, cons
 }
 
 void vfv_mesh_destroy(vfv_mesh* m) { delete m; }
+
+int vfv_mesh_dual_device(vfv_ctx* ctx, vfv_mesh* m) {
+    if (!ctx || !m) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (m->m.tets.empty()) return set_err(ctx, VFV_BAD_INPUT, "mesh has no tetrahedra");
+    Dual d;
+    const std::string e = build_dual_device(ctx, m->m, d);
+    if (!e.empty()) return set_err(ctx, e.rfind("dual on the device", 0) == 0 ? VFV_CUDA_ERROR : VFV_BAD_INPUT, e);
+    m->d = std::move(d);
+    return VFV_OK;
+}
+
+int vfv_mesh_jitter_cubes_device_dual(vfv_ctx* ctx, int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out) {
+    if (!ctx || count <= 0 || !n || !seeds || !out) return set_err(ctx, VFV_BAD_INPUT, "invalid batch arguments");
+    for (int i = 0; i < count; ++i) {
+        out[i] = nullptr;
+        if (n[i] < 3 || n[i] > 400) return set_err(ctx, VFV_BAD_INPUT, "grid size n must be in [3, 400]");
+    }
+    if (!(jitter >= 0.0 && jitter < 0.5)) return set_err(ctx, VFV_BAD_INPUT, "jitter must be in [0, 0.5)");
+    std::vector<std::string> errs(count);
+    std::vector<vfv_mesh*> made(count, nullptr);
+    // Delaunay of the meshes in parallel on the host, largest first
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int t = 0; t < count; ++t) {
+        const int i = order[t];
+        auto* mh = new vfv_mesh();
+        mh->m = make_jitter_cube(n[i], seeds[i], jitter);
+        errs[i] = delaunay(mh->m);
+        made[i] = mh;
+    }
+    int rc = VFV_OK;
+    for (int i = 0; i < count && rc == VFV_OK; ++i) {
+        if (!errs[i].empty()) {
+            rc = set_err(ctx, VFV_BAD_INPUT, errs[i]);
+            break;
+        }
+        rc = vfv_mesh_dual_device(ctx, made[i]);  // the duals one after the other on the device
+    }
+    if (rc != VFV_OK) {
+        for (vfv_mesh* mh : made) delete mh;
+        return rc;
+    }
+    for (int i = 0; i < count; ++i) out[i] = made[i];
+    return VFV_OK;
+}
 
 int vfv_mesh_jitter_cubes(int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out) {
     if (count <= 0 || !n || !seeds || !out) return set_err(nullptr, VFV_BAD_INPUT, "invalid batch arguments");

@@ -49,6 +49,27 @@ class Mesh:
         return [cls(C.c_void_p(out[i])) for i in range(ns.size)]
 
     @classmethod
+    def jitter_cubes_device_dual(cls, ctx, ns, seeds, jitter: float = 0.25) -> list["Mesh"]:
+        """As :meth:`jitter_cubes`, with the Voronoi duals built on the device of ``ctx`` (same bits)."""
+        ns = np.ascontiguousarray(ns, dtype=np.int32)
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+        out = (C.c_void_p * ns.size)()
+        code = L.load().vfv_mesh_jitter_cubes_device_dual(ctx.handle, int(ns.size), L.ptr(ns, C.c_int32), L.ptr(seeds, C.c_uint64),
+                                                           float(jitter), out)
+        if code != 0:
+            msg = L.load().vfv_last_error(ctx.handle)
+            raise_for(code, msg.decode() if msg else f"status {code}")
+        return [cls(C.c_void_p(out[i])) for i in range(ns.size)]
+
+    def build_dual_device(self, ctx) -> None:
+        """Recompute this mesh's dual on the device of ``ctx`` (replaces the host-built one; same bits)."""
+        code = L.load().vfv_mesh_dual_device(ctx.handle, self._h)
+        if code != 0:
+            msg = L.load().vfv_last_error(ctx.handle)
+            raise_for(code, msg.decode() if msg else f"status {code}")
+        self._dual = None
+
+    @classmethod
     def from_vertices(cls, pos: np.ndarray, n_pts: int, node_bnd: np.ndarray) -> "Mesh":
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
         node_bnd = np.ascontiguousarray(node_bnd, dtype=np.int32)

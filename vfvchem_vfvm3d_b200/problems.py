@@ -78,13 +78,15 @@ class TransportBatch:
 
 
 def transport_batch(count: int = 256, nmin: int = 2000, nmax: int = 50000, seed: int = 4, D: float = 1e-3, dt: float = 1e-2,
-                    steps: int = 100) -> TransportBatch:
+                    steps: int = 100, dual_ctx=None) -> TransportBatch:
     """Transport batch: `count` jittered cubes with vertex counts N_i drawn log-uniform in [nmin, nmax]
-    (numpy PCG64, `seed`), n_i = round(N_i^(1/3)) grid points per axis, mesh seeds 1000 + i."""
+    (numpy PCG64, `seed`), n_i = round(N_i^(1/3)) grid points per axis, mesh seeds 1000 + i. With
+    `dual_ctx` the Voronoi duals are built on that context's device (same bits as on the host)."""
     rng = np.random.default_rng(seed)
     N = np.exp(rng.uniform(np.log(nmin), np.log(nmax), count))
     n = np.maximum(3, np.rint(np.cbrt(N))).astype(np.int32)
-    meshes = Mesh.jitter_cubes(n, 1000 + np.arange(count, dtype=np.uint64))
+    seeds = 1000 + np.arange(count, dtype=np.uint64)
+    meshes = Mesh.jitter_cubes_device_dual(dual_ctx, n, seeds) if dual_ctx is not None else Mesh.jitter_cubes(n, seeds)
     return TransportBatch(meshes, n, D, dt, steps)
 
 
