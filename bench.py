@@ -13,9 +13,14 @@ system: FP64 restarted GMRES(50) with a natural-order ILU(0), driven to relres 1
 not finish on 10^6 rows in bench time; that oracle solver agrees with SuperLU to 1.0e-11 at 125,000
 rows).
 
-`roofline` is the kernel with the largest share of the mixed solve's kernel time (the single-launch
-ILU(0) sweeps), timed alone with CUDA events on the library's stream; `roofline_spmv` is the FP64
-SpMV timed the same way.
+The mixed solver's preconditioner is ILU(0) in the natural order with its triangular solves done
+as ILU_SWEEPS Jacobi sweeps of each factor (bandwidth-bound launches over compact triangles); the
+plain FP64 solver is the exact multicolour ILU(0) (level-scheduled sweeps). The FP64 solver with
+the same swept preconditioner and the mixed solver with the exact one are timed beside them.
+
+`roofline` is the kernel with the largest share of the mixed solve's kernel time (the float
+Jacobi sweeps of the factors), timed alone with CUDA events on the library's stream;
+`roofline_spmv` is the FP64 SpMV timed the same way.
 
 `--impl reference` times the reference's own algorithm for this path on the host cores
 (Jacobi-preconditioned restarted GMRES(50), FP64, the oracle port) to the same relres.
@@ -81,43 +86,9 @@ def extras_adjoint(heat, prob, x_ref_h, ctx):
     return out
 
 
-def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16):
-    """Central finite differences of J on the device (assembly + FP64 GMRES(50)+ILU(0) to relres
-    1e-14, warm-started from the base state) along seeded directions e = (e_logk, e_q) with i.i.d.
-    N(0, 1) entries, against the adjoint gradient at the same state: step h = 1e-6 on `ndir`
-    directions, and h = 1e-4 on the first `ndir_wide`. Faces whose skew-corrected face conductivity
-    sits within 1e-4 k_m of the k_f > 0 guard (opscl_dom_diff.rs:80) are counted: a difference
-    quotient across that kink is not a derivative."""
-    from vfvchem_vfvm3d_b200 import GmresOptions
-    from vfvchem_vfvm3d_b200 import _lib as L
-    fo = GmresOptions(tol=1e-14, restart=50, max_outer=4000, precond=L.PRECOND_ILU0)
-    logk, q = np.log(prob.k), prob.q
-
-    def solve_J(lk, qq, x0):
-        b = heat.assemble(np.exp(lk), qq, prob.s, prob.T0, prob.bc_val)
-        x, _ = heat.pattern.solve(b, x0, fo)
-        r = x[sens] - d
-        return 0.5 * float(r @ r), x
-
-    t0 = time.perf_counter()
-    J0, T = solve_J(logk, q, prob.T0)
-    g = np.zeros(prob.n)
-    g[sens] = T[sens] - d
-    _, dk, dq, _ = heat.adjoint(T, g, fo)
-    res = {}
-    for h, nd in ((1e-6, ndir), (1e-4, ndir_wide)):
-        errs = []
-        r2 = np.random.default_rng(64)
-        for _ in range(nd):
-            ek, eq = r2.standard_normal(prob.n), r2.standard_normal(prob.n)
-            jp, _ = solve_J(logk + h * ek, q + h * eq, T)
-            jm, _ = solve_J(logk - h * ek, q - h * eq, T)
-            fd = (jp - jm) / (2 * h)
-            ad = float(dk @ ek + dq @ eq)
-            errs.append(abs(fd - ad) / abs(ad))
-        res[f"h={h:g}"] = {"directions": nd, "median_rel": float(np.median(errs)), "max_rel": float(np.max(errs))}
-    heat.assemble(prob.k, prob.q, prob.s, prob.T0, prob.bc_val)  # leave the base system assembled
-    # faces near the k_f > 0 guard of the face conductivity
+def guard_faces(heat, prob):
+    """Skew-corrected face conductivities k_f of every directed face (opscl_dom_diff.rs:80 guards
+    k_f > 0) with the harmonic means k_m, the face owners and neighbours."""
     dual = prob.mesh.dual()
     gk = heat.grad(prob.k)
     npt = dual["nbr_ptr"]
@@ -127,10 +98,88 @@ def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16):
     km = 2.0 * kv * kn / (kv + kn)
     sk = np.asarray(dual["skew"]).reshape(3, -1)
     kf = km + 0.5 * (sk[0] * (gk[0][v] + gk[0][nb]) + sk[1] * (gk[1][v] + gk[1][nb]) + sk[2] * (gk[2][v] + gk[2][nb]))
-    res.update({"J": J0, "directions": "i.i.d. N(0,1) entries over all 2 x 10^6 parameters (log k, q), seed 64",
-                "forward": "device assembly + FP64 GMRES(50)+ILU(0) to relres 1e-14, warm start from the base state",
+    return kf, km, v, nb, npt
+
+
+def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16, band=1e-2):
+    """Central finite differences of J on the device forward model (assembly + FP64 GMRES(50)+ILU(0)
+    to relres 1e-14) along seeded directions e = (e_logk, e_q), against the adjoint gradient at the
+    same state: step h = 1e-6 on `ndir` directions, h = 1e-4 on the first `ndir_wide`.
+
+    The forward model is only piecewise smooth: a face conductivity k_f is clamped at the k_f > 0
+    guard (opscl_dom_diff.rs:80), and k_f depends on k of the face's vertices and, through the
+    least-squares gradients, of their neighbours. A perturbation of every log k moves the faces
+    that sit near the guard across it, and a difference quotient across that kink is not a
+    derivative. So e_q has i.i.d. N(0, 1) entries everywhere, and e_logk has them everywhere except
+    on the vertices whose k enters a face with |k_f| <= band * k_m (the face's two vertices and
+    their neighbours), where it is zero; the counts are reported.
+
+    The difference J(p + h e) - J(p - h e) is formed without cancellation: with T the computed
+    base state, the solutions at p +- h e are T + delta+- where A+- delta+- = b+- - A+- T (the
+    residual of T in each perturbed system, a vector of size ~h, solved to relres 1e-14 of its own
+    norm). T + delta+- is the perturbed solution whatever error T carries, so J+ - J- =
+    sum_s (T_s - d_s) (delta+_s - delta-_s) + (delta+_s^2 - delta-_s^2) / 2 over the sensors."""
+    import torch
+    from vfvchem_vfvm3d_b200 import GmresOptions
+    from vfvchem_vfvm3d_b200 import _lib as L
+    fo = GmresOptions(tol=1e-14, restart=50, max_outer=4000, precond=L.PRECOND_ILU0)
+    logk, q = np.log(prob.k), prob.q
+    pat = heat.pattern
+    xd = torch.empty(prob.n, dtype=torch.float64, device="cuda")
+    yd = torch.empty_like(xd)
+
+    kf, km, v, nb, npt = guard_faces(heat, prob)
+    near = np.abs(kf) <= band * km
+    touched = np.zeros(prob.n, bool)
+    touched[v[near]] = True
+    touched[nb[near]] = True
+    free = ~touched.copy()
+    for u in np.nonzero(touched)[0]:  # neighbours of the face vertices enter their gradients
+        free[nb[npt[u]:npt[u + 1]]] = False
+
+    def assemble(lk, qq):
+        return heat.assemble(np.exp(lk), qq, prob.s, prob.T0, prob.bc_val)
+
+    def solve(b, x0):
+        x, _ = pat.solve(b, x0, fo)
+        return x
+
+    def residual(b, x):  # b - A x with the pattern's current values (device SpMV, FP64)
+        xd.copy_(torch.from_numpy(x))
+        torch.cuda.synchronize()
+        pat.spmv_device(xd.data_ptr(), yd.data_ptr())
+        heat.ctx.synchronize()
+        return b - yd.cpu().numpy()
+
+    t0 = time.perf_counter()
+    T = solve(assemble(logk, q), prob.T0)
+    r0 = T[sens] - d
+    J0 = 0.5 * float(r0 @ r0)
+    g = np.zeros(prob.n)
+    g[sens] = r0
+    _, dk, dq, _ = heat.adjoint(T, g, fo)
+    res = {}
+    for h, nd in ((1e-6, ndir), (1e-4, ndir_wide)):
+        errs = []
+        r2 = np.random.default_rng(64)
+        for _ in range(nd):
+            ek, eq = r2.standard_normal(prob.n) * free, r2.standard_normal(prob.n)
+            dm = solve(residual(assemble(logk - h * ek, q - h * eq), T), np.zeros(prob.n))[sens]
+            dp = solve(residual(assemble(logk + h * ek, q + h * eq), T), np.zeros(prob.n))[sens]
+            fd = float(r0 @ (dp - dm) + 0.5 * (dp @ dp - dm @ dm)) / (2 * h)
+            ad = float(dk @ ek + dq @ eq)
+            errs.append(abs(fd - ad) / abs(ad))
+        res[f"h={h:g}"] = {"directions": nd, "median_rel": float(np.median(errs)), "max_rel": float(np.max(errs))}
+    res["fd_median_rel"] = res["h=1e-06"]["median_rel"]
+    res["fd_max_rel"] = res["h=1e-06"]["max_rel"]
+    heat.assemble(prob.k, prob.q, prob.s, prob.T0, prob.bc_val)  # leave the base system assembled
+    res.update({"J": J0, "directions": f"seed 64: e_q i.i.d. N(0,1) on all {prob.n} vertices; e_logk i.i.d. N(0,1) on the "
+                                       f"{int(free.sum())} vertices whose k enters no face with |k_f| <= {band:g} k_m, 0 on the "
+                                       f"other {int((~free).sum())}",
+                "forward": "device assembly + FP64 GMRES(50)+ILU(0) to relres 1e-14; J+ - J- from correction solves of the "
+                           "base state in both perturbed systems (no cancellation)",
                 "faces_guard_active": int(np.sum(kf <= 0.0)), "faces_near_guard_1e-4": int(np.sum(np.abs(kf) <= 1e-4 * km)),
-                "directed_faces": int(nb.size), "seconds": time.perf_counter() - t0})
+                f"faces_near_guard_{band:g}": int(near.sum()), "directed_faces": int(nb.size), "seconds": time.perf_counter() - t0})
     return res
 
 
@@ -213,8 +262,9 @@ def extras_transport(ctx, count):
 # lanes per row, from one ncu capture of that launch (profiles/k_spmv_1M.md); reported as the
 # roofline's traffic only when the bench runs that same matrix and lane count.
 SPMV_TRAFFIC_N100_4LANES = 209.2e6
-# DRAM bytes (read + write) of one k_ilu0_chain<float> launch on the same matrix (set from an ncu capture)
-ILU_TRAFFIC_N100 = None
+# DRAM bytes (read + write) of one k_ilu0_sweep<float> launch on the same matrix, averaged over the
+# launches of one apply (set from an ncu capture)
+SWEEP_TRAFFIC_N100 = None
 
 
 def peaks():
@@ -271,6 +321,7 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+ILU_SWEEPS = 4      # Jacobi sweeps per ILU(0) factor in the mixed solver's preconditioner
 TOL_RELRES = 1e-12  # stopping rule of every solver in both arms: ||b - A x|| <= TOL_RELRES ||b||
 REF_TOL = 1e-14     # the oracle's reference solution
 
@@ -367,9 +418,12 @@ def main():
             return None
         return float(torch.linalg.vector_norm(x - x_ref_d) / torch.linalg.vector_norm(x_ref_d))
 
-    ilu = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_MULTICOLOR, engine=args.engine)
-    o64 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, **ilu)
-    omx = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, **ilu)
+    exact = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_MULTICOLOR, engine=args.engine)
+    swept = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_NATURAL, ilu_sweeps=ILU_SWEEPS, engine=args.engine)
+    o64 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, **exact)
+    omx = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, **swept)
+    o64s = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, **swept)
+    omxe = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, **exact)
 
     def timed(opts, steps, warm):
         for _ in range(warm):
@@ -391,11 +445,15 @@ def main():
         t_mx, i_mx, e_mx = timed(omx, args.steps, args.warmup)
         launches_mx = (ctx.launch_count - launches0) // (args.steps + args.warmup) * args.steps
         t_64, i_64, e_64 = timed(o64, args.steps, args.warmup)
+        t_64s, i_64s, e_64s = timed(o64s, args.steps, args.warmup)
+        t_mxe, i_mxe, e_mxe = timed(omxe, args.steps, args.warmup)
     torch.cuda.synchronize()
     mx_s = sum(t_mx) / len(t_mx)
     f64_s = sum(t_64) / len(t_64)
+    f64s_s = sum(t_64s) / len(t_64s)
+    mxe_s = sum(t_mxe) / len(t_mxe)
     replicas.barrier(R)
-    mx_s, f64_s = replicas.max_over_ranks(R, [mx_s, f64_s])
+    mx_s, f64_s, f64s_s, mxe_s = replicas.max_over_ranks(R, [mx_s, f64_s, f64s_s, mxe_s])
 
     # SpMV (FP64 and FP32) timed alone: the kernel the metric names
     xs = torch.randn(n, dtype=torch.float64, device=dev)
@@ -422,16 +480,24 @@ def main():
     gbs64 = bytes64 / sp64 / 1e9
     gbs32 = bytes32 / sp32 / 1e9
 
-    # ILU(0) sweeps with the float factor (one k_ilu0_chain launch per apply), timed alone: the
-    # mixed solve's preconditioner. Algorithmic bytes per apply: L+U values and columns (8 nnz), row
-    # pointer, diagonal position and permutation per sweep (2 x 12 n), r in and z out (8 n), the
-    # next launch's work vectors refilled (8 n); the gathered solved values stay in L2.
+    # The mixed solve's preconditioner timed alone: ILU_SWEEPS Jacobi sweeps of each float factor
+    # (natural-order ILU(0) in A's numbering; 2 x ILU_SWEEPS k_ilu0_sweep launches per apply).
+    # Algorithmic bytes per sweep: the triangle's row pointer (4 (n+1)), column indices (2 or 4
+    # bytes) and float values (4) of its entries (nl = nu = (nnz - n) / 2 strictly lower / upper
+    # entries), right-hand side, previous iterate and new iterate (12 n), the diagonal for the upper
+    # sweeps (4 n); the last lower sweep also writes D^-1 u (4 n) and reads the diagonal (4 n).
     rs32, ts32, zs32 = xs32.clone(), torch.empty_like(xs32), torch.empty_like(xs32)
     torch.cuda.synchronize()
-    ilu_nlev = pat.ilu0_apply_device_f32(rs32.data_ptr(), ts32.data_ptr(), zs32.data_ptr())
-    ilu_s = kernel_time(lambda: pat.ilu0_apply_device_f32(rs32.data_ptr(), ts32.data_ptr(), zs32.data_ptr()), reps=50)
-    bytes_ilu32 = 8 * nnz + 36 * n
+    pat.ilu0_sweep_apply_device(rs32.data_ptr(), zs32.data_ptr(), ILU_SWEEPS, L.ILU_NATURAL, f32=True)
+    ilu_s = kernel_time(lambda: pat.ilu0_sweep_apply_device(rs32.data_ptr(), zs32.data_ptr(), ILU_SWEEPS, L.ILU_NATURAL, f32=True))
+    col_bytes = pat.ilu0_sweep_layout(L.ILU_NATURAL)
+    ilu_launches = 2 * ILU_SWEEPS
+    ntri = (nnz - n) // 2
+    bytes_ilu32 = ILU_SWEEPS * (2 * 4 * (n + 1) + (col_bytes + 4) * 2 * ntri + 28 * n) + 8 * n
     gbs_ilu32 = bytes_ilu32 / ilu_s / 1e9
+    # the exact level-scheduled float apply (the FP64 baseline's preconditioner structure), for context
+    ilu_nlev = pat.ilu0_apply_device_f32(rs32.data_ptr(), ts32.data_ptr(), zs32.data_ptr())
+    lev_s = kernel_time(lambda: pat.ilu0_apply_device_f32(rs32.data_ptr(), ts32.data_ptr(), zs32.data_ptr()))
 
     # assembly (gradients + face coefficients + b), timed alone
     def asm():
@@ -487,14 +553,24 @@ def main():
         "config": bench_config(args, world),
         "fp64_solve_s": f64_s,
         "speedup_mixed_vs_fp64": f64_s / mx_s,
-        "iters_mixed": i_mx[-1].iters, "iters_fp64": i_64[-1].iters, "ilu_levels": i_mx[-1].levels,
-        "err_mixed": e_mx, "err_fp64": e_64, "err_target": ERR_TARGET,
+        "solvers": {
+            "mixed": f"FP32 GMRES({args.restart}) cycles in FP64 refinement, ILU(0) natural order, {ILU_SWEEPS} Jacobi sweeps per factor",
+            "fp64": f"FP64 GMRES({args.restart}), exact multicolour ILU(0) ({ilu_nlev} colour levels, level-scheduled sweeps)",
+            "fp64_same_precond": "FP64 GMRES with the mixed solver's preconditioner",
+            "mixed_exact_ilu": "the mixed solver with the FP64 solver's exact multicolour ILU(0)"},
+        "fp64_same_precond_s": f64s_s, "speedup_mixed_vs_fp64_same_precond": f64s_s / mx_s,
+        "mixed_exact_ilu_s": mxe_s,
+        "iters_mixed": i_mx[-1].iters, "iters_fp64": i_64[-1].iters, "iters_fp64_same_precond": i_64s[-1].iters,
+        "iters_mixed_exact_ilu": i_mxe[-1].iters, "ilu_levels": ilu_nlev,
+        "err_mixed": e_mx, "err_fp64": e_64, "err_fp64_same_precond": e_64s, "err_mixed_exact_ilu": e_mxe, "err_target": ERR_TARGET,
         "nnz": nnz, "engine": args.engine,
-        "roofline": {"bound": "hbm", "kernel": f"k_ilu0_chain<float> (both sweeps, {ilu_nlev} colour levels, one launch per apply)",
+        "roofline": {"bound": "hbm", "kernel": f"k_ilu0_sweep<float> (Jacobi sweeps of the ILU(0) factors, {ilu_launches} launches per apply, "
+                                                f"{col_bytes}-byte columns)",
                      "achieved": gbs_ilu32, "peak": peak, "unit": "GB/s", "frac": gbs_ilu32 / peak, "peak_kind": peak_kind,
-                     "traffic": ILU_TRAFFIC_N100 if args.n == 100 else None,
+                     "traffic": SWEEP_TRAFFIC_N100 if args.n == 100 else None,
                      "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
-                     "algorithmic_bytes_per_apply": bytes_ilu32, "apply_us": ilu_s * 1e6},
+                     "algorithmic_bytes_per_launch": bytes_ilu32 / ilu_launches, "apply_us": ilu_s * 1e6,
+                     "exact_level_apply_us": lev_s * 1e6},
         "roofline_spmv": {"bound": "hbm", "kernel": f"k_spmv<double> (CSR, {lanes64} lanes/row, {strides64} strides/lane)", "achieved": gbs64, "peak": peak, "unit": "GB/s",
                           "frac": gbs64 / peak, "peak_kind": peak_kind,
                           "traffic": SPMV_TRAFFIC_N100_4LANES if (args.n == 100 and (lanes64, strides64) == (4, 4)) else None,

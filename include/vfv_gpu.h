@@ -80,6 +80,11 @@ typedef struct {
                            ends after 2 s): the persistent engine's grid barriers and the single-launch
                            ILU(0) sweeps. A wait that gives up makes the solve return VFV_TIMEOUT and
                            leaves the context usable. */
+    int32_t ilu_sweeps; /* ILU(0) only: 0 = exact triangular solves (level-scheduled sweeps); k in [1, 16] = k Jacobi
+                           sweeps of each factor instead (u = y - N u and w = D^-1 (u - S w), k times each, for
+                           L = I + N, U = D + S; Anzt, Chow & Dongarra 2015): a fixed linear preconditioner whose
+                           sweeps are one bandwidth-bound launch each. With VFV_ILU_NATURAL they run in A's own
+                           numbering. Graph and overlapped engines only. */
 } vfv_gmres_opts;
 
 typedef struct {
@@ -148,6 +153,15 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
  * for measurement: enqueued on the context's stream without synchronising; t is a work vector of n
  * floats that must not alias r or z (r and z may alias). */
 int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const float* r, float* t, float* z, int32_t* levels);
+/* z = M^-1 r with `sweeps` (1..16) Jacobi sweeps of each ILU(0) factor (vfv_gmres_opts::ilu_sweeps),
+ * in double or with the float copy of the factor; enqueued on the context's stream without
+ * synchronisation (calls after the first for a pattern, ordering and precision allocate nothing).
+ * r and z may alias. */
+int vfv_ilu0_sweep_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const double* r, double* z);
+int vfv_ilu0_sweep_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const float* r, float* z);
+/* Storage of the swept factors once built: bytes per column index (2: 16-bit offsets from the row,
+ * when the factor's bandwidth allows; 4: absolute). */
+int vfv_ilu0_sweep_layout(const vfv_pattern* p, int ilu_order, int32_t* col_bytes);
 /* Same result as vfv_ilu0_apply_device, allocating nothing. No counterpart in the reference: for
  * callers that may not allocate device memory while they run (a time-step loop under a fixed
  * memory budget, a host framework whose allocator owns the device memory, code that must not

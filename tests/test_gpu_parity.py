@@ -227,6 +227,97 @@ def test_ilu0_apply_f32_matches_oracle(gpu_ctx, c1h_system, c1_hetero):
         p.ilu0_apply_device_f32(rd.data_ptr(), rd.data_ptr(), zd.data_ptr())
 
 
+@pytest.mark.parametrize("sweeps", [1, 3])
+@pytest.mark.parametrize("order", [0, 1])
+def test_ilu0_sweep_apply_matches_oracle(gpu_ctx, c1h_system, c1_hetero, order, sweeps):
+    """Jacobi sweeps of the ILU(0) factors (double and float), against the oracle's restatement on
+    the same factor; the natural ordering runs in A's numbering, the multicolour one permuted.
+    Repeat calls give identical bits; r and z may alias."""
+    import torch
+    from vfvchem_vfvm3d_b200 import Pattern
+    (rp, ci, va), _, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    r = np.random.default_rng(13).standard_normal(c1_hetero.n)
+    perm, _ = p.ilu0_ordering(order) if order == 0 else (np.arange(c1_hetero.n, dtype=np.int32), None)
+    ilu = oracle.Ilu0(rp, ci, va, perm)
+    zo = ilu.sweep_apply(r, sweeps)
+    rd = torch.tensor(r, device="cuda")
+    zd, z2 = torch.empty_like(rd), torch.empty_like(rd)
+    p.ilu0_sweep_apply_device(rd.data_ptr(), zd.data_ptr(), sweeps, order)
+    p.ilu0_sweep_apply_device(rd.data_ptr(), z2.data_ptr(), sweeps, order)
+    gpu_ctx.synchronize()
+    assert p.ilu0_sweep_layout(order) == 2  # the 2,744-row pattern fits 16-bit column offsets
+    assert _rel(zd.cpu().numpy(), zo) <= 1e-12
+    assert torch.equal(zd, z2)
+    za = rd.clone()
+    p.ilu0_sweep_apply_device(za.data_ptr(), za.data_ptr(), sweeps, order)
+    gpu_ctx.synchronize()
+    assert torch.equal(za, zd)
+    r32 = r.astype(np.float32)
+    rf = torch.tensor(r32, device="cuda")
+    zf = torch.empty_like(rf)
+    p.ilu0_sweep_apply_device(rf.data_ptr(), zf.data_ptr(), sweeps, order, f32=True)
+    gpu_ctx.synchronize()
+    assert _rel(zf.cpu().numpy().astype(np.float64), ilu.sweep_apply(r32.astype(np.float64), sweeps)) <= 1e-5
+
+
+@pytest.fixture(scope="module")
+def heat40_system(lib_built):
+    """The 64,000-vertex heterogeneous heat system (boundary vertices numbered after the interior,
+    so A's own bandwidth exceeds 16-bit column offsets)."""
+    from vfvchem_vfvm3d_b200.problems import steady_heat
+    prob = steady_heat(40, hetero=True)
+    return prob, oracle_system(prob)
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_ilu0_sweeps_wide_pattern_match_oracle(gpu_ctx, heat40_system, order):
+    """A factor whose bandwidth is too wide for 16-bit column offsets is swept with 32-bit columns:
+    same iterates as the oracle's sweeps (double 1e-12, float 1e-5)."""
+    import torch
+    from vfvchem_vfvm3d_b200 import Pattern
+    prob, ((rp, ci, va), _, _) = heat40_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    perm = p.ilu0_ordering(0)[0] if order == 0 else np.arange(prob.n, dtype=np.int32)
+    ilu = oracle.Ilu0(rp, ci, va, perm)
+    r = np.random.default_rng(21).standard_normal(prob.n)
+    rd = torch.tensor(r, device="cuda")
+    zd = torch.empty_like(rd)
+    p.ilu0_sweep_apply_device(rd.data_ptr(), zd.data_ptr(), 2, order)
+    gpu_ctx.synchronize()
+    assert p.ilu0_sweep_layout(order) == 4
+    assert _rel(zd.cpu().numpy(), ilu.sweep_apply(r, 2)) <= 1e-12
+    rf = rd.float()
+    zf = torch.empty_like(rf)
+    p.ilu0_sweep_apply_device(rf.data_ptr(), zf.data_ptr(), 2, order, f32=True)
+    gpu_ctx.synchronize()
+    assert _rel(zf.cpu().numpy().astype(np.float64), ilu.sweep_apply(rf.cpu().numpy().astype(np.float64), 2)) <= 1e-5
+
+
+@pytest.mark.parametrize("engine", [1, 2])
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gmres_ilu_sweeps_matches_lu(gpu_ctx, c1h_system, c1_hetero, precision, order, engine):
+    """GMRES preconditioned by ILU(0) with 3 Jacobi sweeps per factor: the same bars against LU;
+    the persistent engine refuses the sweeps."""
+    from vfvchem_vfvm3d_b200 import GmresOptions, Pattern, VFVChemError
+    (rp, ci, va), b, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    xl = lu_solve(rp, ci, va, b)
+    opts = GmresOptions(tol=1e-12, restart=30, max_outer=2000, precond=2, precision=precision, ilu_order=order, ilu_sweeps=3,
+                        inner_rtol=1e-6 if precision == 1 else 0.0, engine=engine)
+    x, info = p.solve(b, c1_hetero.T0, opts)
+    assert info.status == 0 and info.relres <= 1e-12
+    assert _rel(x, xl) <= SOL_RTOL
+    with pytest.raises(VFVChemError):
+        p.solve(b, None, GmresOptions(precond=2, ilu_sweeps=3, engine=0))
+    with pytest.raises(VFVChemError):
+        p.solve(b, None, GmresOptions(precond=2, ilu_sweeps=17))
+
+
 @pytest.mark.parametrize("engine", [0, 1])
 @pytest.mark.parametrize("precond", [0, 1, 2])
 @pytest.mark.parametrize("precision", [0, 1])

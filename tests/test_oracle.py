@@ -197,6 +197,39 @@ def test_oracle_ilu0_is_exact_on_pattern(c1_hetero, c1h_system):
         assert np.allclose(LU[pr, pc], va, rtol=1e-12, atol=1e-12 * np.abs(va).max())
 
 
+def test_oracle_ilu0_sweeps(c1h_system):
+    """The Jacobi-sweep apply of the ILU(0) factors: as many sweeps as the ordering has levels
+    solve both triangles exactly (N and S are nilpotent over the levels); two sweeps equal the
+    recurrences written with dense factors; the iterates do not depend on the numbering."""
+    (rp, ci, va), _, _ = c1h_system
+    n = rp.size - 1
+    r = np.random.default_rng(5).standard_normal(n)
+    perm, lev = ordering.multicolor(rp, ci)
+    ilu = oracle.Ilu0(rp, ci, va, perm)
+    nlev = int(lev.max()) + 1
+    zx = ilu.apply(r)
+    assert np.linalg.norm(ilu.sweep_apply(r, nlev) - zx) <= 1e-12 * np.linalg.norm(zx)
+    assert np.linalg.norm(ilu.sweep_apply(r, 1) - zx) > 1e-3 * np.linalg.norm(zx)
+    rows = np.repeat(np.arange(n), np.diff(ilu.rp))
+    N = np.zeros((n, n))
+    S = np.zeros((n, n))
+    low, up = ilu.ci < rows, ilu.ci > rows
+    N[rows[low], ilu.ci[low]] = ilu.lu[low]
+    S[rows[up], ilu.ci[up]] = ilu.lu[up]
+    d = ilu.lu[ilu.dg]
+    y = r[perm]
+    u = y - N @ (y - N @ y)
+    w = u / d
+    w = (u - S @ ((u - S @ w) / d)) / d
+    z = np.empty(n)
+    z[perm] = w
+    assert np.linalg.norm(ilu.sweep_apply(r, 2) - z) <= 1e-13 * np.linalg.norm(z)
+    pn, _ = ordering.natural(rp, ci)
+    za = oracle.Ilu0(rp, ci, va, pn).sweep_apply(r, 3)
+    zb = oracle.Ilu0(rp, ci, va, np.arange(n, dtype=np.int32)).sweep_apply(r, 3)
+    assert np.linalg.norm(za - zb) <= 1e-12 * np.linalg.norm(zb)
+
+
 def test_heat_slab_profile(lib_built):
     """T(x) = x + q x (1 - x) / (2 k) for a uniform source (heat_analytic.rs:9 with L = 1)."""
     from vfvchem_vfvm3d_b200.problems import steady_heat

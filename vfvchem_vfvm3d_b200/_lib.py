@@ -32,6 +32,7 @@ class GmresOpts(C.Structure):
         ("engine", C.c_int32),
         ("inner_rtol", C.c_double),
         ("wait_limit", C.c_int64),
+        ("ilu_sweeps", C.c_int32),
     ]
 
 
@@ -75,6 +76,9 @@ SIGNATURES = [
     ("vfv_spmv_device_f32", C.c_int, [_P, _P, _P, _P]),
     ("vfv_ilu0_apply_device", C.c_int, [_P, _P, C.c_int, _P, _P, _I32P]),
     ("vfv_ilu0_apply_device_f32", C.c_int, [_P, _P, C.c_int, _P, _P, _P, _I32P]),
+    ("vfv_ilu0_sweep_apply_device", C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
+    ("vfv_ilu0_sweep_apply_device_f32", C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
+    ("vfv_ilu0_sweep_layout", C.c_int, [_P, C.c_int, _I32P]),
     ("vfv_pattern_autotune", C.c_int, [_P, _P, _I32P, _I32P]),
     ("vfv_pattern_set_spmv_lanes", C.c_int, [_P, _P, C.c_int32, C.c_int32]),
     ("vfv_pattern_spmv_shape", C.c_int, [_P, _I32P, _I32P, _I32P, _I32P]),

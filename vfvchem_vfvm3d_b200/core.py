@@ -31,6 +31,7 @@ class GmresOptions:
     inner_rtol: float = 0.0
     engine: int = L.ENGINE_GRAPH
     wait_limit: int = 0  # polls before a bounded device wait gives up (0: the library default)
+    ilu_sweeps: int = 0  # ILU(0): 0 exact triangular solves, k > 0 k Jacobi sweeps of each factor
 
     def to_c(self) -> L.GmresOpts:
         o = L.GmresOpts()
@@ -39,6 +40,7 @@ class GmresOptions:
         o.inner_rtol = float(self.inner_rtol)
         o.engine = int(self.engine)
         o.wait_limit = int(self.wait_limit)
+        o.ilu_sweeps = int(self.ilu_sweeps)
         return o
 
 
@@ -202,6 +204,18 @@ class Pattern:
         _check(self.ctx.handle, L.load().vfv_ilu0_apply_device_f32(self.ctx.handle, self._h, int(order), C.c_void_p(r_ptr),
                                                                    C.c_void_p(t_ptr), C.c_void_p(z_ptr), C.byref(lev)))
         return lev.value
+
+    def ilu0_sweep_apply_device(self, r_ptr: int, z_ptr: int, sweeps: int, order: int = L.ILU_MULTICOLOR, f32: bool = False) -> None:
+        """z = M^-1 r with `sweeps` Jacobi sweeps of each ILU(0) factor (double, or the float factor
+        with f32), enqueued on the context's stream (no synchronisation)."""
+        fn = L.load().vfv_ilu0_sweep_apply_device_f32 if f32 else L.load().vfv_ilu0_sweep_apply_device
+        _check(self.ctx.handle, fn(self.ctx.handle, self._h, int(order), int(sweeps), C.c_void_p(r_ptr), C.c_void_p(z_ptr)))
+
+    def ilu0_sweep_layout(self, order: int = L.ILU_MULTICOLOR) -> int:
+        """bytes per column index of the swept factors (2: 16-bit offsets from the row, 4: absolute)"""
+        cb = C.c_int32()
+        _check(self.ctx.handle, L.load().vfv_ilu0_sweep_layout(self._h, int(order), C.byref(cb)))
+        return cb.value
 
     def autotune(self):
         """Pick the SpMV lanes per row (double, float) by measurement; call before the first solve."""

@@ -408,6 +408,213 @@ void ilu_apply_levels(cudaStream_t s, const IluStruct& S, const T* lu, const T* 
     for (int l = S.nlev - 1; l >= 0; --l) launch_level<T, false>(s, S, l, true, lu, in, t, out, st, prio, use_prio);
 }
 
+// the buffer of precision T out of a double / float pair
+template <typename T>
+DBuf<T>& of_prec(DBuf<double>& d, DBuf<float>& f) {
+    if constexpr (std::is_same<T, double>::value) return d;
+    else return f;
+}
+
+// Compact triangles of the factor for the Jacobi-sweep apply (k_ilu0_sweep): structure once per
+// ILU structure (host), values per factor refresh and precision (device). The natural ordering is
+// swept in A's own numbering (A's rows with the factor's values scattered back to A's slots), the
+// multicolour ordering in its factor's permuted numbering.
+template <typename T>
+int ilu_split_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S) {
+    cudaStream_t s = ctx->stream;
+    const int64_t n = p->n, nnz = p->nnz;
+    IluStruct::Split& X = S.split;
+    const bool nat = S.order == VFV_ILU_NATURAL;
+    if (!X.built) {
+        // the factor's structure in its numbering F
+        std::vector<int32_t> rp, ci, dg(n);
+        if (nat) {
+            rp = p->h_rp;
+            ci = p->h_ci;
+            for (int64_t i = 0; i < n; ++i)
+                for (int32_t k = rp[i]; k < rp[i + 1]; ++k)
+                    if (ci[k] == i) dg[i] = k;
+        } else {
+            rp.resize(n + 1);
+            ci.resize(nnz);
+            CK(cudaMemcpyAsync(rp.data(), S.rp.p, (n + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(ci.data(), S.ci.p, nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(dg.data(), S.dg.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        int64_t maxd = 0;
+        for (int64_t r = 0; r < n; ++r)
+            for (int32_t k = rp[r]; k < rp[r + 1]; ++k) maxd = std::max<int64_t>(maxd, std::abs((int64_t)ci[k] - r));
+        // 16-bit column offsets when the factor's bandwidth allows. (A reverse Cuthill-McKee
+        // renumbering to make them fit on wider patterns was measured slower on the 10^6-row heat
+        // factor: the sweeps are latency-bound, and renumbered gathers lose the mesh order's locality.)
+        X.delta16 = maxd <= 32767;
+        std::vector<int32_t> lrp(n + 1, 0), urp(n + 1, 0), lc, uc;
+        lc.reserve(nnz / 2);
+        uc.reserve(nnz / 2);
+        for (int64_t r = 0; r < n; ++r) {
+            for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
+                if (k < dg[r]) lc.push_back(ci[k]);
+                else if (k > dg[r]) uc.push_back(ci[k]);
+            }
+            lrp[r + 1] = (int32_t)lc.size();
+            urp[r + 1] = (int32_t)uc.size();
+        }
+        CK(X.lrp.upload(lrp.data(), n + 1, s));
+        CK(X.urp.upload(urp.data(), n + 1, s));
+        if (X.delta16) {
+            std::vector<int16_t> ld(lc.size()), ud(uc.size());
+            for (int64_t r = 0; r < n; ++r) {
+                for (int32_t k = lrp[r]; k < lrp[r + 1]; ++k) ld[k] = (int16_t)(lc[k] - r);
+                for (int32_t k = urp[r]; k < urp[r + 1]; ++k) ud[k] = (int16_t)(uc[k] - r);
+            }
+            CK(X.lcd.upload(ld.data(), ld.size(), s));
+            CK(X.ucd.upload(ud.data(), ud.size(), s));
+        } else {
+            CK(X.lci.upload(lc.data(), lc.size(), s));
+            CK(X.uci.upload(uc.data(), uc.size(), s));
+        }
+        X.built = true;
+    }
+    constexpr bool dbl = std::is_same<T, double>::value;
+    uint64_t& ver = dbl ? X.version64 : X.version32;
+    if (ver == p->version) return VFV_OK;
+    const T* lu = of_prec<T>(S.lu64, S.lu32).p;
+    const int32_t *rp = S.rp.p, *dg = S.dg.p;
+    if (nat) {  // the factor's values back in A's slot order
+        DBuf<T>& nv = of_prec<T>(S.nat64, S.nat32);
+        if (!nv.p) CK(nv.alloc(nnz));
+        k_scatter_vals<T><<<grid_for(nnz), 256, 0, s>>>(nnz, S.src.p, lu, nv.p);
+        ctx->launches += 1;
+        lu = nv.p;
+        rp = p->rp.p;
+        dg = p->diag_pos.p;
+    }
+    DBuf<T>& lv = of_prec<T>(X.lv64, X.lv32);
+    DBuf<T>& uv = of_prec<T>(X.uv64, X.uv32);
+    DBuf<T>& dv = of_prec<T>(X.d64, X.d32);
+    const int64_t nlow = X.delta16 ? (int64_t)X.lcd.n : (int64_t)X.lci.n, nup = X.delta16 ? (int64_t)X.ucd.n : (int64_t)X.uci.n;
+    if (!lv.p) CK(lv.alloc(std::max<int64_t>(nlow, 1)));
+    if (!uv.p) CK(uv.alloc(std::max<int64_t>(nup, 1)));
+    if (!dv.p) CK(dv.alloc(n));
+    k_split_vals<T><<<grid_for(n), 256, 0, s>>>((int32_t)n, rp, dg, lu, X.lrp.p, X.urp.p, lv.p, uv.p, dv.p);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    ver = p->version;
+    return VFV_OK;
+}
+
+// Operands of the Jacobi-sweep apply, from the refreshed compact triangles.
+template <typename T>
+struct SweepOps {
+    int32_t n = 0;
+    int lanes = 4;  // lanes per row (measured on the 10^6-row heat factor: 1 for float values, 2 for double)
+    bool delta16 = false;
+    const int32_t *lrp = nullptr, *urp = nullptr, *perm = nullptr;
+    const void *lcols = nullptr, *ucols = nullptr;
+    const T *lv = nullptr, *uv = nullptr, *d = nullptr;
+};
+
+template <typename T>
+SweepOps<T> sweep_ops(const vfv_pattern* p, IluStruct& S) {
+    IluStruct::Split& X = S.split;
+    SweepOps<T> o;
+    o.n = (int32_t)p->n;
+    o.lanes = std::is_same<T, double>::value ? 2 : 1;
+    if (const char* e = getenv("VFV_SWEEP_LANES")) {
+        const int g = std::atoi(e);
+        if (g == 1 || g == 2 || g == 4 || g == 8) o.lanes = g;
+    }
+    o.delta16 = X.delta16;
+    o.lrp = X.lrp.p;
+    o.urp = X.urp.p;
+    o.lcols = X.delta16 ? (const void*)X.lcd.p : (const void*)X.lci.p;
+    o.ucols = X.delta16 ? (const void*)X.ucd.p : (const void*)X.uci.p;
+    o.lv = of_prec<T>(X.lv64, X.lv32).p;
+    o.uv = of_prec<T>(X.uv64, X.uv32).p;
+    o.d = of_prec<T>(X.d64, X.d32).p;
+    o.perm = S.order == VFV_ILU_NATURAL ? nullptr : S.perm.p;
+    return o;
+}
+
+inline void launch_attrs(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, bool pdl, int prio, bool use_prio) {
+    int na = 0;
+    if (pdl) {
+        attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    if (use_prio) {
+        attr[na].id = cudaLaunchAttributePriority;
+        attr[na].val.priority = prio;
+        ++na;
+    }
+    cfg.attrs = na ? attr : nullptr;
+    cfg.numAttrs = na;
+}
+
+template <typename T, typename TC, bool LOWER, int G>
+cudaError_t launch_sweep_g(cudaLaunchConfig_t& cfg, const SweepOps<T>& o, const T* rhs, const T* prev, T* next, T* w0, T* out,
+                           const DevStatus* st) {
+    cfg.gridDim = dim3((unsigned)grid_for((int64_t)o.n * G, kSwBlock));
+    return cudaLaunchKernelEx(&cfg, k_ilu0_sweep<T, TC, LOWER, G>, o.n, LOWER ? o.lrp : o.urp,
+                              (const TC*)(LOWER ? o.lcols : o.ucols), LOWER ? o.lv : o.uv, o.d, o.perm, rhs, prev, next, w0, out, st);
+}
+
+template <typename T, bool LOWER>
+cudaError_t launch_sweep(cudaLaunchConfig_t& cfg, const SweepOps<T>& o, const T* rhs, const T* prev, T* next, T* w0, T* out,
+                         const DevStatus* st) {
+    if (o.delta16) {
+        if (o.lanes == 1) return launch_sweep_g<T, int16_t, LOWER, 1>(cfg, o, rhs, prev, next, w0, out, st);
+        if (o.lanes == 2) return launch_sweep_g<T, int16_t, LOWER, 2>(cfg, o, rhs, prev, next, w0, out, st);
+        if (o.lanes == 8) return launch_sweep_g<T, int16_t, LOWER, 8>(cfg, o, rhs, prev, next, w0, out, st);
+        return launch_sweep_g<T, int16_t, LOWER, 4>(cfg, o, rhs, prev, next, w0, out, st);
+    }
+    if (o.lanes == 1) return launch_sweep_g<T, int32_t, LOWER, 1>(cfg, o, rhs, prev, next, w0, out, st);
+    if (o.lanes == 2) return launch_sweep_g<T, int32_t, LOWER, 2>(cfg, o, rhs, prev, next, w0, out, st);
+    if (o.lanes == 8) return launch_sweep_g<T, int32_t, LOWER, 8>(cfg, o, rhs, prev, next, w0, out, st);
+    return launch_sweep_g<T, int32_t, LOWER, 4>(cfg, o, rhs, prev, next, w0, out, st);
+}
+
+// z = M^-1 r by `sweeps` Jacobi sweeps of each ILU(0) factor: 2 x sweeps launches (+1 gather of r
+// into the permuted numbering), chained with programmatic dependent launch. buf: 5 work vectors of
+// n entries (permuted r, two lower and two upper iterates) aliasing neither r nor z; r and z may
+// alias (r is read by the lower sweeps only, z written by the last upper sweep only).
+template <typename T>
+void ilu_apply_sweeps(cudaStream_t s, const SweepOps<T>& o, int sweeps, const T* in, T* out, T* const* buf, const DevStatus* st,
+                      int prio = 0, bool use_prio = false) {
+    const T* rhs = in;
+    bool pdl = false;
+    cudaLaunchAttribute attr[2];
+    if (o.perm) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)grid_for(o.n));
+        cfg.blockDim = dim3(256);
+        cfg.stream = s;
+        launch_attrs(cfg, attr, false, prio, use_prio);
+        cudaLaunchKernelEx(&cfg, k_perm_gather<T>, o.n, o.perm, in, buf[0]);
+        rhs = buf[0];
+        pdl = true;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.blockDim = dim3(kSwBlock);
+    cfg.stream = s;
+    T* const ub[2] = {buf[1], buf[2]};
+    T* const wb[2] = {buf[3], buf[4]};
+    for (int k = 1; k <= sweeps; ++k) {
+        launch_attrs(cfg, attr, pdl, prio, use_prio);
+        launch_sweep<T, true>(cfg, o, rhs, k == 1 ? rhs : (const T*)ub[(k - 1) & 1], ub[k & 1], k == sweeps ? wb[0] : (T*)nullptr,
+                              (T*)nullptr, st);
+        pdl = true;
+    }
+    const T* u = ub[sweeps & 1];
+    for (int k = 1; k <= sweeps; ++k) {
+        launch_attrs(cfg, attr, true, prio, use_prio);
+        launch_sweep<T, false>(cfg, o, u, (const T*)wb[(k - 1) & 1], wb[k & 1], (T*)nullptr, k == sweeps ? out : (T*)nullptr, st);
+    }
+}
+
+constexpr int kMaxIluSweeps = 16;
 constexpr long long kDefaultWaitPolls = 20000000LL;  // polls before a bounded device wait gives up (2 s also ends it)
 
 template <typename T>
@@ -525,6 +732,10 @@ struct Gmres : SolverBase {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int ilu_prio = 0;  // greatest stream priority: the sweeps' blocks go first when SM slots free up
     bool ilu_chain = false;  // ILU(0) sweeps as one k_ilu0_chain launch (VFV_ILU_CHAIN=1) instead of one launch per level
+    int sweeps = 0;          // > 0: ILU(0) applied by this many Jacobi sweeps per factor (vfv_gmres_opts::ilu_sweeps)
+    DBuf<T> swbuf;           // the sweeps' 5 work vectors
+    T* swp[5] = {};
+    SweepOps<T> sw_ops{};
     // batch of independent meshes (block-diagonal system), one Krylov recurrence per mesh
     int nm = 0;
     DBuf<int64_t> b_mesh_row, b_tile_row, b_rtile_row;
@@ -542,12 +753,13 @@ struct Gmres : SolverBase {
         if (s2) cudaStreamDestroy(s2);
     }
 
-    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_) {
+    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_, int sweeps_) {
         n = p->n;
         m = m_;
         precond = precond_;
         ilu_order = ilu_order_;
         engine = engine_;
+        sweeps = precond == VFV_PRECOND_ILU0 ? sweeps_ : 0;
         ldv = (n + 63) / 64 * 64;
         nblk_v = (int)((n + kBlk * kRows - 1) / (kBlk * kRows));
         nblk = nblk_v;  // partial dots per vector
@@ -646,7 +858,11 @@ struct Gmres : SolverBase {
                 it = p->ilu.emplace(ilu_order, std::move(S)).first;
             }
             ilu = it->second.get();
-            if (const char* e = getenv("VFV_ILU_CHAIN")) ilu_chain = e[0] == '1';
+            if (sweeps > 0) {
+                CK(swbuf.alloc((size_t)5 * n));
+                for (int q = 0; q < 5; ++q) swp[q] = swbuf.p + (size_t)q * n;
+            }
+            if (const char* e = getenv("VFV_ILU_CHAIN")) ilu_chain = e[0] == '1' && sweeps == 0;
             if (ilu_chain) {
                 int rc = chain_setup<T>(ctx, *ilu, n);
                 if (rc) return rc;
@@ -736,7 +952,8 @@ struct Gmres : SolverBase {
     // z = M^-1 r for the ILU(0) preconditioner; `in` and `out` may alias. st: early exit once the
     // solve is done (null: always run).
     void apply_ilu(cudaStream_t s, const T* in, T* out, const DevStatus* stp, int prio = 0, bool use_prio = false) {
-        if (ilu_chain) ilu_apply_chain<T>(s, *ilu, lu_vals(), in, z2.p, out, stp, &st.p->timeout, prio, use_prio);
+        if (sweeps > 0) ilu_apply_sweeps<T>(s, sw_ops, sweeps, in, out, swp, stp, prio, use_prio);
+        else if (ilu_chain) ilu_apply_chain<T>(s, *ilu, lu_vals(), in, z2.p, out, stp, &st.p->timeout, prio, use_prio);
         else ilu_apply_levels<T>(s, *ilu, lu_vals(), in, z2.p, out, stp, prio, use_prio);
     }
 
@@ -1079,7 +1296,9 @@ struct Gmres : SolverBase {
         }
         if (precond == VFV_PRECOND_ILU0) {
             int rc = ilu_refresh(ctx, p, *ilu, mixed);
+            if (!rc && sweeps > 0) rc = ilu_split_refresh<T>(ctx, p, *ilu);
             if (rc) return rc;
+            if (sweeps > 0) sw_ops = sweep_ops<T>(p, *ilu);
         }
         if (precond == VFV_PRECOND_BJ4 && bj_version != p->version) {
             CK(cudaMemsetAsync(bj_bad.p, 0, sizeof(int), s));
@@ -1268,6 +1487,9 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
     if (o->engine == VFV_ENGINE_OVERLAP && o->precond != VFV_PRECOND_ILU0)
         return set_err(ctx, VFV_BAD_INPUT, "the overlapped engine needs the ILU(0) preconditioner");
     if (o->wait_limit < 0) return set_err(ctx, VFV_BAD_INPUT, "wait_limit must be >= 0 (0 = default)");
+    if (o->ilu_sweeps < 0 || o->ilu_sweeps > kMaxIluSweeps) return set_err(ctx, VFV_BAD_INPUT, "ilu_sweeps must be in [0, 16]");
+    if (o->ilu_sweeps > 0 && o->precond == VFV_PRECOND_ILU0 && o->engine == VFV_ENGINE_PERSISTENT)
+        return set_err(ctx, VFV_BAD_INPUT, "ILU(0) sweeps run on the graph and overlapped engines only");
     return VFV_OK;
 }
 
@@ -1279,20 +1501,19 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
         if (oo.precond == VFV_PRECOND_BJ4) return set_err(ctx, VFV_BAD_INPUT, "block-Jacobi(4) is not offered for batches of meshes");
         oo.engine = VFV_ENGINE_GRAPH;  // the per-mesh recurrences run on the graph engine
     }
-    const auto key = std::make_tuple(oo.precision, oo.precond, oo.precond == VFV_PRECOND_ILU0 ? oo.ilu_order : 0, oo.restart,
-                                     oo.engine + (batched ? 16 : 0));
+    const auto key = solver_key(oo, batched);
     auto it = p->solvers.find(key);
     if (it == p->solvers.end()) {
         std::unique_ptr<SolverBase> sb;
         int rc;
         if (oo.precision == VFV_MIXED) {
             auto g = std::make_unique<Gmres<float>>();
-            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps);
             if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         } else {
             auto g = std::make_unique<Gmres<double>>();
-            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps);
             if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         }
@@ -1305,9 +1526,14 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
 
 // Per-mesh Arnoldi steps of the last batched solve of this pattern with these options (meshes in
 // block order); false when no such solve exists.
+std::tuple<int, int, int, int, int> solver_key(const vfv_gmres_opts& o, bool batched) {
+    const bool ilu = o.precond == VFV_PRECOND_ILU0;
+    return std::make_tuple(o.precision, o.precond, ilu ? o.ilu_order + 16 * o.ilu_sweeps : 0, o.restart,
+                           (batched ? VFV_ENGINE_GRAPH : o.engine) + (batched ? 16 : 0));
+}
+
 bool batch_mesh_steps(const vfv_pattern* p, const vfv_gmres_opts* o, std::vector<int32_t>& steps) {
-    const auto key = std::make_tuple(o->precision, o->precond, o->precond == VFV_PRECOND_ILU0 ? o->ilu_order : 0, o->restart,
-                                     VFV_ENGINE_GRAPH + 16);
+    const auto key = solver_key(*o, true);
     auto it = p->solvers.find(key);
     if (it == p->solvers.end()) return false;
     const std::vector<MeshStat>* ms = nullptr;
@@ -1388,6 +1614,7 @@ void vfv_gmres_default_opts(vfv_gmres_opts* o) {
     o->engine = VFV_ENGINE_GRAPH;
     o->inner_rtol = 0.0;
     o->wait_limit = 0;
+    o->ilu_sweeps = 0;
 }
 
 int vfv_ctx_create(int device, vfv_ctx** out) {
@@ -1623,6 +1850,28 @@ int ilu_for_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, IluStruct** out) 
     return VFV_OK;
 }
 
+// z = M^-1 r with `sweeps` Jacobi sweeps of each factor (the apply of vfv_gmres_opts::ilu_sweeps), in
+// double or with the float copy of the factor. Enqueued on the context's stream with no
+// synchronisation; calls after the first for a pattern, ordering and precision allocate nothing.
+template <typename T>
+int sweep_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const T* r, T* z) {
+    if (!ctx || !p || !r || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
+    if (sweeps < 1 || sweeps > kMaxIluSweeps) return set_err(ctx, VFV_BAD_INPUT, "sweeps must be in [1, 16]");
+    IluStruct* S = nullptr;
+    int rc = ilu_for_apply<T>(ctx, p, ilu_order, &S);
+    if (!rc) rc = ilu_split_refresh<T>(ctx, p, *S);
+    if (rc) return rc;
+    DBuf<unsigned char>& W = S->sweep_work[chain_slot<T>()];
+    if (!W.p) CK(W.alloc((size_t)5 * p->n * sizeof(T)));
+    T* buf[5];
+    for (int q = 0; q < 5; ++q) buf[q] = reinterpret_cast<T*>(W.p) + (size_t)q * p->n;
+    const SweepOps<T> o = sweep_ops<T>(p, *S);
+    ilu_apply_sweeps<T>(ctx->stream, o, sweeps, r, z, buf, nullptr);
+    ctx->launches += 2 * sweeps + (o.perm ? 1 : 0);
+    CK(cudaGetLastError());
+    return VFV_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1653,6 +1902,23 @@ int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const
     ctx->launches += 2 * S->nlev;
     CK(cudaGetLastError());
     if (levels) *levels = S->nlev;
+    return VFV_OK;
+}
+
+int vfv_ilu0_sweep_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const double* r, double* z) {
+    return sweep_apply<double>(ctx, p, ilu_order, sweeps, r, z);
+}
+
+int vfv_ilu0_sweep_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const float* r, float* z) {
+    return sweep_apply<float>(ctx, p, ilu_order, sweeps, r, z);
+}
+
+int vfv_ilu0_sweep_layout(const vfv_pattern* p, int ilu_order, int32_t* col_bytes) {
+    if (!p) return set_err(nullptr, VFV_BAD_INPUT, "NULL argument");
+    auto it = p->ilu.find(ilu_order);
+    if (it == p->ilu.end() || !it->second->split.built)
+        return set_err(nullptr, VFV_BAD_INPUT, "no Jacobi-sweep layout for this ordering yet (apply or solve with sweeps first)");
+    if (col_bytes) *col_bytes = it->second->split.delta16 ? 2 : 4;
     return VFV_OK;
 }
 

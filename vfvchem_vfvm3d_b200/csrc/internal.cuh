@@ -95,6 +95,23 @@ struct IluStruct {
         DBuf<unsigned char> state;  // IluChainState + 2 nlev completion counters
         int grid = 0;
     } chain[2];                     // [0] double, [1] float
+
+    // Jacobi-sweep applies (vfv_gmres_opts::ilu_sweeps): the factor's strictly lower and strictly
+    // upper parts as compact CSR arrays and its diagonal, in A's own numbering for the natural
+    // ordering (nat64/nat32 hold the factor's values scattered back to A's slots) and in the
+    // factor's permuted numbering for the multicolour one
+    struct Split {
+        bool built = false, delta16 = false;  // delta16: columns stored as int16 offsets from the row
+        DBuf<int32_t> lrp, urp;
+        DBuf<int16_t> lcd, ucd;
+        DBuf<int32_t> lci, uci;
+        DBuf<double> lv64, uv64, d64;
+        DBuf<float> lv32, uv32, d32;
+        uint64_t version64 = ~0ull, version32 = ~0ull;
+    } split;
+    DBuf<double> nat64;
+    DBuf<float> nat32;
+    DBuf<unsigned char> sweep_work[2];  // 5 n entries per precision ([0] double, [1] float): standalone sweep applies
 };
 
 struct SolverBase {
@@ -116,6 +133,7 @@ struct vfv_pattern {
     std::vector<int64_t> blocks;          // row ranges of the diagonal blocks of a block-diagonal system (may be empty)
     const vfv_pattern* same_as = nullptr;  // a pattern with identical rows/columns (ILU orderings are shared)
     std::map<int, std::unique_ptr<IluStruct>> ilu;
+    // solvers by (precision, preconditioner, ILU ordering + 16 x ILU sweeps, restart, engine + 16 if batched)
     std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<SolverBase>> solvers;
     DBuf<double> tmp_b, tmp_x;  // staging for host-pointer solves
 };
@@ -130,6 +148,8 @@ struct vfv_mesh {
 // recurrence and stopping test.
 int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* o, vfv_solve_info* info,
               bool batched = false);
+// the key of the solver cache for these options
+std::tuple<int, int, int, int, int> solver_key(const vfv_gmres_opts& o, bool batched);
 // per-mesh Arnoldi steps of the last batched solve with these options
 bool batch_mesh_steps(const vfv_pattern* p, const vfv_gmres_opts* o, std::vector<int32_t>& steps);
 // the Voronoi dual of a mesh's tetrahedra computed on the device of ctx (same arrays, bit for bit,

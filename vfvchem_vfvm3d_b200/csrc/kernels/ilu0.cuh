@@ -123,6 +123,108 @@ __global__ void __launch_bounds__(kLevBlock, kLevMinBlocks) k_ilu0_level(int32_t
     }
 }
 
+// ---------------------------------------------------------------- Jacobi sweeps of the factors
+// The triangular solves of ILU(0) replaced by a fixed number of Jacobi sweeps of each factor
+// (Anzt, Chow & Dongarra, "Iterative sparse triangular solves for preconditioning", Euro-Par 2015):
+// with L = I + N (N strictly lower) and U = D + S (S strictly upper),
+//     u^0 = y,        u^k = y - N u^(k-1)            (k = 1..sweeps)
+//     w^0 = D^-1 u,   w^k = D^-1 (u - S w^(k-1))     (k = 1..sweeps, u = u^sweeps)
+// and z = w^sweeps. Every row of a sweep is independent, so a sweep is one bandwidth-bound launch
+// over all rows (an SpMV over one triangle) instead of one latency-bound launch per level; the
+// operator is linear and fixed, so flexible and plain GMRES both accept it.
+//
+// Storage: N and S as separate compact CSR arrays (a sweep streams only its own triangle's bytes;
+// inside A's rows the two halves share DRAM sectors), columns as 16-bit offsets from the row when
+// the pattern's bandwidth allows (TC = int16_t; int32_t absolute columns otherwise), and D apart.
+// G lanes per row, sweep_k(G) entries per lane loaded before the programmatic-dependent-launch wait (the
+// factor does not change between sweeps); lane partial sums are combined by a butterfly (fixed order).
+constexpr int kSwBlock = 256;
+__host__ __device__ constexpr int sweep_k(int G) { return G >= 4 ? 2 : 8 / G; }  // ~8 entries of a row held before the wait
+
+template <typename TC>
+__device__ __forceinline__ int32_t sweep_col(TC c, int32_t row) {
+    if constexpr (sizeof(TC) == 2) return row + (int32_t)c;
+    else return (int32_t)c;
+}
+
+// LOWER: next[i] = rhs[i] - sum_k val[k] prev[col k]; w0 (if set) also gets next[i] / d[i].
+// UPPER: w[i] = (rhs[i] - sum_k val[k] prev[col k]) / d[i], stored to next[i], or to out[perm[i]]
+//        (out[i] without perm) on the last sweep (out set).
+template <typename T, typename TC, bool LOWER, int G>
+__global__ void __launch_bounds__(kSwBlock) k_ilu0_sweep(int32_t n, const int32_t* __restrict__ rowp, const TC* __restrict__ cols,
+                                                         const T* __restrict__ val, const T* __restrict__ d,
+                                                         const int32_t* __restrict__ perm, const T* rhs, const T* prev, T* next, T* w0,
+                                                         T* out, const DevStatus* __restrict__ st) {
+    const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t i = (int32_t)(gt / G);
+    const int lane = (int)(gt & (G - 1));
+    int32_t kb = 0, ke = 0;
+    constexpr int kSwK = sweep_k(G);
+    int32_t c[kSwK];
+    T v[kSwK];
+    if (i < n) {
+        kb = __ldg(rowp + i);
+        ke = __ldg(rowp + i + 1);
+    }
+#pragma unroll
+    for (int q = 0; q < kSwK; ++q) {
+        const int32_t k = kb + lane + q * G;
+        c[q] = k < ke ? sweep_col<TC>(__ldg(cols + k), i) : -1;
+        v[q] = k < ke ? __ldg(val + k) : T(0);
+    }
+    pdl_launch_dependents();
+    pdl_wait();
+    if (st && st->done) return;  // uniform over the grid
+    T s = T(0);
+#pragma unroll
+    for (int q = 0; q < kSwK; ++q)
+        if (c[q] >= 0) s += v[q] * prev[c[q]];
+    for (int32_t k = kb + lane + kSwK * G; k < ke; k += G) s += __ldg(val + k) * prev[sweep_col<TC>(__ldg(cols + k), i)];
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
+    if (i >= n || lane != 0) return;
+    if (LOWER) {
+        const T u = rhs[i] - s;
+        next[i] = u;
+        if (w0) w0[i] = u / __ldg(d + i);
+    } else {
+        const T w = (rhs[i] - s) / __ldg(d + i);
+        if (out) out[perm ? __ldg(perm + i) : i] = w;
+        else next[i] = w;
+    }
+}
+
+// Values of the compact triangles from the factor's rows (thread per row): the strictly lower
+// entries of row i to lv[lrp[i]..], the strictly upper ones to uv[urp[i]..], the diagonal to dv[i].
+template <typename T>
+__global__ void k_split_vals(int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ dg, const T* __restrict__ lu,
+                             const int32_t* __restrict__ lrp, const int32_t* __restrict__ urp, T* __restrict__ lv, T* __restrict__ uv,
+                             T* __restrict__ dv) {
+    const int32_t i = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= n) return;
+    const int32_t b = rp[i], dd = dg[i], e = rp[i + 1];
+    int32_t o = lrp[i];
+    for (int32_t k = b; k < dd; ++k) lv[o++] = lu[k];
+    dv[i] = lu[dd];
+    o = urp[i];
+    for (int32_t k = dd + 1; k < e; ++k) uv[o++] = lu[k];
+}
+
+// y[i] = in[perm[i]]: the right-hand side in the factor's numbering (first step of a sweep apply)
+template <typename T>
+__global__ void k_perm_gather(int32_t n, const int32_t* __restrict__ perm, const T* in, T* __restrict__ y) {
+    pdl_launch_dependents();
+    const int32_t i = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i < n) y[i] = in[__ldg(perm + i)];
+}
+
+// Factor values back in A's own slot order (natural ordering): out[src[k]] = lu[k].
+template <typename T>
+__global__ void k_scatter_vals(int64_t nnz, const int32_t* __restrict__ src, const T* __restrict__ lu, T* __restrict__ out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nnz) out[src[k]] = lu[k];
+}
+
 }  // namespace vfv
 
 namespace vfv {
