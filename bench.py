@@ -117,7 +117,9 @@ def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16, band=1e-2):
     The difference J(p + h e) - J(p - h e) is formed without cancellation: with T the computed
     base state, the solutions at p +- h e are T + delta+- where A+- delta+- = b+- - A+- T (the
     residual of T in each perturbed system, a vector of size ~h, solved to relres 1e-14 of its own
-    norm). T + delta+- is the perturbed solution whatever error T carries, so J+ - J- =
+    norm, plus one step of iterative refinement: the solve's error, up to cond(A) x 1e-14 of delta,
+    would otherwise set a floor of ~1e-6 on the quotient at h = 1e-6). T + delta+- is the perturbed
+    solution whatever error T carries, so J+ - J- =
     sum_s (T_s - d_s) (delta+_s - delta-_s) + (delta+_s^2 - delta-_s^2) / 2 over the sensors."""
     import torch
     from vfvchem_vfvm3d_b200 import GmresOptions
@@ -151,6 +153,10 @@ def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16, band=1e-2):
         heat.ctx.synchronize()
         return b - yd.cpu().numpy()
 
+    def correction(b):  # A^-1 b for a small right-hand side, plus one step of iterative refinement
+        d1 = solve(b, np.zeros(prob.n))
+        return d1 + solve(residual(b, d1), np.zeros(prob.n))
+
     t0 = time.perf_counter()
     T = solve(assemble(logk, q), prob.T0)
     r0 = T[sens] - d
@@ -164,8 +170,8 @@ def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16, band=1e-2):
         r2 = np.random.default_rng(64)
         for _ in range(nd):
             ek, eq = r2.standard_normal(prob.n) * free, r2.standard_normal(prob.n)
-            dm = solve(residual(assemble(logk - h * ek, q - h * eq), T), np.zeros(prob.n))[sens]
-            dp = solve(residual(assemble(logk + h * ek, q + h * eq), T), np.zeros(prob.n))[sens]
+            dm = correction(residual(assemble(logk - h * ek, q - h * eq), T))[sens]
+            dp = correction(residual(assemble(logk + h * ek, q + h * eq), T))[sens]
             fd = float(r0 @ (dp - dm) + 0.5 * (dp @ dp - dm @ dm)) / (2 * h)
             ad = float(dk @ ek + dq @ eq)
             errs.append(abs(fd - ad) / abs(ad))

@@ -708,7 +708,7 @@ struct Gmres : SolverBase {
     int64_t n = 0, ldv = 0;
     int m = 0, precond = 0, ilu_order = 0, engine = 0;
     int nblk = 0, mega_grid = 0, mega_chunk = 0;
-    int nblk_v = 0;       // blocks of the multi-vector kernels (kBlk * kRows rows each)
+    int nblk_v = 0;       // blocks of the multi-vector kernels (vec_block_rows<T>() rows each)
     DBuf<T> V, z, z2, zc, valK;
     DBuf<unsigned> bar;
     DBuf<unsigned long long> trace;  // per-phase timestamps of the last cycle (VFV_TRACE_CYCLE=1)
@@ -761,7 +761,7 @@ struct Gmres : SolverBase {
         engine = engine_;
         sweeps = precond == VFV_PRECOND_ILU0 ? sweeps_ : 0;
         ldv = (n + 63) / 64 * 64;
-        nblk_v = (int)((n + kBlk * kRows - 1) / (kBlk * kRows));
+        nblk_v = (int)((n + vec_block_rows<T>() - 1) / vec_block_rows<T>());
         nblk = nblk_v;  // partial dots per vector
         const int64_t res_blocks = (n * kSpG + kBlk - 1) / kBlk;
         CK(V.alloc((size_t)(m + 1) * ldv));
@@ -871,13 +871,13 @@ struct Gmres : SolverBase {
         return VFV_OK;
     }
 
-    // Tiles of the batched kernels from the mesh row ranges: vector tiles of kBlk * kRows rows and
+    // Tiles of the batched kernels from the mesh row ranges: vector tiles of vec_block_rows<T>() rows and
     // residual tiles of kBlk / kSpG rows, each starting at its mesh's first row.
     int init_batch(vfv_ctx* ctx, const std::vector<int64_t>& rows) {
         nm = (int)rows.size() - 1;
         std::vector<int64_t> tr, rr;
         std::vector<int32_t> tm, mt(nm + 1), rm, mr(nm + 1);
-        const int64_t tv = (int64_t)kBlk * kRows, tres = kBlk / kSpG;
+        const int64_t tv = vec_block_rows<T>(), tres = kBlk / kSpG;
         for (int q = 0; q < nm; ++q) {
             mt[q] = (int32_t)tm.size();
             mr[q] = (int32_t)rm.size();

@@ -21,10 +21,18 @@
 namespace vfv {
 
 constexpr int kBlk = 256;        // threads per block of the vector kernels
-constexpr int kRows = 4;         // rows per thread in the multi-vector kernels
-constexpr int kVecMinBlocks = 4; // <= 64 registers: room for the loads of kVecGroup basis vectors
-constexpr int kVecGroup = 4;     // basis vectors whose rows a thread loads before using any of them
+constexpr int kVecMinBlocks = 8; // 32 registers: a full SM of threads for the multi-vector kernels
+constexpr int kVecGroup = 2;     // basis vectors whose rows a thread loads before using any of them
 constexpr int kMaxBasis = 128;   // m + 1 <= kMaxBasis
+
+// Rows of one 16-byte chunk (4 floats, 2 doubles): a thread of the multi-vector kernels owns one
+// chunk, a block kBlk chunks.
+template <typename T>
+constexpr int kVecRows = 16 / (int)sizeof(T);
+template <typename T>
+__host__ __device__ constexpr int64_t vec_block_rows() {
+    return (int64_t)kBlk * kVecRows<T>;
+}
 
 // Per-solve device workspace pointers used by the Krylov kernels.
 struct KrylovDev {
@@ -194,86 +202,81 @@ __global__ void __launch_bounds__(kBlk) k_residual(KrylovDev K, const int32_t* _
 }
 
 // ---------------------------------------------------------------- grouped multi-vector passes
-// A thread owns kRows rows (stride kBlk) of a block; rows past `end` read as zero. The basis rows
-// of kVecGroup vectors are loaded before any of them is used, so a thread keeps 16 loads in flight
-// instead of 4 between dependent warp reductions. Per vector and row the arithmetic (and its
-// order) is that of one vector at a time.
-
-// red[i][warp] = this warp's partial of <u_i, wr> for i < nvec
+// A thread owns the kVecRows<T> consecutive rows [row0, row0 + R) of one 16-byte chunk; rows past
+// `end` read as zero. A chunk is moved with one 16-byte load or store when it is complete and
+// aligned, else row by row: the same values either way, so tiles that start at any row (the
+// batched kernels' per-mesh tiles) give the arithmetic of aligned ones. The chunks of kVecGroup
+// basis vectors are loaded before any of them is used. Per vector the thread's rows are summed in
+// row order, then across the warp (butterfly), the block's warps and the blocks, in fixed orders.
 template <typename T>
-__device__ __forceinline__ void group_dots(const T* __restrict__ V, int64_t ldv, int64_t base, int64_t end, const double* wr, int nvec,
-                                           double (*red)[kBlk / 32]) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const bool full = base + (kRows - 1) * kBlk < end;
-    int i = 0;
-    for (; i + kVecGroup <= nvec; i += kVecGroup) {
-        T x[kVecGroup][kRows];
-#pragma unroll
-        for (int q = 0; q < kVecGroup; ++q)
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const int64_t row = base + r * kBlk;
-                x[q][r] = (full || row < end) ? V[(int64_t)(i + q) * ldv + row] : T(0);
-            }
-        double sq[kVecGroup];
-#pragma unroll
-        for (int q = 0; q < kVecGroup; ++q) {
-            sq[q] = 0.0;
-#pragma unroll
-            for (int r = 0; r < kRows; ++r)
-                if (full || base + r * kBlk < end) sq[q] += (double)x[q][r] * wr[r];
+__device__ __forceinline__ void load_chunk(const T* p, int64_t row0, int64_t end, T (&x)[kVecRows<T>]) {
+    constexpr int R = kVecRows<T>;
+    if (row0 + R <= end && (reinterpret_cast<uintptr_t>(p + row0) & 15u) == 0) {
+        if constexpr (R == 4) {
+            const float4 t = *reinterpret_cast<const float4*>(p + row0);
+            x[0] = t.x, x[1] = t.y, x[2] = t.z, x[3] = t.w;
+        } else {
+            const double2 t = *reinterpret_cast<const double2*>(p + row0);
+            x[0] = t.x, x[1] = t.y;
         }
+    } else {
 #pragma unroll
-        for (int q = 0; q < kVecGroup; ++q) {
-            const double t = warp_sum(sq[q]);
-            if (lane == 0) red[i + q][wid] = t;
-        }
-    }
-    for (; i < nvec; ++i) {
-        const T* u = V + (int64_t)i * ldv;
-        double sv = 0.0;
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            const int64_t row = base + r * kBlk;
-            if (row < end) sv += (double)u[row] * wr[r];
-        }
-        sv = warp_sum(sv);
-        if (lane == 0) red[i][wid] = sv;
+        for (int r = 0; r < R; ++r) x[r] = row0 + r < end ? p[row0 + r] : T(0);
     }
 }
 
-// acc[r] = sum_i coef[i] u_i[row_r] for i < nvec, i in order
 template <typename T>
-__device__ __forceinline__ void group_combine(const T* __restrict__ V, int64_t ldv, int64_t base, int64_t end, const double* coef, int nvec,
-                                              double* acc) {
-    const bool full = base + (kRows - 1) * kBlk < end;
+__device__ __forceinline__ void store_chunk(T* p, int64_t row0, int64_t end, const T (&x)[kVecRows<T>]) {
+    constexpr int R = kVecRows<T>;
+    if (row0 + R <= end && (reinterpret_cast<uintptr_t>(p + row0) & 15u) == 0) {
+        if constexpr (R == 4) *reinterpret_cast<float4*>(p + row0) = make_float4(x[0], x[1], x[2], x[3]);
+        else *reinterpret_cast<double2*>(p + row0) = make_double2(x[0], x[1]);
+    } else {
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) acc[r] = 0.0;
-    int i = 0;
-    for (; i + kVecGroup <= nvec; i += kVecGroup) {
-        T x[kVecGroup][kRows];
+        for (int r = 0; r < R; ++r)
+            if (row0 + r < end) p[row0 + r] = x[r];
+    }
+}
+
+// red[i][warp] = this warp's partial of <u_i, wt> for i < nvec (products in double)
+template <typename T>
+__device__ __forceinline__ void group_dots(const T* __restrict__ V, int64_t ldv, int64_t row0, int64_t end, const T* wt, int nvec,
+                                           double (*red)[kBlk / 32]) {
+    constexpr int R = kVecRows<T>;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = 0; i < nvec; i += kVecGroup) {
+        T x[kVecGroup][R];
 #pragma unroll
-        for (int q = 0; q < kVecGroup; ++q)
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const int64_t row = base + r * kBlk;
-                x[q][r] = (full || row < end) ? V[(int64_t)(i + q) * ldv + row] : T(0);
-            }
+        for (int q = 0; q < kVecGroup; ++q) load_chunk(V + (int64_t)(i + q) * ldv, row0, i + q < nvec ? end : 0, x[q]);
 #pragma unroll
         for (int q = 0; q < kVecGroup; ++q) {
-            const double c = coef[i + q];
+            double sq = 0.0;
 #pragma unroll
-            for (int r = 0; r < kRows; ++r)
-                if (full || base + r * kBlk < end) acc[r] += c * (double)x[q][r];
+            for (int r = 0; r < R; ++r) sq += (double)x[q][r] * (double)wt[r];
+            sq = warp_sum(sq);
+            if (lane == 0 && i + q < nvec) red[i + q][wid] = sq;
         }
     }
-    for (; i < nvec; ++i) {
-        const T* u = V + (int64_t)i * ldv;
-        const double c = coef[i];
+}
+
+// acc[r] = sum_i coef[i] u_i[row0 + r] for i < nvec, i in order
+template <typename T>
+__device__ __forceinline__ void group_combine(const T* __restrict__ V, int64_t ldv, int64_t row0, int64_t end, const double* coef, int nvec,
+                                              double* acc) {
+    constexpr int R = kVecRows<T>;
 #pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            const int64_t row = base + r * kBlk;
-            if (row < end) acc[r] += c * (double)u[row];
+    for (int r = 0; r < R; ++r) acc[r] = 0.0;
+    for (int i = 0; i < nvec; i += kVecGroup) {
+        T x[kVecGroup][R];
+#pragma unroll
+        for (int q = 0; q < kVecGroup; ++q) load_chunk(V + (int64_t)(i + q) * ldv, row0, i + q < nvec ? end : 0, x[q]);
+#pragma unroll
+        for (int q = 0; q < kVecGroup; ++q) {
+            if (i + q < nvec) {
+                const double c = coef[i + q];
+#pragma unroll
+                for (int r = 0; r < R; ++r) acc[r] += c * (double)x[q][r];
+            }
         }
     }
 }
@@ -284,16 +287,12 @@ template <typename T>
 __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_mdot(KrylovDev K, const T* __restrict__ V, const T* __restrict__ w, int nvec) {
     if (K.st->done) return;
     __shared__ double red[kMaxBasis][kBlk / 32];
-    __shared__ double red2[kBlk / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int64_t base = (int64_t)blockIdx.x * (kBlk * kRows) + threadIdx.x;
-    double wr[kRows];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int64_t row = base + r * kBlk;
-        wr[r] = row < K.n ? (double)w[row] : 0.0;
-    }
-    group_dots(V, K.ldv, base, K.n, wr, nvec, red);
+    constexpr int R = kVecRows<T>;
+    const int nw = blockDim.x >> 5;
+    const int64_t row0 = (int64_t)blockIdx.x * vec_block_rows<T>() + (int64_t)R * threadIdx.x;
+    T wt[R];
+    load_chunk(w, row0, K.n, wt);
+    group_dots(V, K.ldv, row0, K.n, wt, nvec, red);
     __syncthreads();
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
         double s = 0.0;
@@ -392,26 +391,20 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, con
     __shared__ double red[kMaxBasis][kBlk / 32];
     __shared__ double red2[kBlk / 32];
     __shared__ double s_coef[kMaxBasis];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int R = kVecRows<T>;
+    const int nw = blockDim.x >> 5;
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) s_coef[i] = K.coef[i];
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * (kBlk * kRows) + threadIdx.x;
-    double acc[kRows];
-    group_combine(V, K.ldv, base, K.n, s_coef, nvec, acc);
-    double wr[kRows];
+    const int64_t row0 = (int64_t)blockIdx.x * vec_block_rows<T>() + (int64_t)R * threadIdx.x;
+    double acc[R];
+    group_combine(V, K.ldv, row0, K.n, s_coef, nvec, acc);
+    T wt[R];
+    load_chunk(win, row0, K.n, wt);
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int64_t row = base + r * kBlk;
-        if (row < K.n) {
-            const T nv = (T)((double)win[row] - acc[r]);
-            w[row] = nv;
-            wr[r] = (double)nv;
-        } else {
-            wr[r] = 0.0;
-        }
-    }
+    for (int r = 0; r < R; ++r) wt[r] = (T)((double)wt[r] - acc[r]);  // rows past the end: 0 - 0
+    store_chunk(w, row0, K.n, wt);
     if (!FINAL) {
-        group_dots(V, K.ldv, base, K.n, wr, nvec, red);
+        group_dots(V, K.ldv, row0, K.n, wt, nvec, red);
         __syncthreads();
         for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
             double s = 0.0;
@@ -421,7 +414,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, con
     } else {
         double s = 0.0;
 #pragma unroll
-        for (int r = 0; r < kRows; ++r) s += wr[r] * wr[r];
+        for (int r = 0; r < R; ++r) s += (double)wt[r] * (double)wt[r];
         s = block_sum(s, red2);
         if (threadIdx.x == 0) publish_partial(K.part + blockIdx.x, s);
         if (!last_block_arrive(K.counter + 3)) return;
@@ -444,15 +437,15 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_zupdate(KrylovDev K, T*
     __shared__ double s_c[kMaxBasis];
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) s_c[i] = K.coefz[i];
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * (kBlk * kRows) + threadIdx.x;
-    double acc[kRows];
-    group_combine(Z, K.ldv, base, K.n, s_c, nvec, acc);
-    T* out = Z + (int64_t)(j + 1) * K.ldv;
+    constexpr int R = kVecRows<T>;
+    const int64_t row0 = (int64_t)blockIdx.x * vec_block_rows<T>() + (int64_t)R * threadIdx.x;
+    double acc[R];
+    group_combine(Z, K.ldv, row0, K.n, s_c, nvec, acc);
+    T qt[R];
+    load_chunk(q, row0, K.n, qt);
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int64_t row = base + r * kBlk;
-        if (row < K.n) out[row] = (T)((double)q[row] - acc[r]);
-    }
+    for (int r = 0; r < R; ++r) qt[r] = (T)((double)qt[r] - acc[r]);
+    store_chunk(Z + (int64_t)(j + 1) * K.ldv, row0, K.n, qt);
 }
 
 __global__ void k_backsolve(KrylovDev K) {

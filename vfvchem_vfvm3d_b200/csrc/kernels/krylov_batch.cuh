@@ -8,8 +8,8 @@
 // `done` flag. A mesh that has converged (or finished its m steps of the cycle) is masked out of the
 // orthogonalisation kernels; the cycle ends once every mesh is done.
 //
-// Bitwise equality with a mesh solved alone: the vector kernels work on tiles of kBlk * kRows rows
-// that start at each mesh's first row (the single-system kernels' blocks, shifted), the residual on
+// Bitwise equality with a mesh solved alone: the vector kernels work on tiles of vec_block_rows<T>()
+// rows that start at each mesh's first row (the single-system kernels' blocks, shifted), the residual on
 // tiles of kBlk / kSpG rows, and every per-mesh sum uses the single-system kernels' reduction order
 // over the mesh's own tiles, so a mesh's iterates do not depend on the rest of the batch.
 #pragma once
@@ -34,7 +34,7 @@ struct BatchDev {
     int nm, m;
     int64_t ldv;
     const int64_t* mesh_row;   // [nm+1] first row of each mesh
-    const int64_t* tile_row;   // [ntile+1] vector tiles (kBlk * kRows rows, inside one mesh)
+    const int64_t* tile_row;   // [ntile+1] vector tiles (vec_block_rows<T>() rows, inside one mesh)
     const int32_t* tile_mesh;  // [ntile]
     const int32_t* mesh_tile;  // [nm+1]
     const int64_t* rtile_row;  // [nrtile+1] residual tiles (kBlk / kSpG rows, inside one mesh)
@@ -210,15 +210,12 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_bmdot(BatchDev B, const
     const int t = blockIdx.x;
     if (B.ms[B.tile_mesh[t]].done) return;
     __shared__ double red[kMaxBasis][kBlk / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int64_t base = B.tile_row[t] + threadIdx.x, end = B.tile_row[t + 1];
-    double wr[kRows];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int64_t row = base + r * kBlk;
-        wr[r] = row < end ? (double)w[row] : 0.0;
-    }
-    group_dots(V, B.ldv, base, end, wr, nvec, red);
+    constexpr int R = kVecRows<T>;
+    const int nw = blockDim.x >> 5;
+    const int64_t row0 = B.tile_row[t] + (int64_t)R * threadIdx.x, end = B.tile_row[t + 1];
+    T wt[R];
+    load_chunk(w, row0, end, wt);
+    group_dots(V, B.ldv, row0, end, wt, nvec, red);
     __syncthreads();
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
         double s = 0.0;
@@ -274,26 +271,20 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_bupdate(BatchDev B, con
     __shared__ double red[kMaxBasis][kBlk / 32];
     __shared__ double red2[kBlk / 32];
     __shared__ double s_coef[kMaxBasis];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int R = kVecRows<T>;
+    const int nw = blockDim.x >> 5;
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) s_coef[i] = B.coef[(int64_t)m * kMaxBasis + i];
     __syncthreads();
-    const int64_t base = B.tile_row[t] + threadIdx.x, end = B.tile_row[t + 1];
-    double acc[kRows];
-    group_combine(V, B.ldv, base, end, s_coef, nvec, acc);
-    double wr[kRows];
+    const int64_t row0 = B.tile_row[t] + (int64_t)R * threadIdx.x, end = B.tile_row[t + 1];
+    double acc[R];
+    group_combine(V, B.ldv, row0, end, s_coef, nvec, acc);
+    T wt[R];
+    load_chunk(win, row0, end, wt);
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int64_t row = base + r * kBlk;
-        if (row < end) {
-            const T nv = (T)((double)win[row] - acc[r]);
-            w[row] = nv;
-            wr[r] = (double)nv;
-        } else {
-            wr[r] = 0.0;
-        }
-    }
+    for (int r = 0; r < R; ++r) wt[r] = (T)((double)wt[r] - acc[r]);  // rows past the end: 0 - 0
+    store_chunk(w, row0, end, wt);
     if (!FINAL) {
-        group_dots(V, B.ldv, base, end, wr, nvec, red);
+        group_dots(V, B.ldv, row0, end, wt, nvec, red);
         __syncthreads();
         for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
             double s = 0.0;
@@ -303,7 +294,7 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_bupdate(BatchDev B, con
     } else {
         double s = 0.0;
 #pragma unroll
-        for (int r = 0; r < kRows; ++r) s += wr[r] * wr[r];
+        for (int r = 0; r < R; ++r) s += (double)wt[r] * (double)wt[r];
         s = block_sum(s, red2);
         if (threadIdx.x == 0) B.part[t] = s;
     }
@@ -400,11 +391,8 @@ __global__ void __launch_bounds__(kBlk) k_bcombine(BatchDev B, const T* __restri
     const int k = B.ms[m].converged ? 0 : B.ms[m].steps;
     for (int i = threadIdx.x; i < k; i += blockDim.x) s_y[i] = B.y[(int64_t)m * B.m + i];
     __syncthreads();
-    const int64_t base = B.tile_row[t] + threadIdx.x, end = B.tile_row[t + 1];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int64_t row = base + r * kBlk;
-        if (row >= end) continue;
+    const int64_t end = B.tile_row[t + 1];
+    for (int64_t row = B.tile_row[t] + threadIdx.x; row < end; row += kBlk) {
         double z = 0.0;
         for (int i = 0; i < k; ++i) z += s_y[i] * (double)V[(int64_t)i * B.ldv + row];
         if (MODE == 0) x[row] += z;
