@@ -117,10 +117,11 @@ def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16, band=1e-2):
     The difference J(p + h e) - J(p - h e) is formed without cancellation: with T the computed
     base state, the solutions at p +- h e are T + delta+- where A+- delta+- = b+- - A+- T (the
     residual of T in each perturbed system, a vector of size ~h, solved to relres 1e-14 of its own
-    norm, plus one step of iterative refinement: the solve's error, up to cond(A) x 1e-14 of delta,
-    would otherwise set a floor of ~1e-6 on the quotient at h = 1e-6). T + delta+- is the perturbed
-    solution whatever error T carries, so J+ - J- =
-    sum_s (T_s - d_s) (delta+_s - delta-_s) + (delta+_s^2 - delta-_s^2) / 2 over the sensors."""
+    norm). T + delta+- is the perturbed solution whatever error T carries, so J+ - J- =
+    sum_s (T_s - d_s) (delta+_s - delta-_s) + (delta+_s^2 - delta-_s^2) / 2 over the sensors.
+    What remains at h = 1e-6 is FP64 round-off of the perturbed assembly and residual relative to a
+    perturbation of size ~1e-6 (measured: a median of ~1e-6 at h = 1e-6 against ~2e-8 at h = 1e-4,
+    an error that scales as 1/h; an iterative-refinement step on delta did not change it)."""
     import torch
     from vfvchem_vfvm3d_b200 import GmresOptions
     from vfvchem_vfvm3d_b200 import _lib as L
@@ -153,9 +154,8 @@ def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16, band=1e-2):
         heat.ctx.synchronize()
         return b - yd.cpu().numpy()
 
-    def correction(b):  # A^-1 b for a small right-hand side, plus one step of iterative refinement
-        d1 = solve(b, np.zeros(prob.n))
-        return d1 + solve(residual(b, d1), np.zeros(prob.n))
+    def correction(b):  # A^-1 b for a right-hand side of size ~h
+        return solve(b, np.zeros(prob.n))
 
     t0 = time.perf_counter()
     T = solve(assemble(logk, q), prob.T0)
@@ -509,6 +509,15 @@ def main():
     def asm():
         heat.assemble_device(k_d.data_ptr(), q_d.data_ptr(), s_d.data_ptr(), T_d.data_ptr(), bc_d.data_ptr())
     asm_s = kernel_time(asm, reps=10)
+    # Algorithmic bytes of one assembly (k_grad_lsq<4> over k, q, T, s + k_assemble_heat): per
+    # directed face the neighbour index and 3 LSQ weights (gradients) and the neighbour index, 3 skew
+    # components, area and distance (coefficients), 72 bytes; per row 132 bytes for the gradients
+    # (row pointer, 4 fields in, 12 components out) and 184 for the rest (kind, row and face
+    # pointers, diagonal slot, k, q, s, boundary value, 3 x 4 gradient components, skew centroid
+    # offset, volume, b out); 8 bytes per value written. Gathers of neighbours' fields hit L2.
+    n_dir = int(prob.mesh.n_dir)
+    bytes_asm = 72 * n_dir + 316 * n + 8 * nnz
+    gbs_asm = bytes_asm / asm_s / 1e9
 
     # end to end through the C ABI with host buffers: values + b + x0 in, x out, every step
     rp_h, ci_h, va_h = pat.export()
@@ -589,6 +598,9 @@ def main():
         "ref_solution": ref_info,
         "spmv_fp64_gbs": gbs64, "spmv_fp32_gbs": gbs32, "spmv_shape_f32": [lanes32, strides32], "spmv_fp64_ms": sp64 * 1e3, "spmv_fp32_ms": sp32 * 1e3,
         "assembly_ms": asm_s * 1e3, "mesh_setup_s": t_mesh,
+        "roofline_assembly": {"bound": "hbm", "kernel": "k_grad_lsq<4> (thread per row) + k_assemble_heat (4 lanes per row)",
+                              "achieved": gbs_asm, "peak": peak, "unit": "GB/s", "frac": gbs_asm / peak, "peak_kind": peak_kind,
+                              "algorithmic_bytes": bytes_asm, "ms": asm_s * 1e3},
         "extras": extras,
     }
     if rank == 0:

@@ -355,7 +355,8 @@ int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
         CK(cudaMemsetAsync(S.bad.p, 0, sizeof(int), s));
         for (int l = 0; l < S.nlev; ++l) {
             const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
-            k_ilu0_factor_level<<<grid_for(r1 - r0, 128), 128, 0, s>>>(r0, r1, S.rp.p, S.ci.p, S.dg.p, S.lu64.p, S.bad.p);
+            k_ilu0_factor_level_warp<<<(unsigned)((r1 - r0 + kFacWarps - 1) / kFacWarps), 32 * kFacWarps, 0, s>>>(r0, r1, S.rp.p, S.ci.p,
+                                                                                                      S.dg.p, S.lu64.p, S.bad.p);
         }
         int bad = 0;
         CK(cudaMemcpyAsync(&bad, S.bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));

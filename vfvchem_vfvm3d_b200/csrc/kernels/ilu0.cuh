@@ -48,6 +48,98 @@ __global__ void k_ilu0_factor_level(int32_t r0, int32_t r1, const int32_t* __res
     if (a[dg[i]] == 0.0) *bad = 1;
 }
 
+// The same level, one warp per row. Every pivot row k of row i belongs to an earlier level and is
+// final, so the warp first stages, for each of row i's lower entries, the pivot u_kk and row k's
+// upper part (columns and values) in shared memory - one round of independent loads instead of a
+// chain of dependent ones per merge step. Lane l then holds entry l of row i, and the eliminations
+// run in the serial kernel's order: for each lower entry t in turn, l_it = a_it / u_kk and every
+// later entry whose column occurs in row k's upper part subtracts l_it times that entry (the merge
+// of the serial kernel, as a column match across the lanes). Rows longer than a warp, or with more
+// lower entries or longer pivot rows than the staging holds, take the serial kernel's loop on lane 0.
+constexpr int kFacWarps = 8;  // rows per block
+constexpr int kFacLow = 16;   // lower entries of a row staged
+constexpr int kFacUp = 24;    // upper entries of each pivot row staged
+
+__global__ void __launch_bounds__(32 * kFacWarps) k_ilu0_factor_level_warp(int32_t r0, int32_t r1, const int32_t* __restrict__ rp,
+                                                                            const int32_t* __restrict__ ci, const int32_t* __restrict__ dg,
+                                                                            double* __restrict__ a, int* __restrict__ bad) {
+    __shared__ int32_t s_col[kFacWarps][kFacLow][kFacUp];
+    __shared__ double s_val[kFacWarps][kFacLow][kFacUp];
+    __shared__ int32_t s_dk[kFacWarps][kFacLow], s_len[kFacWarps][kFacLow];
+    __shared__ double s_piv[kFacWarps][kFacLow];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int32_t i = r0 + (int32_t)blockIdx.x * kFacWarps + w;
+    if (i >= r1) return;  // whole warps leave together
+    const int32_t b = rp[i], e = rp[i + 1], d = dg[i];
+    const int32_t len = e - b, nl = d - b;
+    bool ok = len <= 32 && nl <= kFacLow;
+    if (ok && lane < nl) {
+        const int32_t k = ci[b + lane];
+        const int32_t dk = dg[k], ul = rp[k + 1] - dk - 1;
+        s_dk[w][lane] = dk;
+        s_len[w][lane] = ul;
+        s_piv[w][lane] = a[dk];
+        if (ul > kFacUp) ok = false;
+    }
+    ok = __all_sync(full, ok);
+    if (!ok) {  // the serial kernel's loop
+        if (lane != 0) return;
+        for (int32_t kk = b; kk < d; ++kk) {
+            const int32_t k = ci[kk];
+            const double ukk = a[dg[k]];
+            if (ukk == 0.0) {
+                *bad = 1;
+                return;
+            }
+            const double lik = a[kk] / ukk;
+            a[kk] = lik;
+            int32_t p = kk + 1, q = dg[k] + 1;
+            const int32_t e_k = rp[k + 1];
+            while (p < e && q < e_k) {
+                const int32_t cp = ci[p], cq = ci[q];
+                if (cp == cq) {
+                    a[p] -= lik * a[q];
+                    ++p;
+                    ++q;
+                } else if (cp < cq) {
+                    ++p;
+                } else {
+                    ++q;
+                }
+            }
+        }
+        if (a[d] == 0.0) *bad = 1;
+        return;
+    }
+    __syncwarp(full);
+    for (int idx = lane; idx < nl * kFacUp; idx += 32) {
+        const int t = idx / kFacUp, u = idx - t * kFacUp;
+        if (u < s_len[w][t]) {
+            const int32_t q = s_dk[w][t] + 1 + u;
+            s_col[w][t][u] = ci[q];
+            s_val[w][t][u] = a[q];
+        }
+    }
+    const int32_t c = lane < len ? ci[b + lane] : -1;
+    double v = lane < len ? a[b + lane] : 0.0;
+    __syncwarp(full);
+    for (int t = 0; t < nl; ++t) {
+        const double ukk = s_piv[w][t];
+        if (ukk == 0.0) {
+            if (lane == 0) *bad = 1;
+            return;
+        }
+        const double lik = __shfl_sync(full, v, t) / ukk;
+        if (lane == t) v = lik;
+        const int ul = s_len[w][t];
+        for (int u = 0; u < ul; ++u)
+            if (lane > t && c == s_col[w][t][u]) v -= lik * s_val[w][t][u];
+    }
+    if (lane < len) a[b + lane] = v;
+    if (lane == nl && v == 0.0) *bad = 1;
+}
+
 // Gather A's values into the permuted factor storage: lu[k] = (T) val[src[k]].
 template <typename T>
 __global__ void k_gather_vals(int64_t nnz, const int32_t* __restrict__ src, const double* __restrict__ val, T* __restrict__ out) {
