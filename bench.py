@@ -268,9 +268,9 @@ def extras_transport(ctx, count):
 # lanes per row, from one ncu capture of that launch (profiles/k_spmv_1M.md); reported as the
 # roofline's traffic only when the bench runs that same matrix and lane count.
 SPMV_TRAFFIC_N100_4LANES = 209.2e6
-# DRAM bytes (read + write) of one k_ilu0_sweep<float> launch on the same matrix, averaged over the
-# launches of one apply (set from an ncu capture)
-SWEEP_TRAFFIC_N100 = None
+# DRAM bytes (read + write) of one k_ilu0_sweep<float> launch on the same matrix (4-sweep natural-order
+# factors, 32-bit columns), from one ncu capture of a lower and an upper sweep (profiles/k_ilu0_sweep_1M.md)
+SWEEP_TRAFFIC_N100 = 78.5e6
 
 
 def peaks():
