@@ -346,6 +346,23 @@ int clone_ilu_struct(vfv_ctx* ctx, const IluStruct& F, int64_t nnz, IluStruct& S
     return VFV_OK;
 }
 
+// launch attributes: programmatic dependent launch after the previous kernel, stream priority
+inline void launch_attrs(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, bool pdl, int prio, bool use_prio) {
+    int na = 0;
+    if (pdl) {
+        attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    if (use_prio) {
+        attr[na].id = cudaLaunchAttributePriority;
+        attr[na].val.priority = prio;
+        ++na;
+    }
+    cfg.attrs = na ? attr : nullptr;
+    cfg.numAttrs = na;
+}
+
 // numeric ILU(0) of the pattern's current values (double), cast to float when asked
 int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
     cudaStream_t s = ctx->stream;
@@ -355,8 +372,14 @@ int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
         CK(cudaMemsetAsync(S.bad.p, 0, sizeof(int), s));
         for (int l = 0; l < S.nlev; ++l) {
             const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
-            k_ilu0_factor_level_warp<<<(unsigned)((r1 - r0 + kFacWarps - 1) / kFacWarps), 32 * kFacWarps, 0, s>>>(r0, r1, S.rp.p, S.ci.p,
-                                                                                                      S.dg.p, S.lu64.p, S.bad.p);
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3((unsigned)((r1 - r0 + kFacWarps - 1) / kFacWarps));
+            cfg.blockDim = dim3(32 * kFacWarps);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            launch_attrs(cfg, attr, l > 0, 0, false);  // level 0 follows the value gather in stream order
+            CK(cudaLaunchKernelEx(&cfg, k_ilu0_factor_level_warp, r0, r1, (const int32_t*)S.rp.p, (const int32_t*)S.ci.p,
+                                  (const int32_t*)S.dg.p, S.lu64.p, S.bad.p));
         }
         int bad = 0;
         CK(cudaMemcpyAsync(&bad, S.bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -538,21 +561,6 @@ SweepOps<T> sweep_ops(const vfv_pattern* p, IluStruct& S) {
     return o;
 }
 
-inline void launch_attrs(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, bool pdl, int prio, bool use_prio) {
-    int na = 0;
-    if (pdl) {
-        attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[na].val.programmaticStreamSerializationAllowed = 1;
-        ++na;
-    }
-    if (use_prio) {
-        attr[na].id = cudaLaunchAttributePriority;
-        attr[na].val.priority = prio;
-        ++na;
-    }
-    cfg.attrs = na ? attr : nullptr;
-    cfg.numAttrs = na;
-}
 
 template <typename T, typename TC, bool LOWER, int G>
 cudaError_t launch_sweep_g(cudaLaunchConfig_t& cfg, const SweepOps<T>& o, const T* rhs, const T* prev, T* next, T* w0, T* out,

@@ -15,6 +15,11 @@
 
 namespace vfv {
 
+// Programmatic dependent launch: let the next kernel of the stream start its prologue / wait until
+// the previous kernel has finished and its writes are visible.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // One level of the IKJ factorisation: a thread per row. Rows of one level never touch each other.
 __global__ void k_ilu0_factor_level(int32_t r0, int32_t r1, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                     const int32_t* __restrict__ dg, double* __restrict__ a, int* __restrict__ bad) {
@@ -56,6 +61,9 @@ __global__ void k_ilu0_factor_level(int32_t r0, int32_t r1, const int32_t* __res
 // later entry whose column occurs in row k's upper part subtracts l_it times that entry (the merge
 // of the serial kernel, as a column match across the lanes). Rows longer than a warp, or with more
 // lower entries or longer pivot rows than the staging holds, take the serial kernel's loop on lane 0.
+// Levels are chained with programmatic dependent launch: before waiting for the previous level a
+// warp loads everything that level cannot change (the row's own values, written before the first
+// level, and the structure of its pivot rows); only the pivot rows' values are loaded after the wait.
 constexpr int kFacWarps = 8;  // rows per block
 constexpr int kFacLow = 16;   // lower entries of a row staged
 constexpr int kFacUp = 24;    // upper entries of each pivot row staged
@@ -79,10 +87,20 @@ __global__ void __launch_bounds__(32 * kFacWarps) k_ilu0_factor_level_warp(int32
         const int32_t dk = dg[k], ul = rp[k + 1] - dk - 1;
         s_dk[w][lane] = dk;
         s_len[w][lane] = ul;
-        s_piv[w][lane] = a[dk];
         if (ul > kFacUp) ok = false;
     }
     ok = __all_sync(full, ok);
+    if (ok) {  // pivot rows' columns (structure only)
+        __syncwarp(full);
+        for (int idx = lane; idx < nl * kFacUp; idx += 32) {
+            const int t = idx / kFacUp, u = idx - t * kFacUp;
+            if (u < s_len[w][t]) s_col[w][t][u] = ci[s_dk[w][t] + 1 + u];
+        }
+    }
+    const int32_t c = ok && lane < len ? ci[b + lane] : -1;
+    double v = ok && lane < len ? a[b + lane] : 0.0;
+    pdl_launch_dependents();
+    pdl_wait();
     if (!ok) {  // the serial kernel's loop
         if (lane != 0) return;
         for (int32_t kk = b; kk < d; ++kk) {
@@ -112,17 +130,11 @@ __global__ void __launch_bounds__(32 * kFacWarps) k_ilu0_factor_level_warp(int32
         if (a[d] == 0.0) *bad = 1;
         return;
     }
-    __syncwarp(full);
+    if (lane < nl) s_piv[w][lane] = a[s_dk[w][lane]];
     for (int idx = lane; idx < nl * kFacUp; idx += 32) {
         const int t = idx / kFacUp, u = idx - t * kFacUp;
-        if (u < s_len[w][t]) {
-            const int32_t q = s_dk[w][t] + 1 + u;
-            s_col[w][t][u] = ci[q];
-            s_val[w][t][u] = a[q];
-        }
+        if (u < s_len[w][t]) s_val[w][t][u] = a[s_dk[w][t] + 1 + u];
     }
-    const int32_t c = lane < len ? ci[b + lane] : -1;
-    double v = lane < len ? a[b + lane] : 0.0;
     __syncwarp(full);
     for (int t = 0; t < nl; ++t) {
         const double ukk = s_piv[w][t];
@@ -167,8 +179,6 @@ constexpr int kLevK = 16;          // entries of a row held in registers before 
                                    // late colours hold up to ~15 lower (early colours: upper) entries,
                                    // and every entry left to the loop costs a dependent round trip
 
-__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // LOWER: t[i] = in[perm[i]] - sum_{k < diag} lu[k] t[ci[k]]
 // UPPER: t[i] = (t[i] - sum_{k > diag} lu[k] t[ci[k]]) / lu[diag] ; out[perm[i]] = t[i]
