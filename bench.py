@@ -117,19 +117,21 @@ def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16, band=1e-2):
     The difference J(p + h e) - J(p - h e) is formed without cancellation: with T the computed
     base state, the solutions at p +- h e are T + delta+- where A+- delta+- = b+- - A+- T (the
     residual of T in each perturbed system, a vector of size ~h, solved to relres 1e-14 of its own
-    norm). T + delta+- is the perturbed solution whatever error T carries, so J+ - J- =
+    norm; the residual is summed in extended precision on the host from the assembled FP64 values,
+    which removes the cancellation of A T against b). T + delta+- is the perturbed solution whatever
+    error T carries, so J+ - J- =
     sum_s (T_s - d_s) (delta+_s - delta-_s) + (delta+_s^2 - delta-_s^2) / 2 over the sensors.
-    What remains at h = 1e-6 is FP64 round-off of the perturbed assembly and residual relative to a
-    perturbation of size ~1e-6 (measured: a median of ~1e-6 at h = 1e-6 against ~2e-8 at h = 1e-4,
-    an error that scales as 1/h; an iterative-refinement step on delta did not change it)."""
-    import torch
+
+    What remains at h = 1e-6 is the FP64 rounding of the perturbed assembly itself: ~1e-16 |A| |T|
+    per row against a perturbation signal of ~h times the neighbour differences of T, about 1e-8 of
+    the residual, which the sensors' cancellation amplifies to ~1e-6 in the quotient (an error
+    that scales as 1/h; an iterative-refinement step of the correction solves does not change it).
+    """
     from vfvchem_vfvm3d_b200 import GmresOptions
     from vfvchem_vfvm3d_b200 import _lib as L
     fo = GmresOptions(tol=1e-14, restart=50, max_outer=4000, precond=L.PRECOND_ILU0)
     logk, q = np.log(prob.k), prob.q
     pat = heat.pattern
-    xd = torch.empty(prob.n, dtype=torch.float64, device="cuda")
-    yd = torch.empty_like(xd)
 
     kf, km, v, nb, npt = guard_faces(heat, prob)
     near = np.abs(kf) <= band * km
@@ -147,12 +149,13 @@ def adjoint_fd_check(heat, prob, sens, d, ndir=64, ndir_wide=16, band=1e-2):
         x, _ = pat.solve(b, x0, fo)
         return x
 
-    def residual(b, x):  # b - A x with the pattern's current values (device SpMV, FP64)
-        xd.copy_(torch.from_numpy(x))
-        torch.cuda.synchronize()
-        pat.spmv_device(xd.data_ptr(), yd.data_ptr())
-        heat.ctx.synchronize()
-        return b - yd.cpu().numpy()
+    rp_a, ci_a, _ = pat.export()
+    starts = rp_a[:-1].astype(np.int64)
+
+    def residual(b, x):  # b - A x with the pattern's current values, summed in extended precision on the host
+        _, _, va = pat.export()
+        ax = np.add.reduceat(va.astype(np.longdouble) * x.astype(np.longdouble)[ci_a], starts)
+        return (b.astype(np.longdouble) - ax).astype(np.float64)
 
     def correction(b):  # A^-1 b for a right-hand side of size ~h
         return solve(b, np.zeros(prob.n))

@@ -48,13 +48,17 @@ def test_transport_assembly_matches_oracle(gpu_ctx, batch):
         assert np.max(np.abs(va[rp[r0]:rp[r1]] - ova)) <= 1e-12 * np.max(np.abs(ova))
 
 
-def test_transport_steps_match_lu(gpu_ctx, batch):
+@pytest.mark.parametrize("sweeps", [0, 3])
+def test_transport_steps_match_lu(gpu_ctx, batch, sweeps):
+    """Per-mesh batched GMRES with exact ILU(0) or with Jacobi sweeps of the natural-order factors
+    (one swept factor for the whole block-diagonal batch) against LU time stepping."""
     from vfvchem_vfvm3d_b200 import GmresOptions, TransientTransportGpu
     from vfvchem_vfvm3d_b200 import _lib as L
     meshes, vel, c0 = batch
     tr = TransientTransportGpu(meshes, DT, ctx=gpu_ctx)
     tr.assemble(1e-3, vel)
-    opts = GmresOptions(tol=1e-12, restart=30, max_outer=500, precond=L.PRECOND_ILU0, precision=L.MIXED, inner_rtol=1e-6)
+    opts = GmresOptions(tol=1e-12, restart=30, max_outer=500, precond=L.PRECOND_ILU0, precision=L.MIXED, inner_rtol=1e-6,
+                        ilu_order=L.ILU_NATURAL if sweeps else L.ILU_MULTICOLOR, ilu_sweeps=sweeps)
     c_gpu, its = tr.run(c0, 5, opts)
     assert np.all(its > 0)
     off = 0
