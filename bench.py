@@ -249,13 +249,16 @@ def extras_transport(ctx, count):
     tr = TransientTransportGpu(tb.meshes, tb.dt, ctx=ctx)
     tr.assemble(tb.D, vel)
     lanes = tr.pattern.autotune()
-    opts = GmresOptions(tol=1e-10, restart=30, max_outer=200, precond=L.PRECOND_ILU0, precision=L.MIXED, inner_rtol=1e-6)
+    # natural-order ILU(0) with 3 Jacobi sweeps per factor (measured on this batch: 0.69 s per 100
+    # steps, 5.0 iterations per step, against 0.76 s and 6.8 with the exact multicolour ILU(0))
+    swept = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_NATURAL, ilu_sweeps=3)
+    opts = GmresOptions(tol=1e-10, restart=30, max_outer=200, precision=L.MIXED, inner_rtol=1e-6, **swept)
     tr.run(c0, 3, opts)
     t0 = time.perf_counter()
     c, its = tr.run(c0, tb.steps, opts)
     t_run = time.perf_counter() - t0
     target = np.full(tr.n, float(np.mean(c0)))
-    aopts = GmresOptions(tol=1e-10, restart=30, max_outer=500, precond=L.PRECOND_ILU0, precision=L.MIXED, inner_rtol=1e-6)
+    aopts = GmresOptions(tol=1e-10, restart=30, max_outer=500, precision=L.MIXED, inner_rtol=1e-6, **swept)
     t0 = time.perf_counter()
     J, dJdD, aits = tr.adjoint_D(c0, tb.steps, target, every=10, opts=aopts, return_iters=True)
     t_adj = time.perf_counter() - t0
@@ -264,7 +267,7 @@ def extras_transport(ctx, count):
             "mesh_setup_s": t_mesh, "per_mesh_steps_mean": float(np.mean(tr.mesh_steps())),
             "per_mesh_steps_min_max": [int(np.min(tr.mesh_steps())), int(np.max(tr.mesh_steps()))],
             "workload": f"{count} jittered cubes, N_i log-uniform in [2000, 50000], D=1e-3, u=(sin pi y, sin pi z, sin pi x), dt=1e-2; "
-                        "GMRES(30)+ILU(0) mixed to 1e-10 relres per mesh and step; host arrays in/out"}
+                        "GMRES(30) + natural-order ILU(0) with 3 Jacobi sweeps, mixed, to 1e-10 relres per mesh and step; host arrays in/out"}
 
 
 # DRAM bytes (read + write) of one k_spmv<double> launch on the 10^6-vertex heat matrix with 4
