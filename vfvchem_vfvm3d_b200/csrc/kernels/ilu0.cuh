@@ -20,47 +20,16 @@ namespace vfv {
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
-// One level of the IKJ factorisation: a thread per row. Rows of one level never touch each other.
-__global__ void k_ilu0_factor_level(int32_t r0, int32_t r1, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                    const int32_t* __restrict__ dg, double* __restrict__ a, int* __restrict__ bad) {
-    const int32_t i = r0 + (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-    if (i >= r1) return;
-    const int32_t e_i = rp[i + 1];
-    for (int32_t kk = rp[i]; kk < dg[i]; ++kk) {
-        const int32_t k = ci[kk];
-        const double ukk = a[dg[k]];
-        if (ukk == 0.0) {
-            *bad = 1;
-            return;
-        }
-        const double lik = a[kk] / ukk;
-        a[kk] = lik;
-        int32_t p = kk + 1, q = dg[k] + 1;
-        const int32_t e_k = rp[k + 1];
-        while (p < e_i && q < e_k) {
-            const int32_t cp = ci[p], cq = ci[q];
-            if (cp == cq) {
-                a[p] -= lik * a[q];
-                ++p;
-                ++q;
-            } else if (cp < cq) {
-                ++p;
-            } else {
-                ++q;
-            }
-        }
-    }
-    if (a[dg[i]] == 0.0) *bad = 1;
-}
-
-// The same level, one warp per row. Every pivot row k of row i belongs to an earlier level and is
-// final, so the warp first stages, for each of row i's lower entries, the pivot u_kk and row k's
-// upper part (columns and values) in shared memory - one round of independent loads instead of a
-// chain of dependent ones per merge step. Lane l then holds entry l of row i, and the eliminations
-// run in the serial kernel's order: for each lower entry t in turn, l_it = a_it / u_kk and every
-// later entry whose column occurs in row k's upper part subtracts l_it times that entry (the merge
-// of the serial kernel, as a column match across the lanes). Rows longer than a warp, or with more
-// lower entries or longer pivot rows than the staging holds, take the serial kernel's loop on lane 0.
+// One level of the IKJ factorisation, one warp per row; rows of one level never touch each other.
+// Every pivot row k of row i belongs to an earlier level and is final, so the warp first stages,
+// for each of row i's lower entries, the pivot u_kk and row k's upper part (columns and values) in
+// shared memory - one round of independent loads instead of a chain of dependent ones per merge
+// step (a thread per row walking the merges was 5x slower on the 692 natural levels of the 10^6-row
+// heat matrix). Lane l then holds entry l of row i, and the eliminations run in the serial IKJ
+// order: for each lower entry t in turn, l_it = a_it / u_kk, and every later entry whose column
+// occurs in row k's upper part subtracts l_it times that entry (the merge of the serial loop, as a
+// column match across the lanes). Rows longer than a warp, or with more lower entries or longer
+// pivot rows than the staging holds, run the serial loop on lane 0.
 // Levels are chained with programmatic dependent launch: before waiting for the previous level a
 // warp loads everything that level cannot change (the row's own values, written before the first
 // level, and the structure of its pivot rows); only the pivot rows' values are loaded after the wait.
@@ -101,7 +70,7 @@ __global__ void __launch_bounds__(32 * kFacWarps) k_ilu0_factor_level_warp(int32
     double v = ok && lane < len ? a[b + lane] : 0.0;
     pdl_launch_dependents();
     pdl_wait();
-    if (!ok) {  // the serial kernel's loop
+    if (!ok) {  // the serial IKJ loop
         if (lane != 0) return;
         for (int32_t kk = b; kk < d; ++kk) {
             const int32_t k = ci[kk];
