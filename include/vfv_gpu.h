@@ -85,6 +85,7 @@ typedef struct {
                            L = I + N, U = D + S; Anzt, Chow & Dongarra 2015): a fixed linear preconditioner whose
                            sweeps are one bandwidth-bound launch each. With VFV_ILU_NATURAL they run in A's own
                            numbering. Graph and overlapped engines only. */
+    int32_t ilu_sweeps_upper; /* with ilu_sweeps > 0: Jacobi sweeps of the upper factor, in [1, 16] (0 = ilu_sweeps) */
 } vfv_gmres_opts;
 
 typedef struct {

@@ -296,19 +296,20 @@ def test_ilu0_sweeps_wide_pattern_match_oracle(gpu_ctx, heat40_system, order):
     assert _rel(zf.cpu().numpy().astype(np.float64), ilu.sweep_apply(rf.cpu().numpy().astype(np.float64), 2)) <= 1e-5
 
 
+@pytest.mark.parametrize("upper", [0, 5])
 @pytest.mark.parametrize("engine", [1, 2])
 @pytest.mark.parametrize("order", [0, 1])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_gmres_ilu_sweeps_matches_lu(gpu_ctx, c1h_system, c1_hetero, precision, order, engine):
-    """GMRES preconditioned by ILU(0) with 3 Jacobi sweeps per factor: the same bars against LU;
-    the persistent engine refuses the sweeps."""
+def test_gmres_ilu_sweeps_matches_lu(gpu_ctx, c1h_system, c1_hetero, precision, order, engine, upper):
+    """GMRES preconditioned by ILU(0) with 3 Jacobi sweeps of the lower factor and 3 (or 5) of the
+    upper one: the same bars against LU; the persistent engine refuses the sweeps."""
     from vfvchem_vfvm3d_b200 import GmresOptions, Pattern, VFVChemError
     (rp, ci, va), b, _ = c1h_system
     p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
     p.set_values(va)
     xl = lu_solve(rp, ci, va, b)
     opts = GmresOptions(tol=1e-12, restart=30, max_outer=2000, precond=2, precision=precision, ilu_order=order, ilu_sweeps=3,
-                        inner_rtol=1e-6 if precision == 1 else 0.0, engine=engine)
+                        ilu_sweeps_upper=upper, inner_rtol=1e-6 if precision == 1 else 0.0, engine=engine)
     x, info = p.solve(b, c1_hetero.T0, opts)
     assert info.status == 0 and info.relres <= 1e-12
     assert _rel(x, xl) <= SOL_RTOL
@@ -316,6 +317,8 @@ def test_gmres_ilu_sweeps_matches_lu(gpu_ctx, c1h_system, c1_hetero, precision, 
         p.solve(b, None, GmresOptions(precond=2, ilu_sweeps=3, engine=0))
     with pytest.raises(VFVChemError):
         p.solve(b, None, GmresOptions(precond=2, ilu_sweeps=17))
+    with pytest.raises(VFVChemError):
+        p.solve(b, None, GmresOptions(precond=2, ilu_sweeps=3, ilu_sweeps_upper=-1))
 
 
 @pytest.mark.parametrize("engine", [0, 1])

@@ -33,6 +33,7 @@ class GmresOpts(C.Structure):
         ("inner_rtol", C.c_double),
         ("wait_limit", C.c_int64),
         ("ilu_sweeps", C.c_int32),
+        ("ilu_sweeps_upper", C.c_int32),
     ]
 
 

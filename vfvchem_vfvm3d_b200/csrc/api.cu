@@ -585,12 +585,13 @@ cudaError_t launch_sweep(cudaLaunchConfig_t& cfg, const SweepOps<T>& o, const T*
     return launch_sweep_g<T, int32_t, LOWER, 4>(cfg, o, rhs, prev, next, w0, out, st);
 }
 
-// z = M^-1 r by `sweeps` Jacobi sweeps of each ILU(0) factor: 2 x sweeps launches (+1 gather of r
+// z = M^-1 r by `sweeps` Jacobi sweeps of the lower and `usweeps` of the upper ILU(0) factor: one
+// launch per sweep (+1 gather of r
 // into the permuted numbering), chained with programmatic dependent launch. buf: 5 work vectors of
 // n entries (permuted r, two lower and two upper iterates) aliasing neither r nor z; r and z may
 // alias (r is read by the lower sweeps only, z written by the last upper sweep only).
 template <typename T>
-void ilu_apply_sweeps(cudaStream_t s, const SweepOps<T>& o, int sweeps, const T* in, T* out, T* const* buf, const DevStatus* st,
+void ilu_apply_sweeps(cudaStream_t s, const SweepOps<T>& o, int sweeps, int usweeps, const T* in, T* out, T* const* buf, const DevStatus* st,
                       int prio = 0, bool use_prio = false) {
     const T* rhs = in;
     bool pdl = false;
@@ -617,9 +618,9 @@ void ilu_apply_sweeps(cudaStream_t s, const SweepOps<T>& o, int sweeps, const T*
         pdl = true;
     }
     const T* u = ub[sweeps & 1];
-    for (int k = 1; k <= sweeps; ++k) {
+    for (int k = 1; k <= usweeps; ++k) {
         launch_attrs(cfg, attr, true, prio, use_prio);
-        launch_sweep<T, false>(cfg, o, u, (const T*)wb[(k - 1) & 1], wb[k & 1], (T*)nullptr, k == sweeps ? out : (T*)nullptr, st);
+        launch_sweep<T, false>(cfg, o, u, (const T*)wb[(k - 1) & 1], wb[k & 1], (T*)nullptr, k == usweeps ? out : (T*)nullptr, st);
     }
 }
 
@@ -741,7 +742,8 @@ struct Gmres : SolverBase {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int ilu_prio = 0;  // greatest stream priority: the sweeps' blocks go first when SM slots free up
     bool ilu_chain = false;  // ILU(0) sweeps as one k_ilu0_chain launch (VFV_ILU_CHAIN=1) instead of one launch per level
-    int sweeps = 0;          // > 0: ILU(0) applied by this many Jacobi sweeps per factor (vfv_gmres_opts::ilu_sweeps)
+    int sweeps = 0;          // > 0: ILU(0) applied by this many Jacobi sweeps of the lower factor (vfv_gmres_opts::ilu_sweeps)
+    int usweeps = 0;         // and this many of the upper factor (ilu_sweeps_upper, or ilu_sweeps when 0)
     DBuf<T> swbuf;           // the sweeps' 5 work vectors
     T* swp[5] = {};
     SweepOps<T> sw_ops{};
@@ -762,13 +764,14 @@ struct Gmres : SolverBase {
         if (s2) cudaStreamDestroy(s2);
     }
 
-    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_, int sweeps_) {
+    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_, int sweeps_, int usweeps_) {
         n = p->n;
         m = m_;
         precond = precond_;
         ilu_order = ilu_order_;
         engine = engine_;
         sweeps = precond == VFV_PRECOND_ILU0 ? sweeps_ : 0;
+        usweeps = sweeps > 0 ? (usweeps_ > 0 ? usweeps_ : sweeps) : 0;
         ldv = (n + 63) / 64 * 64;
         nblk_v = (int)((n + vec_block_rows<T>() - 1) / vec_block_rows<T>());
         nblk = nblk_v;  // partial dots per vector
@@ -961,7 +964,7 @@ struct Gmres : SolverBase {
     // z = M^-1 r for the ILU(0) preconditioner; `in` and `out` may alias. st: early exit once the
     // solve is done (null: always run).
     void apply_ilu(cudaStream_t s, const T* in, T* out, const DevStatus* stp, int prio = 0, bool use_prio = false) {
-        if (sweeps > 0) ilu_apply_sweeps<T>(s, sw_ops, sweeps, in, out, swp, stp, prio, use_prio);
+        if (sweeps > 0) ilu_apply_sweeps<T>(s, sw_ops, sweeps, usweeps, in, out, swp, stp, prio, use_prio);
         else if (ilu_chain) ilu_apply_chain<T>(s, *ilu, lu_vals(), in, z2.p, out, stp, &st.p->timeout, prio, use_prio);
         else ilu_apply_levels<T>(s, *ilu, lu_vals(), in, z2.p, out, stp, prio, use_prio);
     }
@@ -1497,6 +1500,8 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
         return set_err(ctx, VFV_BAD_INPUT, "the overlapped engine needs the ILU(0) preconditioner");
     if (o->wait_limit < 0) return set_err(ctx, VFV_BAD_INPUT, "wait_limit must be >= 0 (0 = default)");
     if (o->ilu_sweeps < 0 || o->ilu_sweeps > kMaxIluSweeps) return set_err(ctx, VFV_BAD_INPUT, "ilu_sweeps must be in [0, 16]");
+    if (o->ilu_sweeps_upper < 0 || o->ilu_sweeps_upper > kMaxIluSweeps)
+        return set_err(ctx, VFV_BAD_INPUT, "ilu_sweeps_upper must be in [0, 16]");
     if (o->ilu_sweeps > 0 && o->precond == VFV_PRECOND_ILU0 && o->engine == VFV_ENGINE_PERSISTENT)
         return set_err(ctx, VFV_BAD_INPUT, "ILU(0) sweeps run on the graph and overlapped engines only");
     return VFV_OK;
@@ -1517,12 +1522,12 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
         int rc;
         if (oo.precision == VFV_MIXED) {
             auto g = std::make_unique<Gmres<float>>();
-            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper);
             if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         } else {
             auto g = std::make_unique<Gmres<double>>();
-            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper);
             if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         }
@@ -1537,7 +1542,8 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
 // block order); false when no such solve exists.
 std::tuple<int, int, int, int, int> solver_key(const vfv_gmres_opts& o, bool batched) {
     const bool ilu = o.precond == VFV_PRECOND_ILU0;
-    return std::make_tuple(o.precision, o.precond, ilu ? o.ilu_order + 16 * o.ilu_sweeps : 0, o.restart,
+    const int up = o.ilu_sweeps > 0 ? (o.ilu_sweeps_upper > 0 ? o.ilu_sweeps_upper : o.ilu_sweeps) : 0;
+    return std::make_tuple(o.precision, o.precond, ilu ? o.ilu_order + 16 * (o.ilu_sweeps + 32 * up) : 0, o.restart,
                            (batched ? VFV_ENGINE_GRAPH : o.engine) + (batched ? 16 : 0));
 }
 
@@ -1624,6 +1630,7 @@ void vfv_gmres_default_opts(vfv_gmres_opts* o) {
     o->inner_rtol = 0.0;
     o->wait_limit = 0;
     o->ilu_sweeps = 0;
+    o->ilu_sweeps_upper = 0;
 }
 
 int vfv_ctx_create(int device, vfv_ctx** out) {
@@ -1875,7 +1882,7 @@ int sweep_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const T
     T* buf[5];
     for (int q = 0; q < 5; ++q) buf[q] = reinterpret_cast<T*>(W.p) + (size_t)q * p->n;
     const SweepOps<T> o = sweep_ops<T>(p, *S);
-    ilu_apply_sweeps<T>(ctx->stream, o, sweeps, r, z, buf, nullptr);
+    ilu_apply_sweeps<T>(ctx->stream, o, sweeps, sweeps, r, z, buf, nullptr);
     ctx->launches += 2 * sweeps + (o.perm ? 1 : 0);
     CK(cudaGetLastError());
     return VFV_OK;
