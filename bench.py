@@ -438,6 +438,11 @@ def main():
     omx = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, **swept)
     o64s = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, **swept)
     omxe = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, **exact)
+    # the same solvers with one-pass classical Gram-Schmidt (no reorthogonalisation)
+    omx1 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, ortho=L.ORTHO_CGS,
+                        **swept)
+    o641 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, ortho=L.ORTHO_CGS, **exact)
+    o64s1 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, ortho=L.ORTHO_CGS, **swept)
 
     def timed(opts, steps, warm):
         for _ in range(warm):
@@ -461,13 +466,17 @@ def main():
         t_64, i_64, e_64 = timed(o64, args.steps, args.warmup)
         t_64s, i_64s, e_64s = timed(o64s, args.steps, args.warmup)
         t_mxe, i_mxe, e_mxe = timed(omxe, args.steps, args.warmup)
+        t_mx1, i_mx1, e_mx1 = timed(omx1, args.steps, args.warmup)
+        t_641, i_641, e_641 = timed(o641, args.steps, args.warmup)
+        t_64s1, i_64s1, e_64s1 = timed(o64s1, args.steps, args.warmup)
     torch.cuda.synchronize()
     mx_s = sum(t_mx) / len(t_mx)
     f64_s = sum(t_64) / len(t_64)
     f64s_s = sum(t_64s) / len(t_64s)
     mxe_s = sum(t_mxe) / len(t_mxe)
     replicas.barrier(R)
-    mx_s, f64_s, f64s_s, mxe_s = replicas.max_over_ranks(R, [mx_s, f64_s, f64s_s, mxe_s])
+    mx1_s, f641_s, f64s1_s = (sum(t) / len(t) for t in (t_mx1, t_641, t_64s1))
+    mx_s, f64_s, f64s_s, mxe_s, mx1_s, f641_s, f64s1_s = replicas.max_over_ranks(R, [mx_s, f64_s, f64s_s, mxe_s, mx1_s, f641_s, f64s1_s])
 
     # SpMV (FP64 and FP32) timed alone: the kernel the metric names
     xs = torch.randn(n, dtype=torch.float64, device=dev)
@@ -583,6 +592,11 @@ def main():
             "mixed_exact_ilu": "the mixed solver with the FP64 solver's exact multicolour ILU(0)"},
         "fp64_same_precond_s": f64s_s, "speedup_mixed_vs_fp64_same_precond": f64s_s / mx_s,
         "mixed_exact_ilu_s": mxe_s,
+        "gram_schmidt_one_pass": {
+            "note": "the same three solvers with one-pass classical Gram-Schmidt (VFV_ORTHO_CGS) instead of two passes",
+            "mixed_s": mx1_s, "fp64_s": f641_s, "fp64_same_precond_s": f64s1_s,
+            "speedup_mixed_vs_fp64": f641_s / mx1_s, "speedup_mixed_vs_fp64_same_precond": f64s1_s / mx1_s,
+            "iters_mixed": i_mx1[-1].iters, "iters_fp64": i_641[-1].iters, "err_mixed": e_mx1, "err_fp64": e_641},
         "iters_mixed": i_mx[-1].iters, "iters_fp64": i_64[-1].iters, "iters_fp64_same_precond": i_64s[-1].iters,
         "iters_mixed_exact_ilu": i_mxe[-1].iters, "ilu_levels": ilu_nlev,
         "err_mixed": e_mx, "err_fp64": e_64, "err_fp64_same_precond": e_64s, "err_mixed_exact_ilu": e_mxe, "err_target": ERR_TARGET,

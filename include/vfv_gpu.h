@@ -48,6 +48,10 @@ extern "C" {
 #define VFV_MIXED 1          /* float inner GMRES cycles inside double iterative refinement */
 #define VFV_ILU_MULTICOLOR 0 /* ILU(0) of the greedy-multicolour permutation (few levels) */
 #define VFV_ILU_NATURAL 1    /* ILU(0) in the given order, level scheduled */
+#define VFV_ORTHO_CGS2 0     /* classical Gram-Schmidt, two passes every step (default) */
+#define VFV_ORTHO_DGKS 1     /* classical Gram-Schmidt, a second pass only when the first removed more than half of
+                                ||w||^2 (Daniel, Gragg, Kaufman & Stewart 1976) */
+#define VFV_ORTHO_CGS 2      /* classical Gram-Schmidt, one pass */
 #define VFV_ENGINE_PERSISTENT 0 /* one cooperative kernel per restart cycle, grid barriers between phases */
 #define VFV_ENGINE_GRAPH 1      /* a CUDA graph of one kernel per phase, replayed per restart cycle (default) */
 #define VFV_ENGINE_OVERLAP 2    /* graph engine as flexible GMRES whose ILU(0) sweeps run on a second stream,
@@ -86,6 +90,8 @@ typedef struct {
                            sweeps are one bandwidth-bound launch each. With VFV_ILU_NATURAL they run in A's own
                            numbering. Graph and overlapped engines only. */
     int32_t ilu_sweeps_upper; /* with ilu_sweeps > 0: Jacobi sweeps of the upper factor, in [1, 16] (0 = ilu_sweeps) */
+    int32_t ortho;      /* VFV_ORTHO_*: Gram-Schmidt of each Arnoldi step (graph and overlapped engines; batches of
+                           meshes and the persistent engine use CGS2) */
 } vfv_gmres_opts;
 
 typedef struct {

@@ -337,6 +337,31 @@ def test_gmres_matches_lu(gpu_ctx, c1h_system, c1_hetero, precond, precision, en
     assert _rel(x, xl) <= SOL_RTOL
 
 
+@pytest.mark.parametrize("ortho", [1, 2])
+@pytest.mark.parametrize("engine", [1, 2])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gram_schmidt_variants_match_lu(gpu_ctx, c1h_system, c1_hetero, precision, engine, ortho):
+    """Classical Gram-Schmidt with a second pass only when needed (DGKS test) and with one pass: the
+    same bars against LU, and within a few iterations of two passes; the persistent engine refuses
+    them."""
+    from vfvchem_vfvm3d_b200 import GmresOptions, Pattern, VFVChemError
+    (rp, ci, va), b, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    xl = lu_solve(rp, ci, va, b)
+    kw = dict(tol=1e-12, restart=30, max_outer=2000, precond=2, precision=precision, engine=engine,
+              inner_rtol=1e-6 if precision == 1 else 0.0)
+    x, info = p.solve(b, c1_hetero.T0, GmresOptions(ortho=ortho, **kw))
+    assert info.status == 0 and info.relres <= 1e-12
+    assert _rel(x, xl) <= SOL_RTOL
+    _, ref = p.solve(b, c1_hetero.T0, GmresOptions(**kw))
+    assert abs(info.iters - ref.iters) <= max(3, ref.iters // 10)
+    with pytest.raises(VFVChemError):
+        p.solve(b, None, GmresOptions(precond=2, ortho=ortho, engine=0))
+    with pytest.raises(VFVChemError):
+        p.solve(b, None, GmresOptions(precond=2, ortho=3))
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("order", [0, 1])
 def test_overlap_engine_matches_lu(gpu_ctx, c1h_system, c1_hetero, precision, order):

@@ -17,6 +17,7 @@ VFV_OK, VFV_NOT_CONVERGED, VFV_NONFINITE, VFV_BAD_INPUT, VFV_CUDA_ERROR, VFV_TIM
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_BJ4 = 0, 1, 2, 3
 FP64, MIXED = 0, 1
 ILU_MULTICOLOR, ILU_NATURAL = 0, 1
+ORTHO_CGS2, ORTHO_DGKS, ORTHO_CGS = 0, 1, 2
 ENGINE_PERSISTENT, ENGINE_GRAPH, ENGINE_OVERLAP = 0, 1, 2
 BC_TEMP, BC_FLUX = 0, 1
 
@@ -34,6 +35,7 @@ class GmresOpts(C.Structure):
         ("wait_limit", C.c_int64),
         ("ilu_sweeps", C.c_int32),
         ("ilu_sweeps_upper", C.c_int32),
+        ("ortho", C.c_int32),
     ]
 
 

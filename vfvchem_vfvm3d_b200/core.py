@@ -33,6 +33,7 @@ class GmresOptions:
     wait_limit: int = 0  # polls before a bounded device wait gives up (0: the library default)
     ilu_sweeps: int = 0  # ILU(0): 0 exact triangular solves, k > 0 k Jacobi sweeps of each factor
     ilu_sweeps_upper: int = 0  # with ilu_sweeps > 0: sweeps of the upper factor (0: ilu_sweeps)
+    ortho: int = L.ORTHO_CGS2  # Gram-Schmidt: two passes, a second pass only when needed (DGKS), or one pass
 
     def to_c(self) -> L.GmresOpts:
         o = L.GmresOpts()
@@ -43,6 +44,7 @@ class GmresOptions:
         o.wait_limit = int(self.wait_limit)
         o.ilu_sweeps = int(self.ilu_sweeps)
         o.ilu_sweeps_upper = int(self.ilu_sweeps_upper)
+        o.ortho = int(self.ortho)
         return o
 
 

@@ -742,6 +742,8 @@ struct Gmres : SolverBase {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int ilu_prio = 0;  // greatest stream priority: the sweeps' blocks go first when SM slots free up
     bool ilu_chain = false;  // ILU(0) sweeps as one k_ilu0_chain launch (VFV_ILU_CHAIN=1) instead of one launch per level
+    int ortho = VFV_ORTHO_CGS2;  // Gram-Schmidt of the Arnoldi steps (vfv_gmres_opts::ortho)
+    DBuf<double> wn2;            // ||w||^2 for the reorthogonalisation test
     int sweeps = 0;          // > 0: ILU(0) applied by this many Jacobi sweeps of the lower factor (vfv_gmres_opts::ilu_sweeps)
     int usweeps = 0;         // and this many of the upper factor (ilu_sweeps_upper, or ilu_sweeps when 0)
     DBuf<T> swbuf;           // the sweeps' 5 work vectors
@@ -764,7 +766,7 @@ struct Gmres : SolverBase {
         if (s2) cudaStreamDestroy(s2);
     }
 
-    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_, int sweeps_, int usweeps_) {
+    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_, int sweeps_, int usweeps_, int ortho_) {
         n = p->n;
         m = m_;
         precond = precond_;
@@ -772,6 +774,7 @@ struct Gmres : SolverBase {
         engine = engine_;
         sweeps = precond == VFV_PRECOND_ILU0 ? sweeps_ : 0;
         usweeps = sweeps > 0 ? (usweeps_ > 0 ? usweeps_ : sweeps) : 0;
+        ortho = ortho_;
         ldv = (n + 63) / 64 * 64;
         nblk_v = (int)((n + vec_block_rows<T>() - 1) / vec_block_rows<T>());
         nblk = nblk_v;  // partial dots per vector
@@ -855,6 +858,8 @@ struct Gmres : SolverBase {
         K.y = y.p;
         K.st = st.p;
         K.scal = scal.p;
+        CK(wn2.alloc(1));
+        K.wnorm2 = wn2.p;
         K.coefz = coefz.p;
         if (precond == VFV_PRECOND_ILU0) {
             auto it = p->ilu.find(ilu_order);
@@ -984,13 +989,26 @@ struct Gmres : SolverBase {
 
     // The CGS2 passes of Arnoldi step j on w = A M^-1 u_j (in `win`; the result goes to `w`, which
     // may be the same vector): first-pass dots, update + second-pass dots, update + norm + Givens.
+    // VFV_ORTHO_DGKS: first pass with ||w||^2, then a second pass whose three kernels return at once
+    // unless the first pass's test asked for it; VFV_ORTHO_CGS: the first pass alone.
     void enqueue_ortho(cudaStream_t s, const T* win, T* w, int j) {
-        const int nv = j + 1, fb = grid_for((int64_t)nv * 32);
-        k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, win, nv);
-        k_dots_finish<true><<<fb, 256, 0, s>>>(K, nv);
-        k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, win, w, nv, j);
-        k_dots_finish<false><<<fb, 256, 0, s>>>(K, nv);
-        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, nv, j);
+        const int nv = j + 1, fb = grid_for((int64_t)nv * 32), fb1 = grid_for((int64_t)(nv + 1) * 32);
+        if (ortho == VFV_ORTHO_CGS2) {
+            k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, win, nv, 0, 0);
+            k_dots_finish<true><<<fb, 256, 0, s>>>(K, nv, 0, 0);
+            k_update<T, false><<<nblk, kBlk, 0, s>>>(K, V.p, win, w, nv, j, 0, 0);
+            k_dots_finish<false><<<fb, 256, 0, s>>>(K, nv, 0, 0);
+            k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, nv, j, 0, 0);
+            return;
+        }
+        const int dgks = ortho == VFV_ORTHO_DGKS ? 1 : 0;
+        k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, win, nv, dgks, 0);
+        k_dots_finish<true><<<dgks ? fb1 : fb, 256, 0, s>>>(K, nv, dgks, 0);
+        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, win, w, nv, j, dgks, 0);
+        if (!dgks) return;
+        k_mdot<T><<<nblk, kBlk, 0, s>>>(K, V.p, w, nv, 0, 1);
+        k_dots_finish<false><<<fb, 256, 0, s>>>(K, nv, 0, 1);
+        k_update<T, true><<<nblk, kBlk, 0, s>>>(K, V.p, w, w, nv, j, 0, 1);
     }
 
     // phase timestamps of the last cycle, averaged over its steps (diagnostics, VFV_TRACE_CYCLE=1)
@@ -1502,6 +1520,10 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
     if (o->ilu_sweeps < 0 || o->ilu_sweeps > kMaxIluSweeps) return set_err(ctx, VFV_BAD_INPUT, "ilu_sweeps must be in [0, 16]");
     if (o->ilu_sweeps_upper < 0 || o->ilu_sweeps_upper > kMaxIluSweeps)
         return set_err(ctx, VFV_BAD_INPUT, "ilu_sweeps_upper must be in [0, 16]");
+    if (o->ortho != VFV_ORTHO_CGS2 && o->ortho != VFV_ORTHO_DGKS && o->ortho != VFV_ORTHO_CGS)
+        return set_err(ctx, VFV_BAD_INPUT, "unknown orthogonalisation");
+    if (o->ortho != VFV_ORTHO_CGS2 && o->engine == VFV_ENGINE_PERSISTENT)
+        return set_err(ctx, VFV_BAD_INPUT, "the persistent engine orthogonalises with CGS2 only");
     if (o->ilu_sweeps > 0 && o->precond == VFV_PRECOND_ILU0 && o->engine == VFV_ENGINE_PERSISTENT)
         return set_err(ctx, VFV_BAD_INPUT, "ILU(0) sweeps run on the graph and overlapped engines only");
     return VFV_OK;
@@ -1522,12 +1544,12 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
         int rc;
         if (oo.precision == VFV_MIXED) {
             auto g = std::make_unique<Gmres<float>>();
-            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper, batched ? VFV_ORTHO_CGS2 : oo.ortho);
             if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         } else {
             auto g = std::make_unique<Gmres<double>>();
-            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper, batched ? VFV_ORTHO_CGS2 : oo.ortho);
             if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         }
@@ -1544,7 +1566,7 @@ std::tuple<int, int, int, int, int> solver_key(const vfv_gmres_opts& o, bool bat
     const bool ilu = o.precond == VFV_PRECOND_ILU0;
     const int up = o.ilu_sweeps > 0 ? (o.ilu_sweeps_upper > 0 ? o.ilu_sweeps_upper : o.ilu_sweeps) : 0;
     return std::make_tuple(o.precision, o.precond, ilu ? o.ilu_order + 16 * (o.ilu_sweeps + 32 * up) : 0, o.restart,
-                           (batched ? VFV_ENGINE_GRAPH : o.engine) + (batched ? 16 : 0));
+                           (batched ? VFV_ENGINE_GRAPH : o.engine) + (batched ? 16 : 64 * o.ortho));
 }
 
 bool batch_mesh_steps(const vfv_pattern* p, const vfv_gmres_opts* o, std::vector<int32_t>& steps) {
@@ -1631,6 +1653,7 @@ void vfv_gmres_default_opts(vfv_gmres_opts* o) {
     o->wait_limit = 0;
     o->ilu_sweeps = 0;
     o->ilu_sweeps_upper = 0;
+    o->ortho = VFV_ORTHO_CGS2;
 }
 
 int vfv_ctx_create(int device, vfv_ctx** out) {

@@ -43,6 +43,8 @@ struct DevStatus {
     int32_t timeout;     // a bounded grid barrier gave up (the kernel left early)
     double resid_est;    // |g_{j+1}|, the residual-norm estimate after the last step
     double beta0;        // ||r_0|| of the current cycle
+    int32_t reorth;      // the current Arnoldi step takes a second Gram-Schmidt pass (DGKS test)
+    int32_t unused;
 };
 
 }  // namespace vfv

@@ -53,6 +53,7 @@ struct KrylovDev {
     double* inv_beta;   // [m+1]
     double* y;          // [m] least-squares solution scaled by 1/beta_i
     DevStatus* st;
+    double* wnorm2;     // [1] ||w||^2 of the vector being orthogonalised (the reorthogonalisation test)
     const double* scal; // [0] tol_abs: converged when ||r|| <= tol_abs
                         // [1] inner_floor_rel: a cycle also stops once resid_est <= inner_floor_rel * beta0
 };
@@ -283,9 +284,12 @@ __device__ __forceinline__ void group_combine(const T* __restrict__ V, int64_t l
 
 // ---------------------------------------------------------------- multi-dot (first CGS pass)
 // Per-block partials of d_i = <u_i, w> for i < nvec (k_dots_finish<true> completes them).
+// with_norm: also the partials of ||w||^2, as vector nvec (the first pass of the reorthogonalise-
+// if-needed scheme); only_reorth: a second pass, skipped unless the first pass asked for it.
 template <typename T>
-__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_mdot(KrylovDev K, const T* __restrict__ V, const T* __restrict__ w, int nvec) {
-    if (K.st->done) return;
+__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_mdot(KrylovDev K, const T* __restrict__ V, const T* __restrict__ w, int nvec,
+                                                               int with_norm, int only_reorth) {
+    if (K.st->done || (only_reorth && !K.st->reorth)) return;
     __shared__ double red[kMaxBasis][kBlk / 32];
     constexpr int R = kVecRows<T>;
     const int nw = blockDim.x >> 5;
@@ -293,8 +297,16 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_mdot(KrylovDev K, const
     T wt[R];
     load_chunk(w, row0, K.n, wt);
     group_dots(V, K.ldv, row0, K.n, wt, nvec, red);
+    if (with_norm) {
+        double sq = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) sq += (double)wt[r] * (double)wt[r];
+        sq = warp_sum(sq);
+        if ((threadIdx.x & 31) == 0) red[nvec][threadIdx.x >> 5] = sq;
+    }
     __syncthreads();
-    for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+    const int nout = nvec + (with_norm ? 1 : 0);
+    for (int i = threadIdx.x; i < nout; i += blockDim.x) {
         double s = 0.0;
         for (int q = 0; q < nw; ++q) s += red[i][q];
         K.part[(int64_t)i * K.nblk + blockIdx.x] = s;  // summed by k_dots_finish (the next launch)
@@ -305,12 +317,13 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_mdot(KrylovDev K, const
 // last-block reduction here would leave the GPU idle for ~15 µs while one block walks
 // nvec x nblk partials). FIRST: hacc_i = d_i / beta_i; else hacc_i += d_i / beta_i; both set
 // coef_i = d_i / beta_i^2 for the update that follows.
+// with_norm: warp nvec sums the partials of ||w||^2 into wnorm2; only_reorth as in k_mdot.
 template <bool FIRST>
-__global__ void __launch_bounds__(256) k_dots_finish(KrylovDev K, int nvec) {
-    if (K.st->done) return;
+__global__ void __launch_bounds__(256) k_dots_finish(KrylovDev K, int nvec, int with_norm, int only_reorth) {
+    if (K.st->done || (only_reorth && !K.st->reorth)) return;
     const int lane = threadIdx.x & 31;
     const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (c >= nvec) return;
+    if (c >= nvec + (with_norm ? 1 : 0)) return;
     const double* p = K.part + (int64_t)c * K.nblk;
     constexpr int kB = 16;
     double s = 0.0;
@@ -328,6 +341,10 @@ __global__ void __launch_bounds__(256) k_dots_finish(KrylovDev K, int nvec) {
         s += v[0];
     }
     s = warp_sum(s);
+    if (lane == 0 && c == nvec) {
+        K.wnorm2[0] = s;
+        return;
+    }
     if (lane == 0) {
         const double ib = K.inv_beta[c];
         if (FIRST) K.hacc[c] = s * ib;
@@ -384,10 +401,12 @@ __device__ __forceinline__ void finish_column(KrylovDev K, int j, double tot) {
 // w <- win - sum_i coef_i u_i (win == w except in the overlapped engine). Then, with FINAL == false, the partials of the second CGS pass
 // d'_i = <u_i, w> (k_dots_finish<false> adds d'_i/beta_i into hacc and sets coef); with
 // FINAL == true, ||w||^2 and the last block finishes the Hessenberg column j, the Givens rotation
-// and the convergence test.
+// and the convergence test - unless dgks is set and the test asks for a second pass, whose own
+// k_update (launched with only_reorth) then finishes the column.
 template <typename T, bool FINAL>
-__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, const T* __restrict__ V, const T* win, T* w, int nvec, int j) {
-    if (K.st->done) return;
+__global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, const T* __restrict__ V, const T* win, T* w, int nvec, int j,
+                                                                 int dgks, int only_reorth) {
+    if (K.st->done || (only_reorth && !K.st->reorth)) return;
     __shared__ double red[kMaxBasis][kBlk / 32];
     __shared__ double red2[kBlk / 32];
     __shared__ double s_coef[kMaxBasis];
@@ -421,7 +440,11 @@ __global__ void __launch_bounds__(kBlk, kVecMinBlocks) k_update(KrylovDev K, con
         const double tot = reduce_partials(K.part, gridDim.x, red2);
         if (threadIdx.x == 0) {
             K.counter[3] = 0u;
-            finish_column(K, j, tot);
+            // first pass of the reorthogonalise-if-needed scheme (Daniel, Gragg, Kaufman & Stewart
+            // 1976): a second pass only when the projection removed more than half of ||w||^2
+            const bool again = dgks && tot < 0.5 * K.wnorm2[0];
+            K.st->reorth = again ? 1 : 0;
+            if (!again) finish_column(K, j, tot);
         }
     }
 }
