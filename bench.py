@@ -258,9 +258,9 @@ def extras_transport(ctx, count):
     c, its = tr.run(c0, tb.steps, opts)
     t_run = time.perf_counter() - t0
     target = np.full(tr.n, float(np.mean(c0)))
-    # the adjoint's transposed solves keep the exact multicolour ILU(0) (with the swept one: 3.87 s
-    # against 3.24 s for the checkpointed dJ/dD)
-    aopts = GmresOptions(tol=1e-10, restart=30, max_outer=500, precond=L.PRECOND_ILU0, precision=L.MIXED, inner_rtol=1e-6)
+    # the adjoint's forward re-runs and transposed solves use the same preconditioner (another
+    # ordering would build its ILU(0) structures on the host inside the timed adjoint)
+    aopts = GmresOptions(tol=1e-10, restart=30, max_outer=500, precision=L.MIXED, inner_rtol=1e-6, **swept)
     t0 = time.perf_counter()
     J, dJdD, aits = tr.adjoint_D(c0, tb.steps, target, every=10, opts=aopts, return_iters=True)
     t_adj = time.perf_counter() - t0

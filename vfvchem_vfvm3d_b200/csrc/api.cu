@@ -370,16 +370,26 @@ int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
         k_gather_vals<double><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, S.src.p, p->val.p, S.lu64.p);
         ctx->launches += 1 + S.nlev;
         CK(cudaMemsetAsync(S.bad.p, 0, sizeof(int), s));
+        // narrow levels: one warp per row, chained with programmatic dependent launch; wide levels
+        // (>= kFacWideRows rows, e.g. multicolour colours): one thread per row, in stream order
+        constexpr int32_t kFacWideRows = 32768;
+        bool prev_warp = false;
         for (int l = 0; l < S.nlev; ++l) {
             const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
+            if (r1 - r0 >= kFacWideRows) {
+                k_ilu0_factor_level<<<grid_for(r1 - r0, 128), 128, 0, s>>>(r0, r1, S.rp.p, S.ci.p, S.dg.p, S.lu64.p, S.bad.p);
+                prev_warp = false;
+                continue;
+            }
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3((unsigned)((r1 - r0 + kFacWarps - 1) / kFacWarps));
             cfg.blockDim = dim3(32 * kFacWarps);
             cfg.stream = s;
             cudaLaunchAttribute attr[1];
-            launch_attrs(cfg, attr, l > 0, 0, false);  // level 0 follows the value gather in stream order
+            launch_attrs(cfg, attr, prev_warp, 0, false);  // after the value gather or a wide level: stream order
             CK(cudaLaunchKernelEx(&cfg, k_ilu0_factor_level_warp, r0, r1, (const int32_t*)S.rp.p, (const int32_t*)S.ci.p,
                                   (const int32_t*)S.dg.p, S.lu64.p, S.bad.p));
+            prev_warp = true;
         }
         int bad = 0;
         CK(cudaMemcpyAsync(&bad, S.bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -20,9 +20,44 @@ namespace vfv {
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
-// One level of the IKJ factorisation, one warp per row; rows of one level never touch each other.
-// Every pivot row k of row i belongs to an earlier level and is final, so the warp first stages,
-// for each of row i's lower entries, the pivot u_kk and row k's upper part (columns and values) in
+// One level of the IKJ factorisation, a thread per row (rows of one level never touch each other):
+// for wide levels (the multicolour ordering's ~10^5-row colours), where a thread per row already
+// fills the GPU and the rows are too long for the warp kernel's staging.
+__global__ void k_ilu0_factor_level(int32_t r0, int32_t r1, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                    const int32_t* __restrict__ dg, double* __restrict__ a, int* __restrict__ bad) {
+    const int32_t i = r0 + (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= r1) return;
+    const int32_t e_i = rp[i + 1];
+    for (int32_t kk = rp[i]; kk < dg[i]; ++kk) {
+        const int32_t k = ci[kk];
+        const double ukk = a[dg[k]];
+        if (ukk == 0.0) {
+            *bad = 1;
+            return;
+        }
+        const double lik = a[kk] / ukk;
+        a[kk] = lik;
+        int32_t p = kk + 1, q = dg[k] + 1;
+        const int32_t e_k = rp[k + 1];
+        while (p < e_i && q < e_k) {
+            const int32_t cp = ci[p], cq = ci[q];
+            if (cp == cq) {
+                a[p] -= lik * a[q];
+                ++p;
+                ++q;
+            } else if (cp < cq) {
+                ++p;
+            } else {
+                ++q;
+            }
+        }
+    }
+    if (a[dg[i]] == 0.0) *bad = 1;
+}
+
+// The same level, one warp per row, for narrow levels (the natural ordering's ~1,500-row levels).
+// Every pivot row k of row i belongs to an earlier level and is final, so the warp first stages, for
+// each of row i's lower entries, the pivot u_kk and row k's upper part (columns and values) in
 // shared memory - one round of independent loads instead of a chain of dependent ones per merge
 // step (a thread per row walking the merges was 5x slower on the 692 natural levels of the 10^6-row
 // heat matrix). Lane l then holds entry l of row i, and the eliminations run in the serial IKJ
