@@ -1687,6 +1687,7 @@ int vfv_ctx_create(int device, vfv_ctx** out) {
 }
 
 void vfv_ctx_destroy(vfv_ctx* ctx) {
+    DeviceGuard dg_(ctx);
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
@@ -1698,6 +1699,7 @@ void vfv_ctx_destroy(vfv_ctx* ctx) {
 const char* vfv_last_error(const vfv_ctx* ctx) { return ctx ? ctx->err.c_str() : vfv_thread_error().c_str(); }
 
 int vfv_ctx_synchronize(vfv_ctx* ctx) {
+    DeviceGuard dg_(ctx);
     if (!ctx) return set_err(nullptr, VFV_BAD_INPUT, "ctx is NULL");
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
@@ -1709,6 +1711,7 @@ void* vfv_ctx_stream(vfv_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; 
 int64_t vfv_ctx_launch_count(const vfv_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 int vfv_pattern_from_triplets(vfv_ctx* ctx, int64_t n, int64_t ntrip, const uint64_t* rows, const uint64_t* cols, vfv_pattern** out) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     *out = nullptr;
     if (n <= 0 || n >= (int64_t)1 << 31 || ntrip < 0 || (ntrip > 0 && (!rows || !cols)))
@@ -1758,6 +1761,7 @@ int vfv_pattern_from_triplets(vfv_ctx* ctx, int64_t n, int64_t ntrip, const uint
 }
 
 int vfv_pattern_from_csr(vfv_ctx* ctx, int64_t n, const int32_t* rowptr, const int32_t* colind, vfv_pattern** out) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !out || !rowptr) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     *out = nullptr;
     if (n <= 0 || n >= (int64_t)1 << 31 || rowptr[0] != 0) return set_err(ctx, VFV_BAD_INPUT, "invalid CSR");
@@ -1796,6 +1800,7 @@ int vfv_pattern_info(const vfv_pattern* p, int64_t* n, int64_t* nnz, int64_t* nt
 }
 
 int vfv_values_from_triplets(vfv_ctx* ctx, vfv_pattern* p, const double* vals) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (!p->slot_ptr.p && p->ntrip == 0 && p->nnz > 0) return set_err(ctx, VFV_BAD_INPUT, "pattern has no triplet map");
     if (p->ntrip > 0 && !vals) return set_err(ctx, VFV_BAD_INPUT, "vals is NULL");
@@ -1809,6 +1814,7 @@ int vfv_values_from_triplets(vfv_ctx* ctx, vfv_pattern* p, const double* vals) {
 }
 
 int vfv_values_set(vfv_ctx* ctx, vfv_pattern* p, const double* vals, int on_device) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p || !vals) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     CK(cudaMemcpyAsync(p->val.p, vals, p->nnz * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     p->version++;
@@ -1816,6 +1822,7 @@ int vfv_values_set(vfv_ctx* ctx, vfv_pattern* p, const double* vals, int on_devi
 }
 
 int vfv_csr_export(vfv_ctx* ctx, const vfv_pattern* p, int32_t* rowptr, int32_t* colind, double* vals) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (rowptr) std::memcpy(rowptr, p->h_rp.data(), (p->n + 1) * sizeof(int32_t));
     if (colind) std::memcpy(colind, p->h_ci.data(), p->nnz * sizeof(int32_t));
@@ -1828,6 +1835,7 @@ int vfv_csr_export(vfv_ctx* ctx, const vfv_pattern* p, int32_t* rowptr, int32_t*
 
 int vfv_solve_device(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* opts,
                      vfv_solve_info* info) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p || !b || !x0 || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     int rc = check_opts(ctx, opts);
     if (rc) return rc;
@@ -1837,6 +1845,7 @@ int vfv_solve_device(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double
 
 int vfv_solve(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, double* x, const vfv_gmres_opts* opts,
               vfv_solve_info* info) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p || !b || !x0 || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     int rc = check_opts(ctx, opts);
     if (rc) return rc;
@@ -1855,6 +1864,7 @@ int vfv_solve(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
 }
 
 int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double* y) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     launch_spmv<double, double, double, double>(ctx->stream, p->spmv_lanes[0], p->spmv_strides[0], p->n, p->rp.p, p->ci.p, p->val.p, x, y, nullptr, nullptr);
     ctx->launches += 1;
@@ -1863,6 +1873,7 @@ int vfv_spmv_device(vfv_ctx* ctx, const vfv_pattern* p, const double* x, double*
 }
 
 int vfv_spmv_device_f32(vfv_ctx* ctx, vfv_pattern* p, const float* x, float* y) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p || !x || !y) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (p->version32 != p->version) {
         if (!p->val32.p) CK(p->val32.alloc(p->nnz));
@@ -1926,6 +1937,7 @@ int sweep_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const T
 extern "C" {
 
 int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p || !r || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     IluStruct* S = nullptr;
     int rc = ilu_for_apply<double>(ctx, p, ilu_order, &S);
@@ -1942,6 +1954,7 @@ int vfv_ilu0_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const dou
 // Enqueued on the context's stream with no synchronisation, so calls after the first (which builds
 // the factor) allocate nothing and can be timed back to back.
 int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const float* r, float* t, float* z, int32_t* levels) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p || !r || !t || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (t == r || t == z) return set_err(ctx, VFV_BAD_INPUT, "the work vector aliases r or z");
     IluStruct* S = nullptr;
@@ -1955,10 +1968,12 @@ int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const
 }
 
 int vfv_ilu0_sweep_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const double* r, double* z) {
+    DeviceGuard dg_(ctx);
     return sweep_apply<double>(ctx, p, ilu_order, sweeps, r, z);
 }
 
 int vfv_ilu0_sweep_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const float* r, float* z) {
+    DeviceGuard dg_(ctx);
     return sweep_apply<float>(ctx, p, ilu_order, sweeps, r, z);
 }
 
@@ -1998,6 +2013,7 @@ std::atomic<double*> g_ilu_scratch_ptr[kNoAllocMaxDevices] = {};
 }  // namespace
 
 int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p || !r || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
     if (p->n > kNoAllocMaxRows)
@@ -2036,6 +2052,7 @@ int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, c
 // warp per row), keeps the fastest of each for every later SpMV and solver of the pattern.
 // Must run before the pattern's first solve (solvers capture their kernels once).
 int vfv_pattern_autotune(vfv_ctx* ctx, vfv_pattern* p, int32_t* lanes64, int32_t* lanes32) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     cudaStream_t s = ctx->stream;
     const int64_t n = p->n;
@@ -2098,6 +2115,7 @@ int vfv_pattern_spmv_shape(const vfv_pattern* p, int32_t* lanes64, int32_t* stri
 }
 
 int vfv_pattern_set_spmv_lanes(vfv_ctx* ctx, vfv_pattern* p, int32_t lanes64, int32_t lanes32) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     auto ok = [](int32_t g) { return g == 2 || g == 4 || g == 8 || g == 16 || g == 32; };
     if (!ok(lanes64) || !ok(lanes32)) return set_err(ctx, VFV_BAD_INPUT, "SpMV lanes per row must be 2, 4, 8, 16 or 32");
@@ -2108,6 +2126,7 @@ int vfv_pattern_set_spmv_lanes(vfv_ctx* ctx, vfv_pattern* p, int32_t lanes64, in
 }
 
 int vfv_ilu0_ordering(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int32_t* perm, int32_t* lev_ptr, int32_t* nlev) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !p) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (ilu_order != VFV_ILU_MULTICOLOR && ilu_order != VFV_ILU_NATURAL) return set_err(ctx, VFV_BAD_INPUT, "unknown ILU ordering");
     auto it = p->ilu.find(ilu_order);

@@ -233,6 +233,7 @@ int vfv_flow_pattern_host(const vfv_mesh* mh, int64_t pref_vid, int64_t* nnz, in
 
 int vfv_flow_create(vfv_ctx* ctx, const vfv_mesh* mh, const double* rho, const double* mu, const double* fce, const double* bc_vel,
                     int64_t pref_vid, double pref, vfv_flow** out) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !mh || !rho || !mu || !fce || !bc_vel || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     *out = nullptr;
     const Dual& d = mh->d;
@@ -334,6 +335,7 @@ int vfv_flow_info(const vfv_flow* f, int64_t* n_unknowns, int64_t* nnz, int64_t*
 }
 
 int vfv_flow_assemble_device(vfv_ctx* ctx, vfv_flow* f, const double* x, double* b) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !f || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     int rc = flow_assemble(ctx, f, x);
     if (rc) return rc;
@@ -343,6 +345,7 @@ int vfv_flow_assemble_device(vfv_ctx* ctx, vfv_flow* f, const double* x, double*
 }
 
 int vfv_flow_assemble(vfv_ctx* ctx, vfv_flow* f, const double* x, double* b) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !f || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     CK(cudaMemcpyAsync(f->x.p, x, 4 * f->n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     int rc = flow_assemble(ctx, f, f->x.p);
@@ -354,6 +357,7 @@ int vfv_flow_assemble(vfv_ctx* ctx, vfv_flow* f, const double* x, double* b) {
 
 int vfv_flow_picard(vfv_ctx* ctx, vfv_flow* f, double* x, int max_iter, double tol, double damp, const vfv_gmres_opts* opts,
                     double* res, int32_t* lin_iters, int32_t* iters_done, double* solve_seconds) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !f || !x) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (max_iter <= 0) return set_err(ctx, VFV_BAD_INPUT, "max_iter must be positive (SolverNonPositiveMaxIter)");
     if (!(tol > 0.0)) return set_err(ctx, VFV_BAD_INPUT, "tol must be positive (SolverNonPositiveTolerance)");

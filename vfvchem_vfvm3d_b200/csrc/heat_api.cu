@@ -32,6 +32,7 @@ extern "C" {
 
 // ---------------------------------------------------------------- heat operator
 int vfv_heat_create(vfv_ctx* ctx, const vfv_mesh* mh, int32_t n_bnd, const int32_t* bnd_kind, vfv_heat** out) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !mh || !out || (n_bnd > 0 && !bnd_kind)) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     *out = nullptr;
     const Mesh& m = mh->m;
@@ -107,6 +108,7 @@ int vfv_heat_create(vfv_ctx* ctx, const vfv_mesh* mh, int32_t n_bnd, const int32
 // and their gradients from the last vfv_heat_assemble call.
 int vfv_heat_adjoint(vfv_ctx* ctx, vfv_heat* h, const double* T, const double* dJdT, const vfv_gmres_opts* opts, double* lambda,
                      double* dJdlogk, double* dJdq, vfv_solve_info* info) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !h || !T || !dJdT) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     int rc = check_opts(ctx, opts);
     if (rc) return rc;
@@ -185,6 +187,7 @@ const double* vfv_heat_rhs_device(vfv_heat* h) { return h ? h->b.p : nullptr; }
 
 int vfv_heat_assemble(vfv_ctx* ctx, vfv_heat* h, const double* k, const double* q, const double* s_, const double* T,
                       const double* bc_val, int on_device, double* b_out) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !h || !k || !q || !s_ || !T || !bc_val) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     const int64_t n = h->n;
     cudaStream_t s = ctx->stream;
@@ -236,6 +239,7 @@ int vfv_heat_assemble(vfv_ctx* ctx, vfv_heat* h, const double* k, const double* 
 }
 
 int vfv_update_grad(vfv_ctx* ctx, vfv_heat* h, const double* f, double* grad) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !h || !f || !grad) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     const int64_t n = h->n;
     cudaStream_t s = ctx->stream;

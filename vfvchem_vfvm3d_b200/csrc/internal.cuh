@@ -29,6 +29,23 @@ struct vfv_ctx {
     int64_t launches = 0;           // kernels launched by this context (graph nodes counted per replay)
 };
 
+// Makes a context's device current for the duration of an entry point and gives the calling
+// thread its previous device back afterwards, so one host thread can drive contexts on several
+// devices (kernels, allocations and streams of a context all live on its device).
+struct DeviceGuard {
+    int prev = -1;
+    bool switched = false;
+    explicit DeviceGuard(const vfv_ctx* ctx) {
+        if (ctx && cudaGetDevice(&prev) == cudaSuccess && prev != ctx->device && cudaSetDevice(ctx->device) == cudaSuccess)
+            switched = true;
+    }
+    ~DeviceGuard() {
+        if (switched) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 inline int set_err(vfv_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->err = msg;
     vfv_thread_error() = msg;

@@ -74,6 +74,7 @@ int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, cons
 void vfv_mesh_destroy(vfv_mesh* m) { delete m; }
 
 int vfv_mesh_dual_device(vfv_ctx* ctx, vfv_mesh* m) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !m) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (m->m.tets.empty()) return set_err(ctx, VFV_BAD_INPUT, "mesh has no tetrahedra");
     Dual d;
@@ -84,6 +85,7 @@ int vfv_mesh_dual_device(vfv_ctx* ctx, vfv_mesh* m) {
 }
 
 int vfv_mesh_jitter_cubes_device_dual(vfv_ctx* ctx, int count, const int32_t* n, const uint64_t* seeds, double jitter, vfv_mesh** out) {
+    DeviceGuard dg_(ctx);
     if (!ctx || count <= 0 || !n || !seeds || !out) return set_err(ctx, VFV_BAD_INPUT, "invalid batch arguments");
     for (int i = 0; i < count; ++i) {
         out[i] = nullptr;

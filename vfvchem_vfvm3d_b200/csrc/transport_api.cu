@@ -59,6 +59,7 @@ extern "C" {
 
 // ---------------------------------------------------------------- transient transport (batched meshes)
 int vfv_transport_create(vfv_ctx* ctx, int nmesh, vfv_mesh* const* meshes, double dt, vfv_transport** out) {
+    DeviceGuard dg_(ctx);
     if (!ctx || nmesh <= 0 || !meshes || !out) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (!(dt > 0.0)) return set_err(ctx, VFV_BAD_INPUT, "dt must be positive");
     *out = nullptr;
@@ -154,6 +155,7 @@ int vfv_transport_info(const vfv_transport* t, int64_t* n_tot, int64_t* nnz, int
 }
 
 int vfv_transport_assemble(vfv_ctx* ctx, vfv_transport* t, const double* D, const double* vel, int on_device) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !t || !D || !vel) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     const int64_t n = t->n;
     cudaStream_t s = ctx->stream;
@@ -175,6 +177,7 @@ int vfv_transport_assemble(vfv_ctx* ctx, vfv_transport* t, const double* D, cons
 // per step with the per-mesh stopping rule; the state stays on the device between steps.
 int vfv_transport_run(vfv_ctx* ctx, vfv_transport* t, const double* c0, int nsteps, const vfv_gmres_opts* opts, double* c_out,
                       int32_t* iters) {
+    DeviceGuard dg_(ctx);
     if (!ctx || !t || !c0 || !c_out || nsteps < 0) return set_err(ctx, VFV_BAD_INPUT, "invalid argument");
     int rc = check_opts(ctx, opts);
     if (rc) return rc;
