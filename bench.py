@@ -14,7 +14,8 @@ not finish on 10^6 rows in bench time; that oracle solver agrees with SuperLU to
 rows).
 
 The mixed solver's preconditioner is ILU(0) in the natural order with its triangular solves done
-as ILU_SWEEPS Jacobi sweeps of each factor (bandwidth-bound launches over compact triangles); the
+as ILU_SWEEPS Jacobi sweeps of each factor (bandwidth-bound launches over compact triangles whose
+values are stored in half precision, each row scaled by its largest magnitude); the
 plain FP64 solver is the exact multicolour ILU(0) (level-scheduled sweeps). The FP64 solver with
 the same swept preconditioner and the mixed solver with the exact one are timed beside them.
 
@@ -276,9 +277,10 @@ def extras_transport(ctx, count):
 # lanes per row, from one ncu capture of that launch (profiles/k_spmv_1M.md); reported as the
 # roofline's traffic only when the bench runs that same matrix and lane count.
 SPMV_TRAFFIC_N100_4LANES = 209.2e6
-# DRAM bytes (read + write) of one k_ilu0_sweep<float> launch on the same matrix (4-sweep natural-order
-# factors, 32-bit columns), from one ncu capture of a lower and an upper sweep (profiles/k_ilu0_sweep_1M.md)
-SWEEP_TRAFFIC_N100 = 78.5e6
+# DRAM bytes (read + write) of one k_ilu0_sweep<float, half values> launch on the same matrix (4-sweep
+# natural-order factors, 32-bit columns), from one ncu capture of a lower and an upper sweep
+# (profiles/k_ilu0_sweep_1M.md); None until that capture exists
+SWEEP_TRAFFIC_N100 = None
 
 
 def peaks():
@@ -435,12 +437,13 @@ def main():
     exact = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_MULTICOLOR, engine=args.engine)
     swept = dict(precond=L.PRECOND_ILU0, ilu_order=L.ILU_NATURAL, ilu_sweeps=ILU_SWEEPS, engine=args.engine)
     o64 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, **exact)
-    omx = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, **swept)
+    omx = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, ilu_sweep_half=1,
+                       **swept)
     o64s = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, **swept)
     omxe = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, **exact)
     # the same solvers with one-pass classical Gram-Schmidt (no reorthogonalisation)
     omx1 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.MIXED, inner_rtol=1e-6, ortho=L.ORTHO_CGS,
-                        **swept)
+                        ilu_sweep_half=1, **swept)
     o641 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, ortho=L.ORTHO_CGS, **exact)
     o64s1 = GmresOptions(tol=TOL_RELRES, restart=args.restart, max_outer=2000, precision=L.FP64, ortho=L.ORTHO_CGS, **swept)
 
@@ -503,20 +506,21 @@ def main():
     gbs64 = bytes64 / sp64 / 1e9
     gbs32 = bytes32 / sp32 / 1e9
 
-    # The mixed solve's preconditioner timed alone: ILU_SWEEPS Jacobi sweeps of each float factor
-    # (natural-order ILU(0) in A's numbering; 2 x ILU_SWEEPS k_ilu0_sweep launches per apply).
-    # Algorithmic bytes per sweep: the triangle's row pointer (4 (n+1)), column indices (2 or 4
-    # bytes) and float values (4) of its entries (nl = nu = (nnz - n) / 2 strictly lower / upper
-    # entries), right-hand side, previous iterate and new iterate (12 n), the diagonal for the upper
-    # sweeps (4 n); the last lower sweep also writes D^-1 u (4 n) and reads the diagonal (4 n).
+    # The mixed solve's preconditioner timed alone: ILU_SWEEPS Jacobi sweeps of each factor in float
+    # arithmetic over the row-scaled half-precision values (natural-order ILU(0) in A's numbering;
+    # 2 x ILU_SWEEPS k_ilu0_sweep launches per apply). Algorithmic bytes per sweep: the triangle's
+    # row pointer (4 (n+1)) and row scales (4 n), column indices (2 or 4 bytes) and half values (2)
+    # of its entries (nl = nu = (nnz - n) / 2 strictly lower / upper entries), right-hand side,
+    # previous iterate and new iterate (12 n), the diagonal for the upper sweeps (4 n); the last
+    # lower sweep also writes D^-1 u (4 n) and reads the diagonal (4 n).
     rs32, ts32, zs32 = xs32.clone(), torch.empty_like(xs32), torch.empty_like(xs32)
     torch.cuda.synchronize()
-    pat.ilu0_sweep_apply_device(rs32.data_ptr(), zs32.data_ptr(), ILU_SWEEPS, L.ILU_NATURAL, f32=True)
-    ilu_s = kernel_time(lambda: pat.ilu0_sweep_apply_device(rs32.data_ptr(), zs32.data_ptr(), ILU_SWEEPS, L.ILU_NATURAL, f32=True))
+    pat.ilu0_sweep_apply_device(rs32.data_ptr(), zs32.data_ptr(), ILU_SWEEPS, L.ILU_NATURAL, half=True)
+    ilu_s = kernel_time(lambda: pat.ilu0_sweep_apply_device(rs32.data_ptr(), zs32.data_ptr(), ILU_SWEEPS, L.ILU_NATURAL, half=True))
     col_bytes = pat.ilu0_sweep_layout(L.ILU_NATURAL)
     ilu_launches = 2 * ILU_SWEEPS
     ntri = (nnz - n) // 2
-    bytes_ilu32 = ILU_SWEEPS * (2 * 4 * (n + 1) + (col_bytes + 4) * 2 * ntri + 28 * n) + 8 * n
+    bytes_ilu32 = ILU_SWEEPS * (2 * 4 * (n + 1) + (col_bytes + 2) * 2 * ntri + 36 * n) + 8 * n
     gbs_ilu32 = bytes_ilu32 / ilu_s / 1e9
     # the exact level-scheduled float apply (the FP64 baseline's preconditioner structure), for context
     ilu_nlev = pat.ilu0_apply_device_f32(rs32.data_ptr(), ts32.data_ptr(), zs32.data_ptr())
@@ -586,7 +590,8 @@ def main():
         "fp64_solve_s": f64_s,
         "speedup_mixed_vs_fp64": f64_s / mx_s,
         "solvers": {
-            "mixed": f"FP32 GMRES({args.restart}) cycles in FP64 refinement, ILU(0) natural order, {ILU_SWEEPS} Jacobi sweeps per factor",
+            "mixed": f"FP32 GMRES({args.restart}) cycles in FP64 refinement, ILU(0) natural order, {ILU_SWEEPS} Jacobi sweeps per factor "
+                     "over row-scaled half-precision factor values",
             "fp64": f"FP64 GMRES({args.restart}), exact multicolour ILU(0) ({ilu_nlev} colour levels, level-scheduled sweeps)",
             "fp64_same_precond": "FP64 GMRES with the mixed solver's preconditioner",
             "mixed_exact_ilu": "the mixed solver with the FP64 solver's exact multicolour ILU(0)"},
@@ -601,8 +606,8 @@ def main():
         "iters_mixed_exact_ilu": i_mxe[-1].iters, "ilu_levels": ilu_nlev,
         "err_mixed": e_mx, "err_fp64": e_64, "err_fp64_same_precond": e_64s, "err_mixed_exact_ilu": e_mxe, "err_target": ERR_TARGET,
         "nnz": nnz, "engine": args.engine,
-        "roofline": {"bound": "hbm", "kernel": f"k_ilu0_sweep<float> (Jacobi sweeps of the ILU(0) factors, {ilu_launches} launches per apply, "
-                                                f"{col_bytes}-byte columns)",
+        "roofline": {"bound": "hbm", "kernel": f"k_ilu0_sweep<float, half values> (Jacobi sweeps of the ILU(0) factors, {ilu_launches} "
+                                                f"launches per apply, {col_bytes}-byte columns)",
                      "achieved": gbs_ilu32, "peak": peak, "unit": "GB/s", "frac": gbs_ilu32 / peak, "peak_kind": peak_kind,
                      "traffic": SWEEP_TRAFFIC_N100 if args.n == 100 else None,
                      "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",

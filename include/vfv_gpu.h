@@ -92,6 +92,9 @@ typedef struct {
     int32_t ilu_sweeps_upper; /* with ilu_sweeps > 0: Jacobi sweeps of the upper factor, in [1, 16] (0 = ilu_sweeps) */
     int32_t ortho;      /* VFV_ORTHO_*: Gram-Schmidt of each Arnoldi step (graph and overlapped engines; batches of
                            meshes and the persistent engine use CGS2) */
+    int32_t ilu_sweep_half; /* VFV_MIXED with ilu_sweeps > 0: nonzero stores the swept factors' values in half
+                               precision, each row divided by its largest magnitude (kept in float beside it), so
+                               every stored value lies in [-1, 1]; the sweeps still compute in float */
 } vfv_gmres_opts;
 
 typedef struct {
@@ -166,6 +169,8 @@ int vfv_ilu0_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const
  * r and z may alias. */
 int vfv_ilu0_sweep_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const double* r, double* z);
 int vfv_ilu0_sweep_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const float* r, float* z);
+/* the same with the row-scaled half-precision values of vfv_gmres_opts::ilu_sweep_half */
+int vfv_ilu0_sweep_apply_device_f16(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const float* r, float* z);
 /* Storage of the swept factors once built: bytes per column index (2: 16-bit offsets from the row,
  * when the factor's bandwidth allows; 4: absolute). */
 int vfv_ilu0_sweep_layout(const vfv_pattern* p, int ilu_order, int32_t* col_bytes);

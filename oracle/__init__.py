@@ -185,20 +185,32 @@ class Ilu0:
         lib().orc_ilu0_apply(C.c_int64(self.n), _p(self.rp), _p(self.ci), _p(self.dg), _p(self.lu), _p(self.perm), _p(r), _p(t), _p(z))
         return z
 
-    def sweep_apply(self, r, sweeps: int):
+    def sweep_apply(self, r, sweeps: int, half: bool = False):
         """z = M^-1 r with `sweeps` Jacobi sweeps of each factor instead of the exact triangular
         solves (Anzt, Chow & Dongarra, "Iterative sparse triangular solves for preconditioning",
         Euro-Par 2015), on L = I + N, U = D + S of this factor:
             u^0 = y = P r,   u^k = y - N u^(k-1);   w^0 = D^-1 u,   w^k = D^-1 (u - S w^(k-1));
         z = P^T w^sweeps. The iterates do not depend on the numbering (every row of a sweep reads
-        only the previous sweep)."""
+        only the previous sweep). half: N and S as the mixed solver's half-precision copies of the
+        float factor: per row and triangle, the values divided by the row's largest magnitude
+        (computed in float), rounded to half, and the row's sum multiplied back by that scale."""
         n = self.n
         rows = np.repeat(np.arange(n), np.diff(self.rp))
         low, up = self.ci < rows, self.ci > rows
         d = self.lu[self.dg]
+        vals = self.lu
+        if half:
+            v32 = self.lu.astype(np.float32)
+            vals = np.empty(self.lu.size)
+            for mask in (low, up):
+                sc = np.zeros(n, np.float32)
+                np.maximum.at(sc, rows[mask], np.abs(v32[mask]))
+                sc[sc == 0] = 1.0
+                h = (v32[mask] / sc[rows[mask]]).astype(np.float16)
+                vals[mask] = h.astype(np.float64) * sc[rows[mask]].astype(np.float64)
 
         def tri(mask, x):
-            return np.bincount(rows[mask], weights=self.lu[mask] * x[self.ci[mask]], minlength=n)
+            return np.bincount(rows[mask], weights=vals[mask] * x[self.ci[mask]], minlength=n)
 
         y = _c(r, np.float64)[self.perm]
         u = y.copy()

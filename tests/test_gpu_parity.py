@@ -260,6 +260,10 @@ def test_ilu0_sweep_apply_matches_oracle(gpu_ctx, c1h_system, c1_hetero, order, 
     p.ilu0_sweep_apply_device(rf.data_ptr(), zf.data_ptr(), sweeps, order, f32=True)
     gpu_ctx.synchronize()
     assert _rel(zf.cpu().numpy().astype(np.float64), ilu.sweep_apply(r32.astype(np.float64), sweeps)) <= 1e-5
+    zh = torch.empty_like(rf)  # the row-scaled half-precision values
+    p.ilu0_sweep_apply_device(rf.data_ptr(), zh.data_ptr(), sweeps, order, half=True)
+    gpu_ctx.synchronize()
+    assert _rel(zh.cpu().numpy().astype(np.float64), ilu.sweep_apply(r32.astype(np.float64), sweeps, half=True)) <= 1e-5
 
 
 @pytest.fixture(scope="module")
@@ -335,6 +339,27 @@ def test_gmres_matches_lu(gpu_ctx, c1h_system, c1_hetero, precond, precision, en
     x, info = p.solve(b, c1_hetero.T0, opts)
     assert info.status == 0 and info.relres <= 1e-12
     assert _rel(x, xl) <= SOL_RTOL
+
+
+@pytest.mark.parametrize("engine", [1, 2])
+@pytest.mark.parametrize("order", [0, 1])
+def test_gmres_ilu_sweeps_half_matches_lu(gpu_ctx, c1h_system, c1_hetero, order, engine):
+    """The mixed solver with the swept factors in row-scaled half precision: the same bars against LU
+    (the FP64 refinement keeps the answer exact); refused outside that combination."""
+    from vfvchem_vfvm3d_b200 import GmresOptions, Pattern, VFVChemError
+    (rp, ci, va), b, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    xl = lu_solve(rp, ci, va, b)
+    opts = GmresOptions(tol=1e-12, restart=30, max_outer=2000, precond=2, precision=1, ilu_order=order, ilu_sweeps=3, ilu_sweep_half=1,
+                        inner_rtol=1e-6, engine=engine)
+    x, info = p.solve(b, c1_hetero.T0, opts)
+    assert info.status == 0 and info.relres <= 1e-12
+    assert _rel(x, xl) <= SOL_RTOL
+    with pytest.raises(VFVChemError):
+        p.solve(b, None, GmresOptions(precond=2, ilu_sweeps=3, ilu_sweep_half=1))  # FP64
+    with pytest.raises(VFVChemError):
+        p.solve(b, None, GmresOptions(precond=2, precision=1, ilu_sweep_half=1))  # exact ILU(0)
 
 
 @pytest.mark.parametrize("ortho", [1, 2])

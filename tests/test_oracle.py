@@ -224,6 +224,8 @@ def test_oracle_ilu0_sweeps(c1h_system):
     z = np.empty(n)
     z[perm] = w
     assert np.linalg.norm(ilu.sweep_apply(r, 2) - z) <= 1e-13 * np.linalg.norm(z)
+    zh = ilu.sweep_apply(r, 2, half=True)  # half-precision copies: close to, but not, the float sweeps
+    assert 1e-7 < np.linalg.norm(zh - z) / np.linalg.norm(z) < 1e-2
     pn, _ = ordering.natural(rp, ci)
     za = oracle.Ilu0(rp, ci, va, pn).sweep_apply(r, 3)
     zb = oracle.Ilu0(rp, ci, va, np.arange(n, dtype=np.int32)).sweep_apply(r, 3)

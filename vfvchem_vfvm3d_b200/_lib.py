@@ -36,6 +36,7 @@ class GmresOpts(C.Structure):
         ("ilu_sweeps", C.c_int32),
         ("ilu_sweeps_upper", C.c_int32),
         ("ortho", C.c_int32),
+        ("ilu_sweep_half", C.c_int32),
     ]
 
 
@@ -81,6 +82,7 @@ SIGNATURES = [
     ("vfv_ilu0_apply_device_f32", C.c_int, [_P, _P, C.c_int, _P, _P, _P, _I32P]),
     ("vfv_ilu0_sweep_apply_device", C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
     ("vfv_ilu0_sweep_apply_device_f32", C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
+    ("vfv_ilu0_sweep_apply_device_f16", C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
     ("vfv_ilu0_sweep_layout", C.c_int, [_P, C.c_int, _I32P]),
     ("vfv_pattern_autotune", C.c_int, [_P, _P, _I32P, _I32P]),
     ("vfv_pattern_set_spmv_lanes", C.c_int, [_P, _P, C.c_int32, C.c_int32]),

@@ -34,6 +34,7 @@ class GmresOptions:
     ilu_sweeps: int = 0  # ILU(0): 0 exact triangular solves, k > 0 k Jacobi sweeps of each factor
     ilu_sweeps_upper: int = 0  # with ilu_sweeps > 0: sweeps of the upper factor (0: ilu_sweeps)
     ortho: int = L.ORTHO_CGS2  # Gram-Schmidt: two passes, a second pass only when needed (DGKS), or one pass
+    ilu_sweep_half: int = 0  # mixed + ilu_sweeps: swept factors stored as row-scaled half-precision values
 
     def to_c(self) -> L.GmresOpts:
         o = L.GmresOpts()
@@ -45,6 +46,7 @@ class GmresOptions:
         o.ilu_sweeps = int(self.ilu_sweeps)
         o.ilu_sweeps_upper = int(self.ilu_sweeps_upper)
         o.ortho = int(self.ortho)
+        o.ilu_sweep_half = int(self.ilu_sweep_half)
         return o
 
 
@@ -209,10 +211,13 @@ class Pattern:
                                                                    C.c_void_p(t_ptr), C.c_void_p(z_ptr), C.byref(lev)))
         return lev.value
 
-    def ilu0_sweep_apply_device(self, r_ptr: int, z_ptr: int, sweeps: int, order: int = L.ILU_MULTICOLOR, f32: bool = False) -> None:
-        """z = M^-1 r with `sweeps` Jacobi sweeps of each ILU(0) factor (double, or the float factor
-        with f32), enqueued on the context's stream (no synchronisation)."""
-        fn = L.load().vfv_ilu0_sweep_apply_device_f32 if f32 else L.load().vfv_ilu0_sweep_apply_device
+    def ilu0_sweep_apply_device(self, r_ptr: int, z_ptr: int, sweeps: int, order: int = L.ILU_MULTICOLOR, f32: bool = False,
+                                half: bool = False) -> None:
+        """z = M^-1 r with `sweeps` Jacobi sweeps of each ILU(0) factor (double, the float factor
+        with f32, its row-scaled half-precision values with half; float vectors for both), enqueued
+        on the context's stream (no synchronisation)."""
+        lib = L.load()
+        fn = lib.vfv_ilu0_sweep_apply_device_f16 if half else lib.vfv_ilu0_sweep_apply_device_f32 if f32 else lib.vfv_ilu0_sweep_apply_device
         _check(self.ctx.handle, fn(self.ctx.handle, self._h, int(order), int(sweeps), C.c_void_p(r_ptr), C.c_void_p(z_ptr)))
 
     def ilu0_sweep_layout(self, order: int = L.ILU_MULTICOLOR) -> int:

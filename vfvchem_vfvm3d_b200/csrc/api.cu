@@ -454,7 +454,7 @@ DBuf<T>& of_prec(DBuf<double>& d, DBuf<float>& f) {
 // swept in A's own numbering (A's rows with the factor's values scattered back to A's slots), the
 // multicolour ordering in its factor's permuted numbering.
 template <typename T>
-int ilu_split_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S) {
+int ilu_split_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool half = false) {
     cudaStream_t s = ctx->stream;
     const int64_t n = p->n, nnz = p->nnz;
     IluStruct::Split& X = S.split;
@@ -512,7 +512,8 @@ int ilu_split_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S) {
     }
     constexpr bool dbl = std::is_same<T, double>::value;
     uint64_t& ver = dbl ? X.version64 : X.version32;
-    if (ver == p->version) return VFV_OK;
+    const int64_t nlow = X.delta16 ? (int64_t)X.lcd.n : (int64_t)X.lci.n, nup = X.delta16 ? (int64_t)X.ucd.n : (int64_t)X.uci.n;
+    if (ver != p->version) {
     const T* lu = of_prec<T>(S.lu64, S.lu32).p;
     const int32_t *rp = S.rp.p, *dg = S.dg.p;
     if (nat) {  // the factor's values back in A's slot order
@@ -527,7 +528,6 @@ int ilu_split_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S) {
     DBuf<T>& lv = of_prec<T>(X.lv64, X.lv32);
     DBuf<T>& uv = of_prec<T>(X.uv64, X.uv32);
     DBuf<T>& dv = of_prec<T>(X.d64, X.d32);
-    const int64_t nlow = X.delta16 ? (int64_t)X.lcd.n : (int64_t)X.lci.n, nup = X.delta16 ? (int64_t)X.ucd.n : (int64_t)X.uci.n;
     if (!lv.p) CK(lv.alloc(std::max<int64_t>(nlow, 1)));
     if (!uv.p) CK(uv.alloc(std::max<int64_t>(nup, 1)));
     if (!dv.p) CK(dv.alloc(n));
@@ -535,6 +535,20 @@ int ilu_split_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S) {
     ctx->launches += 1;
     CK(cudaGetLastError());
     ver = p->version;
+    }
+    if constexpr (!dbl) {  // the row-scaled half copies of the float values, when asked for
+        if (half && X.version_half != p->version) {
+            if (!X.lvh.p) CK(X.lvh.alloc(std::max<int64_t>(nlow, 1)));
+            if (!X.uvh.p) CK(X.uvh.alloc(std::max<int64_t>(nup, 1)));
+            if (!X.lsc.p) CK(X.lsc.alloc(n));
+            if (!X.usc.p) CK(X.usc.alloc(n));
+            k_half_rows<<<grid_for(n), 256, 0, s>>>((int32_t)n, X.lrp.p, X.lv32.p, reinterpret_cast<__half*>(X.lvh.p), X.lsc.p);
+            k_half_rows<<<grid_for(n), 256, 0, s>>>((int32_t)n, X.urp.p, X.uv32.p, reinterpret_cast<__half*>(X.uvh.p), X.usc.p);
+            ctx->launches += 2;
+            CK(cudaGetLastError());
+            X.version_half = p->version;
+        }
+    }
     return VFV_OK;
 }
 
@@ -547,12 +561,21 @@ struct SweepOps {
     const int32_t *lrp = nullptr, *urp = nullptr, *perm = nullptr;
     const void *lcols = nullptr, *ucols = nullptr;
     const T *lv = nullptr, *uv = nullptr, *d = nullptr;
+    // float factors only: the row-scaled half-precision values and their row scales (vfv_gmres_opts::ilu_sweep_half)
+    const __half *lvh = nullptr, *uvh = nullptr;
+    const float *lsc = nullptr, *usc = nullptr;
 };
 
 template <typename T>
-SweepOps<T> sweep_ops(const vfv_pattern* p, IluStruct& S) {
+SweepOps<T> sweep_ops(const vfv_pattern* p, IluStruct& S, bool half = false) {
     IluStruct::Split& X = S.split;
     SweepOps<T> o;
+    if (half && std::is_same<T, float>::value) {
+        o.lvh = reinterpret_cast<const __half*>(X.lvh.p);
+        o.uvh = reinterpret_cast<const __half*>(X.uvh.p);
+        o.lsc = X.lsc.p;
+        o.usc = X.usc.p;
+    }
     o.n = (int32_t)p->n;
     o.lanes = std::is_same<T, double>::value ? 2 : 1;
     if (const char* e = getenv("VFV_SWEEP_LANES")) {
@@ -576,8 +599,14 @@ template <typename T, typename TC, bool LOWER, int G>
 cudaError_t launch_sweep_g(cudaLaunchConfig_t& cfg, const SweepOps<T>& o, const T* rhs, const T* prev, T* next, T* w0, T* out,
                            const DevStatus* st) {
     cfg.gridDim = dim3((unsigned)grid_for((int64_t)o.n * G, kSwBlock));
-    return cudaLaunchKernelEx(&cfg, k_ilu0_sweep<T, TC, LOWER, G>, o.n, LOWER ? o.lrp : o.urp,
-                              (const TC*)(LOWER ? o.lcols : o.ucols), LOWER ? o.lv : o.uv, o.d, o.perm, rhs, prev, next, w0, out, st);
+    if constexpr (std::is_same<T, float>::value) {
+        if (o.lvh)
+            return cudaLaunchKernelEx(&cfg, k_ilu0_sweep<T, TC, LOWER, G, __half>, o.n, LOWER ? o.lrp : o.urp,
+                                      (const TC*)(LOWER ? o.lcols : o.ucols), LOWER ? o.lvh : o.uvh, LOWER ? o.lsc : o.usc, o.d, o.perm,
+                                      rhs, prev, next, w0, out, st);
+    }
+    return cudaLaunchKernelEx(&cfg, k_ilu0_sweep<T, TC, LOWER, G, T>, o.n, LOWER ? o.lrp : o.urp, (const TC*)(LOWER ? o.lcols : o.ucols),
+                              LOWER ? o.lv : o.uv, (const float*)nullptr, o.d, o.perm, rhs, prev, next, w0, out, st);
 }
 
 template <typename T, bool LOWER>
@@ -753,6 +782,7 @@ struct Gmres : SolverBase {
     int ilu_prio = 0;  // greatest stream priority: the sweeps' blocks go first when SM slots free up
     bool ilu_chain = false;  // ILU(0) sweeps as one k_ilu0_chain launch (VFV_ILU_CHAIN=1) instead of one launch per level
     int ortho = VFV_ORTHO_CGS2;  // Gram-Schmidt of the Arnoldi steps (vfv_gmres_opts::ortho)
+    bool sweep_half = false;     // float solver: swept factors in row-scaled half precision (vfv_gmres_opts::ilu_sweep_half)
     DBuf<double> wn2;            // ||w||^2 for the reorthogonalisation test
     int sweeps = 0;          // > 0: ILU(0) applied by this many Jacobi sweeps of the lower factor (vfv_gmres_opts::ilu_sweeps)
     int usweeps = 0;         // and this many of the upper factor (ilu_sweeps_upper, or ilu_sweeps when 0)
@@ -776,7 +806,8 @@ struct Gmres : SolverBase {
         if (s2) cudaStreamDestroy(s2);
     }
 
-    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_, int sweeps_, int usweeps_, int ortho_) {
+    int init(vfv_ctx* ctx, vfv_pattern* p, int m_, int precond_, int ilu_order_, int engine_, int sweeps_, int usweeps_, int ortho_,
+             bool sweep_half_) {
         n = p->n;
         m = m_;
         precond = precond_;
@@ -785,6 +816,7 @@ struct Gmres : SolverBase {
         sweeps = precond == VFV_PRECOND_ILU0 ? sweeps_ : 0;
         usweeps = sweeps > 0 ? (usweeps_ > 0 ? usweeps_ : sweeps) : 0;
         ortho = ortho_;
+        sweep_half = sweep_half_ && sweeps > 0 && !std::is_same<T, double>::value;
         ldv = (n + 63) / 64 * 64;
         nblk_v = (int)((n + vec_block_rows<T>() - 1) / vec_block_rows<T>());
         nblk = nblk_v;  // partial dots per vector
@@ -1336,9 +1368,9 @@ struct Gmres : SolverBase {
         }
         if (precond == VFV_PRECOND_ILU0) {
             int rc = ilu_refresh(ctx, p, *ilu, mixed);
-            if (!rc && sweeps > 0) rc = ilu_split_refresh<T>(ctx, p, *ilu);
+            if (!rc && sweeps > 0) rc = ilu_split_refresh<T>(ctx, p, *ilu, sweep_half);
             if (rc) return rc;
-            if (sweeps > 0) sw_ops = sweep_ops<T>(p, *ilu);
+            if (sweeps > 0) sw_ops = sweep_ops<T>(p, *ilu, sweep_half);
         }
         if (precond == VFV_PRECOND_BJ4 && bj_version != p->version) {
             CK(cudaMemsetAsync(bj_bad.p, 0, sizeof(int), s));
@@ -1530,6 +1562,8 @@ int check_opts(vfv_ctx* ctx, const vfv_gmres_opts* o) {
     if (o->ilu_sweeps < 0 || o->ilu_sweeps > kMaxIluSweeps) return set_err(ctx, VFV_BAD_INPUT, "ilu_sweeps must be in [0, 16]");
     if (o->ilu_sweeps_upper < 0 || o->ilu_sweeps_upper > kMaxIluSweeps)
         return set_err(ctx, VFV_BAD_INPUT, "ilu_sweeps_upper must be in [0, 16]");
+    if (o->ilu_sweep_half != 0 && (o->precond != VFV_PRECOND_ILU0 || o->ilu_sweeps == 0 || o->precision != VFV_MIXED))
+        return set_err(ctx, VFV_BAD_INPUT, "ilu_sweep_half needs the mixed precision and ILU(0) with ilu_sweeps > 0");
     if (o->ortho != VFV_ORTHO_CGS2 && o->ortho != VFV_ORTHO_DGKS && o->ortho != VFV_ORTHO_CGS)
         return set_err(ctx, VFV_BAD_INPUT, "unknown orthogonalisation");
     if (o->ortho != VFV_ORTHO_CGS2 && o->engine == VFV_ENGINE_PERSISTENT)
@@ -1554,12 +1588,14 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
         int rc;
         if (oo.precision == VFV_MIXED) {
             auto g = std::make_unique<Gmres<float>>();
-            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper, batched ? VFV_ORTHO_CGS2 : oo.ortho);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper, batched ? VFV_ORTHO_CGS2 : oo.ortho,
+                         oo.ilu_sweep_half != 0);
             if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         } else {
             auto g = std::make_unique<Gmres<double>>();
-            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper, batched ? VFV_ORTHO_CGS2 : oo.ortho);
+            rc = g->init(ctx, p, oo.restart, oo.precond, oo.ilu_order, oo.engine, oo.ilu_sweeps, oo.ilu_sweeps_upper, batched ? VFV_ORTHO_CGS2 : oo.ortho,
+                         oo.ilu_sweep_half != 0);
             if (!rc && batched) rc = g->init_batch(ctx, p->blocks);
             sb = std::move(g);
         }
@@ -1575,7 +1611,8 @@ int solve_dev(vfv_ctx* ctx, vfv_pattern* p, const double* b, const double* x0, d
 std::tuple<int, int, int, int, int> solver_key(const vfv_gmres_opts& o, bool batched) {
     const bool ilu = o.precond == VFV_PRECOND_ILU0;
     const int up = o.ilu_sweeps > 0 ? (o.ilu_sweeps_upper > 0 ? o.ilu_sweeps_upper : o.ilu_sweeps) : 0;
-    return std::make_tuple(o.precision, o.precond, ilu ? o.ilu_order + 16 * (o.ilu_sweeps + 32 * up) : 0, o.restart,
+    return std::make_tuple(o.precision, o.precond, ilu ? o.ilu_order + 16 * (o.ilu_sweeps + 32 * up + 1024 * (o.ilu_sweep_half != 0)) : 0,
+                           o.restart,
                            (batched ? VFV_ENGINE_GRAPH : o.engine) + (batched ? 16 : 64 * o.ortho));
 }
 
@@ -1664,6 +1701,7 @@ void vfv_gmres_default_opts(vfv_gmres_opts* o) {
     o->ilu_sweeps = 0;
     o->ilu_sweeps_upper = 0;
     o->ortho = VFV_ORTHO_CGS2;
+    o->ilu_sweep_half = 0;
 }
 
 int vfv_ctx_create(int device, vfv_ctx** out) {
@@ -1914,18 +1952,18 @@ int ilu_for_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, IluStruct** out) 
 // double or with the float copy of the factor. Enqueued on the context's stream with no
 // synchronisation; calls after the first for a pattern, ordering and precision allocate nothing.
 template <typename T>
-int sweep_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const T* r, T* z) {
+int sweep_apply(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const T* r, T* z, bool half = false) {
     if (!ctx || !p || !r || !z) return set_err(ctx, VFV_BAD_INPUT, "NULL argument");
     if (sweeps < 1 || sweeps > kMaxIluSweeps) return set_err(ctx, VFV_BAD_INPUT, "sweeps must be in [1, 16]");
     IluStruct* S = nullptr;
     int rc = ilu_for_apply<T>(ctx, p, ilu_order, &S);
-    if (!rc) rc = ilu_split_refresh<T>(ctx, p, *S);
+    if (!rc) rc = ilu_split_refresh<T>(ctx, p, *S, half);
     if (rc) return rc;
     DBuf<unsigned char>& W = S->sweep_work[chain_slot<T>()];
     if (!W.p) CK(W.alloc((size_t)5 * p->n * sizeof(T)));
     T* buf[5];
     for (int q = 0; q < 5; ++q) buf[q] = reinterpret_cast<T*>(W.p) + (size_t)q * p->n;
-    const SweepOps<T> o = sweep_ops<T>(p, *S);
+    const SweepOps<T> o = sweep_ops<T>(p, *S, half);
     ilu_apply_sweeps<T>(ctx->stream, o, sweeps, sweeps, r, z, buf, nullptr);
     ctx->launches += 2 * sweeps + (o.perm ? 1 : 0);
     CK(cudaGetLastError());
@@ -1975,6 +2013,11 @@ int vfv_ilu0_sweep_apply_device(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int
 int vfv_ilu0_sweep_apply_device_f32(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const float* r, float* z) {
     DeviceGuard dg_(ctx);
     return sweep_apply<float>(ctx, p, ilu_order, sweeps, r, z);
+}
+
+int vfv_ilu0_sweep_apply_device_f16(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int sweeps, const float* r, float* z) {
+    DeviceGuard dg_(ctx);
+    return sweep_apply<float>(ctx, p, ilu_order, sweeps, r, z, true);
 }
 
 int vfv_ilu0_sweep_layout(const vfv_pattern* p, int ilu_order, int32_t* col_bytes) {

@@ -124,7 +124,9 @@ struct IluStruct {
         DBuf<int32_t> lci, uci;
         DBuf<double> lv64, uv64, d64;
         DBuf<float> lv32, uv32, d32;
-        uint64_t version64 = ~0ull, version32 = ~0ull;
+        DBuf<uint16_t> lvh, uvh;  // half-precision copies of lv32 / uv32 divided by their row scales
+        DBuf<float> lsc, usc;     // row scales: the largest magnitude of the row in each triangle
+        uint64_t version64 = ~0ull, version32 = ~0ull, version_half = ~0ull;
     } split;
     DBuf<double> nat64;
     DBuf<float> nat32;

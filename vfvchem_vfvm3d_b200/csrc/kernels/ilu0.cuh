@@ -13,6 +13,8 @@
 #pragma once
 #include "../common.cuh"
 
+#include <cuda_fp16.h>
+
 namespace vfv {
 
 // Programmatic dependent launch: let the next kernel of the stream start its prologue / wait until
@@ -256,9 +258,17 @@ __device__ __forceinline__ int32_t sweep_col(TC c, int32_t row) {
 // LOWER: next[i] = rhs[i] - sum_k val[k] prev[col k]; w0 (if set) also gets next[i] / d[i].
 // UPPER: w[i] = (rhs[i] - sum_k val[k] prev[col k]) / d[i], stored to next[i], or to out[perm[i]]
 //        (out[i] without perm) on the last sweep (out set).
-template <typename T, typename TC, bool LOWER, int G>
+// TV: the stored value type, T or (for float) __half; half values are stored divided by their row's
+// largest magnitude in that triangle, rs[i], and the row's sum is multiplied back by it.
+template <typename T>
+__device__ __forceinline__ T sweep_val(T v) {
+    return v;
+}
+__device__ __forceinline__ float sweep_val(__half v) { return __half2float(v); }
+
+template <typename T, typename TC, bool LOWER, int G, typename TV = T>
 __global__ void __launch_bounds__(kSwBlock) k_ilu0_sweep(int32_t n, const int32_t* __restrict__ rowp, const TC* __restrict__ cols,
-                                                         const T* __restrict__ val, const T* __restrict__ d,
+                                                         const TV* __restrict__ val, const float* __restrict__ rs, const T* __restrict__ d,
                                                          const int32_t* __restrict__ perm, const T* rhs, const T* prev, T* next, T* w0,
                                                          T* out, const DevStatus* __restrict__ st) {
     const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -276,7 +286,7 @@ __global__ void __launch_bounds__(kSwBlock) k_ilu0_sweep(int32_t n, const int32_
     for (int q = 0; q < kSwK; ++q) {
         const int32_t k = kb + lane + q * G;
         c[q] = k < ke ? sweep_col<TC>(__ldg(cols + k), i) : -1;
-        v[q] = k < ke ? __ldg(val + k) : T(0);
+        v[q] = k < ke ? (T)sweep_val(__ldg(val + k)) : T(0);
     }
     pdl_launch_dependents();
     pdl_wait();
@@ -285,10 +295,11 @@ __global__ void __launch_bounds__(kSwBlock) k_ilu0_sweep(int32_t n, const int32_
 #pragma unroll
     for (int q = 0; q < kSwK; ++q)
         if (c[q] >= 0) s += v[q] * prev[c[q]];
-    for (int32_t k = kb + lane + kSwK * G; k < ke; k += G) s += __ldg(val + k) * prev[sweep_col<TC>(__ldg(cols + k), i)];
+    for (int32_t k = kb + lane + kSwK * G; k < ke; k += G) s += (T)sweep_val(__ldg(val + k)) * prev[sweep_col<TC>(__ldg(cols + k), i)];
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
     if (i >= n || lane != 0) return;
+    if (rs) s *= (T)__ldg(rs + i);
     if (LOWER) {
         const T u = rhs[i] - s;
         next[i] = u;
@@ -322,6 +333,21 @@ __global__ void k_perm_gather(int32_t n, const int32_t* __restrict__ perm, const
     pdl_launch_dependents();
     const int32_t i = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
     if (i < n) y[i] = in[__ldg(perm + i)];
+}
+
+// Half-precision copies of the compact triangles' float values, row-scaled: scale[i] = the row's
+// largest magnitude in the triangle (1 for an empty or all-zero row), h[k] = half(v[k] / scale[i])
+// rounded to nearest, so every stored value lies in [-1, 1] whatever the matrix's scaling.
+__global__ void k_half_rows(int32_t n, const int32_t* __restrict__ rowp, const float* __restrict__ v, __half* __restrict__ h,
+                            float* __restrict__ scale) {
+    const int32_t i = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= n) return;
+    const int32_t b = rowp[i], e = rowp[i + 1];
+    float m = 0.f;
+    for (int32_t k = b; k < e; ++k) m = fmaxf(m, fabsf(v[k]));
+    const float sc = m > 0.f ? m : 1.f;
+    scale[i] = sc;
+    for (int32_t k = b; k < e; ++k) h[k] = __float2half_rn(v[k] / sc);
 }
 
 // Factor values back in A's own slot order (natural ordering): out[src[k]] = lu[k].

@@ -1,6 +1,6 @@
 """Standard workloads of this package, runnable from the command line (for timing and profiling).
 
-    python -m vfvchem_vfvm3d_b200.workloads heat --n 100 --solves 1 --precision mixed --engine 2 --sweeps 4
+    python -m vfvchem_vfvm3d_b200.workloads heat --n 100 --solves 1 --precision mixed --engine 2 --sweeps 4 --half
     python -m vfvchem_vfvm3d_b200.workloads flow --n 32 --picard 2 --precision mixed
     python -m vfvchem_vfvm3d_b200.workloads transport --count 16 --steps 5
     python -m vfvchem_vfvm3d_b200.workloads spmv --n 100 --reps 3 --lanes 4,4
@@ -36,7 +36,8 @@ def heat(args):
     h.pattern.autotune()
     opts = GmresOptions(tol=1e-10, restart=50, max_outer=2000, precond=L.PRECOND_ILU0,
                         precision=L.MIXED if args.precision == "mixed" else L.FP64, inner_rtol=1e-6, engine=args.engine,
-                        ilu_order=L.ILU_NATURAL if args.sweeps > 0 else L.ILU_MULTICOLOR, ilu_sweeps=args.sweeps)
+                        ilu_order=L.ILU_NATURAL if args.sweeps > 0 else L.ILU_MULTICOLOR, ilu_sweeps=args.sweeps,
+                        ilu_sweep_half=1 if args.half else 0)
     if args.solves == 0:
         print(f"heat n={prob.n} nnz={h.pattern.nnz}: assembled")
     for _ in range(args.solves):
@@ -110,6 +111,7 @@ def main(argv=None):
     a.add_argument("--engine", type=int, default=2)
     a.add_argument("--sweeps", type=int, default=0,
                    help="ILU(0) applied by this many Jacobi sweeps per factor in the natural order (0: exact multicolour ILU(0))")
+    a.add_argument("--half", action="store_true", help="mixed + sweeps: the swept factors' values in row-scaled half precision")
     a = sub.add_parser("flow")
     a.add_argument("--n", type=int, default=32)
     a.add_argument("--picard", type=int, default=2)
