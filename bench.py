@@ -279,8 +279,8 @@ def extras_transport(ctx, count):
 SPMV_TRAFFIC_N100_4LANES = 209.2e6
 # DRAM bytes (read + write) of one k_ilu0_sweep<float, half values> launch on the same matrix (4-sweep
 # natural-order factors, 32-bit columns), from one ncu capture of a lower and an upper sweep
-# (profiles/k_ilu0_sweep_1M.md); None until that capture exists
-SWEEP_TRAFFIC_N100 = None
+# (profiles/k_ilu0_sweep_1M.md)
+SWEEP_TRAFFIC_N100 = 66.1e6
 
 
 def peaks():
