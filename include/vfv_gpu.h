@@ -81,9 +81,10 @@ typedef struct {
     int32_t engine;    /* VFV_ENGINE_*: how a restart cycle is launched */
     double inner_rtol; /* VFV_MIXED: an inner cycle also ends once its estimate drops by this factor (0 = full cycles) */
     int64_t wait_limit; /* polls before a bounded device wait gives up (0 = default 20,000,000; any wait also
-                           ends after 2 s): the persistent engine's grid barriers and the single-launch
-                           ILU(0) sweeps. A wait that gives up makes the solve return VFV_TIMEOUT and
-                           leaves the context usable. */
+                           ends after 2 s): the persistent engine's grid barriers, the single-launch
+                           ILU(0) sweeps and the dataflow ILU(0) factorisation (orderings with many
+                           levels: a warp per row waits for its pivot rows). A wait that gives up makes
+                           the solve return VFV_TIMEOUT and leaves the context usable. */
     int32_t ilu_sweeps; /* ILU(0) only: 0 = exact triangular solves (level-scheduled sweeps); k in [1, 16] = k Jacobi
                            sweeps of each factor instead (u = y - N u and w = D^-1 (u - S w), k times each, for
                            L = I + N, U = D + S; Anzt, Chow & Dongarra 2015): a fixed linear preconditioner whose

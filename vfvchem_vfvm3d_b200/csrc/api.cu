@@ -364,17 +364,79 @@ inline void launch_attrs(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, boo
 }
 
 // numeric ILU(0) of the pattern's current values (double), cast to float when asked
-int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32) {
+// The factorisation as one dataflow launch (k_ilu0_factor_flow) when the ordering has many levels,
+// all narrow (the natural order); level by level otherwise, or with VFV_ILU_FACTOR=levels.
+constexpr int32_t kFacWideRows = 32768;  // levels this wide run one thread per row
+constexpr int kFlowMinLevels = 32;
+constexpr long long kDefaultWaitPolls = 20000000LL;  // polls before a bounded device wait gives up (2 s also ends it)
+
+bool ilu_use_flow(const IluStruct& S) {
+    if (S.nlev < kFlowMinLevels) return false;
+    if (const char* e = getenv("VFV_ILU_FACTOR"))
+        if (std::string(e) == "levels") return false;
+    for (int l = 0; l < S.nlev; ++l)
+        if (S.lev_ptr[l + 1] - S.lev_ptr[l] >= kFacWideRows) return false;
+    return true;
+}
+
+// k_ilu0_factor_flow over S.lu64 (values already gathered); VFV_TIMEOUT if a bounded wait gave up
+// (polls: its poll limit, 0 = default)
+int ilu_factor_flow(vfv_ctx* ctx, IluStruct& S, int32_t n, long long polls) {
+    cudaStream_t s = ctx->stream;
+    if (!S.flow_grid) {
+        int per_sm = 0, sms = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ilu0_factor_flow, 32 * kFacWarps, 0));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        if (per_sm < 1) return set_err(ctx, VFV_CUDA_ERROR, "ILU(0): the dataflow factorisation does not fit an SM");
+        CK(S.ready.alloc(std::max<int64_t>(n, 1)));
+        CK(cudaMemsetAsync(S.ready.p, 0, S.ready.n * sizeof(unsigned), s));
+        CK(S.flow_state.alloc(2));
+        CK(cudaMemsetAsync(S.flow_state.p, 0, 2 * sizeof(unsigned), s));
+        S.flow_grid = (int)std::min<int64_t>((int64_t)per_sm * sms, std::max<int64_t>(1, ((int64_t)n + kFacWarps - 1) / kFacWarps));
+        S.epoch = 0;
+    }
+    if (++S.epoch == 0) {  // the flags wrapped around: no row may look finished
+        CK(cudaMemsetAsync(S.ready.p, 0, S.ready.n * sizeof(unsigned), s));
+        S.epoch = 1;
+    }
+    FlowSync fs{S.ready.p, S.epoch, S.flow_state.p, reinterpret_cast<int*>(S.flow_state.p + 1),
+                polls > 0 ? polls : kDefaultWaitPolls};
+    const int32_t* rp = S.rp.p;
+    const int32_t* ci = S.ci.p;
+    const int32_t* dg = S.dg.p;
+    double* a = S.lu64.p;
+    int* bad = S.bad.p;
+    void* args[] = {(void*)&n, (void*)&rp, (void*)&ci, (void*)&dg, (void*)&a, (void*)&bad, (void*)&fs};
+    CK(cudaLaunchCooperativeKernel((const void*)k_ilu0_factor_flow, dim3(S.flow_grid), dim3(32 * kFacWarps), args, 0, s));
+    unsigned st[2] = {0u, 0u};
+    CK(cudaMemcpyAsync(st, S.flow_state.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (st[0] || st[1]) {
+        CK(cudaMemsetAsync(S.flow_state.p, 0, 2 * sizeof(unsigned), s));
+        CK(cudaStreamSynchronize(s));
+        return set_err(ctx, VFV_TIMEOUT, "ILU(0): a bounded device wait of the dataflow factorisation gave up");
+    }
+    return VFV_OK;
+}
+
+// The numeric factor (and its float copy with want32) for the pattern's current values. polls: poll
+// limit of the dataflow factorisation's waits (0 = default); without may_alloc the dataflow
+// factorisation runs only if its buffers already exist (level by level otherwise).
+int ilu_refresh(vfv_ctx* ctx, vfv_pattern* p, IluStruct& S, bool want32, long long polls = 0, bool may_alloc = true) {
     cudaStream_t s = ctx->stream;
     if (S.version64 != p->version) {
         k_gather_vals<double><<<grid_for(p->nnz), 256, 0, s>>>(p->nnz, S.src.p, p->val.p, S.lu64.p);
-        ctx->launches += 1 + S.nlev;
         CK(cudaMemsetAsync(S.bad.p, 0, sizeof(int), s));
+        const bool flow = ilu_use_flow(S) && (may_alloc || S.flow_grid > 0);
+        ctx->launches += 1 + (flow ? 1 : S.nlev);
+        if (flow) {
+            const int rc = ilu_factor_flow(ctx, S, (int32_t)p->n, polls);
+            if (rc != VFV_OK) return rc;
+        }
         // narrow levels: one warp per row, chained with programmatic dependent launch; wide levels
         // (>= kFacWideRows rows, e.g. multicolour colours): one thread per row, in stream order
-        constexpr int32_t kFacWideRows = 32768;
         bool prev_warp = false;
-        for (int l = 0; l < S.nlev; ++l) {
+        for (int l = 0; l < (flow ? 0 : S.nlev); ++l) {
             const int32_t r0 = S.lev_ptr[l], r1 = S.lev_ptr[l + 1];
             if (r1 - r0 >= kFacWideRows) {
                 k_ilu0_factor_level<<<grid_for(r1 - r0, 128), 128, 0, s>>>(r0, r1, S.rp.p, S.ci.p, S.dg.p, S.lu64.p, S.bad.p);
@@ -664,7 +726,6 @@ void ilu_apply_sweeps(cudaStream_t s, const SweepOps<T>& o, int sweeps, int uswe
 }
 
 constexpr int kMaxIluSweeps = 16;
-constexpr long long kDefaultWaitPolls = 20000000LL;  // polls before a bounded device wait gives up (2 s also ends it)
 
 template <typename T>
 constexpr int chain_slot() {
@@ -1367,7 +1428,7 @@ struct Gmres : SolverBase {
             ctx->launches += 1;
         }
         if (precond == VFV_PRECOND_ILU0) {
-            int rc = ilu_refresh(ctx, p, *ilu, mixed);
+            int rc = ilu_refresh(ctx, p, *ilu, mixed, wait_polls);
             if (!rc && sweeps > 0) rc = ilu_split_refresh<T>(ctx, p, *ilu, sweep_half);
             if (rc) return rc;
             if (sweeps > 0) sw_ops = sweep_ops<T>(p, *ilu, sweep_half);
@@ -2079,7 +2140,7 @@ int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, c
         if (e != cudaSuccess) return set_err(ctx, VFV_CUDA_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         g_ilu_scratch_ptr[ctx->device].store(scratch, std::memory_order_release);
     }
-    int rc = ilu_refresh(ctx, p, S, false);  // numeric factor into the storage made at set-up
+    int rc = ilu_refresh(ctx, p, S, false, 0, false);  // numeric factor into the storage made at set-up
     if (rc) return rc;
     ilu_apply_levels<double>(ctx->stream, S, S.lu64.p, r, scratch, z, nullptr);
     ctx->launches += 2 * S.nlev;

@@ -102,6 +102,13 @@ struct IluStruct {
     DBuf<int> bad;
     uint64_t version64 = ~0ull, version32 = ~0ull;
 
+    // dataflow factorisation (k_ilu0_factor_flow): per-row ready flags holding the epoch of the
+    // factorisation that finished the row, the abort word and timeout flag of its bounded waits, and
+    // the cooperative grid (0: not set up)
+    DBuf<unsigned> ready, flow_state;
+    unsigned epoch = 0;
+    int flow_grid = 0;
+
     // single-launch sweeps (k_ilu0_chain): row tasks inside levels (row starts, levels, tasks per
     // level), and per precision a work vector for standalone applies and the claim and completion
     // counters

@@ -58,104 +58,248 @@ __global__ void k_ilu0_factor_level(int32_t r0, int32_t r1, const int32_t* __res
 }
 
 // The same level, one warp per row, for narrow levels (the natural ordering's ~1,500-row levels).
-// Every pivot row k of row i belongs to an earlier level and is final, so the warp first stages, for
-// each of row i's lower entries, the pivot u_kk and row k's upper part (columns and values) in
-// shared memory - one round of independent loads instead of a chain of dependent ones per merge
-// step (a thread per row walking the merges was 5x slower on the 692 natural levels of the 10^6-row
-// heat matrix). Lane l then holds entry l of row i, and the eliminations run in the serial IKJ
-// order: for each lower entry t in turn, l_it = a_it / u_kk, and every later entry whose column
-// occurs in row k's upper part subtracts l_it times that entry (the merge of the serial loop, as a
-// column match across the lanes). Rows longer than a warp, or with more lower entries or longer
-// pivot rows than the staging holds, run the serial loop on lane 0.
-// Levels are chained with programmatic dependent launch: before waiting for the previous level a
-// warp loads everything that level cannot change (the row's own values, written before the first
-// level, and the structure of its pivot rows); only the pivot rows' values are loaded after the wait.
+// Lane l holds entry l of row i. Every pivot row k of row i belongs to an earlier level and is
+// final. Before waiting for the previous level, the warp stages the structure of row i's pivot rows
+// (upper columns in shared memory) and each lane finds, per pivot row, the entry in its own column
+// (the merge of the serial loop, as a column match across the lanes); these cannot change. After
+// the wait, one round of independent loads brings the pivots and the matched values, and the
+// eliminations run in the serial IKJ order: for each lower entry t in turn, l_it = a_it / u_kk, and
+// the later entry matching row k's upper part subtracts l_it times it (a thread per row walking the
+// merges was 5x slower on the 692 natural levels of the 10^6-row heat matrix). Rows longer than a
+// warp, or with more lower entries or longer pivot rows than the staging holds, run the serial loop
+// on lane 0. Levels are chained with programmatic dependent launch.
 constexpr int kFacWarps = 8;  // rows per block
 constexpr int kFacLow = 16;   // lower entries of a row staged
 constexpr int kFacUp = 24;    // upper entries of each pivot row staged
 
-__global__ void __launch_bounds__(32 * kFacWarps) k_ilu0_factor_level_warp(int32_t r0, int32_t r1, const int32_t* __restrict__ rp,
-                                                                            const int32_t* __restrict__ ci, const int32_t* __restrict__ dg,
-                                                                            double* __restrict__ a, int* __restrict__ bad) {
-    __shared__ int32_t s_col[kFacWarps][kFacLow][kFacUp];
-    __shared__ double s_val[kFacWarps][kFacLow][kFacUp];
-    __shared__ int32_t s_dk[kFacWarps][kFacLow], s_len[kFacWarps][kFacLow];
-    __shared__ double s_piv[kFacWarps][kFacLow];
+struct FacStage {  // one warp's staging: the pivot rows' indices, diagonal slots, upper lengths and columns
+    int32_t col[kFacLow][kFacUp];
+    int32_t dk[kFacLow], len[kFacLow], k[kFacLow];
+};
+
+__device__ __forceinline__ unsigned ld_relaxed_gpu_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu_u32(unsigned* p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ unsigned long long flow_clock_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Row readiness of the dataflow factorisation (k_ilu0_factor_flow): ready[k] == epoch once row k is
+// final. Waits poll with relaxed loads (one fence after the last one, by the caller); a wait gives up
+// after poll_limit polls or 2 s, raising *abort (which every waiting warp checks) and *timeout_flag.
+struct FlowSync {
+    unsigned* ready;
+    unsigned epoch;
+    unsigned* abort;
+    int* timeout_flag;
+    long long poll_limit;
+    // warp-wide: lane l waits for row k_l when has_l (every lane calls it); each lane that waited
+    // fences once after its last poll. False (on every lane) when the waits gave up.
+    __device__ bool wait_warp(bool has, int32_t k) const {
+        const unsigned full = 0xffffffffu;
+        bool rdy = !has || ld_relaxed_gpu_u32(ready + k) == epoch;
+        if (!__all_sync(full, rdy)) {
+            const unsigned long long t0 = flow_clock_ns();
+            for (long long it = 1;; ++it) {
+                if (it > 8) __nanosleep(64);
+                if (!rdy) rdy = ld_relaxed_gpu_u32(ready + k) == epoch;
+                if (__all_sync(full, rdy)) break;
+                int give_up = 0;
+                if ((threadIdx.x & 31) == 0) {
+                    if ((it & 15) == 0 && *(volatile unsigned*)abort) give_up = 1;
+                    else if (it >= poll_limit || ((it & 255) == 0 && flow_clock_ns() - t0 > 2000000000ull)) {
+                        atomicExch(abort, 1u);
+                        *(volatile int*)timeout_flag = 1;
+                        give_up = 1;
+                    }
+                }
+                if (__shfl_sync(full, give_up, 0)) return false;
+            }
+        }
+        if (has) fence_acq_rel_gpu();
+        __syncwarp(full);
+        return true;
+    }
+    __device__ bool wait(int32_t k) const {
+        if (ld_relaxed_gpu_u32(ready + k) == epoch) return true;
+        const unsigned long long t0 = flow_clock_ns();
+        for (long long it = 1;; ++it) {
+            if (it > 8) __nanosleep(64);
+            if (ld_relaxed_gpu_u32(ready + k) == epoch) return true;
+            if ((it & 15) == 0 && *(volatile unsigned*)abort) return false;
+            if (it >= poll_limit || ((it & 255) == 0 && flow_clock_ns() - t0 > 2000000000ull)) {
+                atomicExch(abort, 1u);
+                *(volatile int*)timeout_flag = 1;
+                return false;
+            }
+        }
+    }
+};
+
+// Factors row i (one warp). FLOW: lane t waits for pivot row t through fs (values then read from
+// L2, past the SM's L1), and the row is published in ready[] when done; otherwise the previous level
+// has finished (programmatic dependent launch). False when a wait gave up.
+template <bool FLOW>
+__device__ __forceinline__ bool factor_row_warp(int32_t i, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                const int32_t* __restrict__ dg, double* a, int* __restrict__ bad, FacStage& sg,
+                                                const FlowSync& fs) {
     const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int32_t i = r0 + (int32_t)blockIdx.x * kFacWarps + w;
-    if (i >= r1) return;  // whole warps leave together
+    const int lane = threadIdx.x & 31;
+    auto piv_ld = [](const double* p) { return FLOW ? __ldcg(p) : *p; };
     const int32_t b = rp[i], e = rp[i + 1], d = dg[i];
     const int32_t len = e - b, nl = d - b;
     bool ok = len <= 32 && nl <= kFacLow;
     if (ok && lane < nl) {
         const int32_t k = ci[b + lane];
         const int32_t dk = dg[k], ul = rp[k + 1] - dk - 1;
-        s_dk[w][lane] = dk;
-        s_len[w][lane] = ul;
+        sg.k[lane] = k;
+        sg.dk[lane] = dk;
+        sg.len[lane] = ul;
         if (ul > kFacUp) ok = false;
     }
     ok = __all_sync(full, ok);
-    if (ok) {  // pivot rows' columns (structure only)
+    const int32_t c = ok && lane < len ? ci[b + lane] : -1;
+    double v = ok && lane < len ? a[b + lane] : 0.0;
+    // slot[t]: the slot of pivot row t's entry in this lane's column (-1: none). Structure only, so
+    // it is found before the wait; the eliminations after it are then one division and at most one
+    // multiply-subtract per pivot.
+    int32_t slot[kFacLow];
+#pragma unroll
+    for (int t = 0; t < kFacLow; ++t) slot[t] = -1;
+    if (ok) {
         __syncwarp(full);
         for (int idx = lane; idx < nl * kFacUp; idx += 32) {
             const int t = idx / kFacUp, u = idx - t * kFacUp;
-            if (u < s_len[w][t]) s_col[w][t][u] = ci[s_dk[w][t] + 1 + u];
+            if (u < sg.len[t]) sg.col[t][u] = ci[sg.dk[t] + 1 + u];
+        }
+        __syncwarp(full);
+#pragma unroll
+        for (int t = 0; t < kFacLow; ++t) {
+            if (t < nl && lane > t && lane < len) {
+                const int ul = sg.len[t];
+                for (int u = 0; u < ul; ++u)
+                    if (sg.col[t][u] == c) {
+                        slot[t] = sg.dk[t] + 1 + u;
+                        break;
+                    }
+            }
         }
     }
-    const int32_t c = ok && lane < len ? ci[b + lane] : -1;
-    double v = ok && lane < len ? a[b + lane] : 0.0;
-    pdl_launch_dependents();
-    pdl_wait();
-    if (!ok) {  // the serial IKJ loop
-        if (lane != 0) return;
-        for (int32_t kk = b; kk < d; ++kk) {
-            const int32_t k = ci[kk];
-            const double ukk = a[dg[k]];
-            if (ukk == 0.0) {
-                *bad = 1;
-                return;
+    if constexpr (FLOW) {
+        // lane t waits for pivot row t; all pivot loads come after every waiting lane's fence
+        const bool has = ok && lane < nl;
+        if (!fs.wait_warp(has, has ? sg.k[lane] : 0)) return false;
+    } else {
+        pdl_launch_dependents();
+        pdl_wait();
+    }
+    if (!ok) {  // the serial IKJ loop on lane 0
+        int go = 1;
+        if (lane == 0) {
+            for (int32_t kk = b; kk < d; ++kk) {
+                const int32_t k = ci[kk];
+                if (FLOW) {
+                    if (!fs.wait(k)) {
+                        go = 0;
+                        break;
+                    }
+                    fence_acq_rel_gpu();
+                }
+                const double ukk = piv_ld(a + dg[k]);
+                if (ukk == 0.0) {
+                    *bad = 1;
+                    break;
+                }
+                const double lik = a[kk] / ukk;
+                a[kk] = lik;
+                int32_t p = kk + 1, q = dg[k] + 1;
+                const int32_t e_k = rp[k + 1];
+                while (p < e && q < e_k) {
+                    const int32_t cp = ci[p], cq = ci[q];
+                    if (cp == cq) {
+                        a[p] -= lik * piv_ld(a + q);
+                        ++p;
+                        ++q;
+                    } else if (cp < cq) {
+                        ++p;
+                    } else {
+                        ++q;
+                    }
+                }
             }
-            const double lik = a[kk] / ukk;
-            a[kk] = lik;
-            int32_t p = kk + 1, q = dg[k] + 1;
-            const int32_t e_k = rp[k + 1];
-            while (p < e && q < e_k) {
-                const int32_t cp = ci[p], cq = ci[q];
-                if (cp == cq) {
-                    a[p] -= lik * a[q];
-                    ++p;
-                    ++q;
-                } else if (cp < cq) {
-                    ++p;
-                } else {
-                    ++q;
+            if (go && a[d] == 0.0) *bad = 1;
+        }
+        if (!__shfl_sync(full, go, 0)) return false;
+    } else {
+        // lane t holds pivot u_kk of pivot row t; every lane its matched pivot-row values (one round
+        // of independent loads), then the serial IKJ order: l_it = a_it / u_kk, and the later entry
+        // matching row k's upper part subtracts l_it times it
+        const double ukk = lane < nl ? piv_ld(a + sg.dk[lane]) : 1.0;
+        double mv[kFacLow];
+#pragma unroll
+        for (int t = 0; t < kFacLow; ++t) mv[t] = slot[t] >= 0 ? piv_ld(a + slot[t]) : 0.0;
+        const bool zero = __any_sync(full, lane < nl && ukk == 0.0);
+        if (!zero) {
+#pragma unroll
+            for (int t = 0; t < kFacLow; ++t) {
+                if (t < nl) {
+                    const double lik = __shfl_sync(full, v, t) / __shfl_sync(full, ukk, t);
+                    if (lane == t) v = lik;
+                    if (slot[t] >= 0) v -= lik * mv[t];
                 }
             }
         }
-        if (a[d] == 0.0) *bad = 1;
-        return;
-    }
-    if (lane < nl) s_piv[w][lane] = a[s_dk[w][lane]];
-    for (int idx = lane; idx < nl * kFacUp; idx += 32) {
-        const int t = idx / kFacUp, u = idx - t * kFacUp;
-        if (u < s_len[w][t]) s_val[w][t][u] = a[s_dk[w][t] + 1 + u];
-    }
-    __syncwarp(full);
-    for (int t = 0; t < nl; ++t) {
-        const double ukk = s_piv[w][t];
-        if (ukk == 0.0) {
+        if (zero) {
             if (lane == 0) *bad = 1;
-            return;
+        } else {
+            if (lane < len) a[b + lane] = v;
+            if (lane == nl && v == 0.0) *bad = 1;
         }
-        const double lik = __shfl_sync(full, v, t) / ukk;
-        if (lane == t) v = lik;
-        const int ul = s_len[w][t];
-        for (int u = 0; u < ul; ++u)
-            if (lane > t && c == s_col[w][t][u]) v -= lik * s_val[w][t][u];
     }
-    if (lane < len) a[b + lane] = v;
-    if (lane == nl && v == 0.0) *bad = 1;
+    if constexpr (FLOW) {  // publish: the warp's stores, one fence, then the row's flag
+        __syncwarp(full);
+        if (lane == 0) {
+            fence_acq_rel_gpu();
+            st_relaxed_gpu_u32(fs.ready + i, fs.epoch);
+        }
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(32 * kFacWarps) k_ilu0_factor_level_warp(int32_t r0, int32_t r1, const int32_t* __restrict__ rp,
+                                                                            const int32_t* __restrict__ ci, const int32_t* __restrict__ dg,
+                                                                            double* __restrict__ a, int* __restrict__ bad) {
+    __shared__ FacStage s_stage[kFacWarps];
+    const int w = threadIdx.x >> 5;
+    const int32_t i = r0 + (int32_t)blockIdx.x * kFacWarps + w;
+    if (i >= r1) return;  // whole warps leave together
+    factor_row_warp<false>(i, rp, ci, dg, a, bad, s_stage[w], FlowSync{});
+}
+
+// The whole factorisation in one launch, for orderings with many narrow levels (the natural order:
+// 692 levels on the 10^6-row heat matrix, ~12 us each as separate launches). Rows are in the
+// permuted numbering, where every pivot row of row i has a smaller index. Warp g of the W warps of
+// the grid factors rows g, g + W, g + 2W, ... in increasing order and, instead of waiting for a whole
+// level, waits only for its row's pivot rows (ready[k] == epoch). Progress needs every warp
+// resident (the smallest unfinished row always has all its pivots finished, and its warp has
+// finished all its earlier rows), hence a cooperative launch. Each row's arithmetic is
+// factor_row_warp's, so the factor is bit-identical to the level-by-level one.
+__global__ void __launch_bounds__(32 * kFacWarps) k_ilu0_factor_flow(int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                                     const int32_t* __restrict__ dg, double* a, int* __restrict__ bad,
+                                                                     FlowSync fs) {
+    __shared__ FacStage s_stage[kFacWarps];
+    const int w = threadIdx.x >> 5;
+    const int32_t nw = (int32_t)gridDim.x * kFacWarps;
+    for (int32_t i = (int32_t)blockIdx.x * kFacWarps + w; i < n; i += nw)
+        if (!factor_row_warp<true>(i, rp, ci, dg, a, bad, s_stage[w], fs)) return;
 }
 
 // Gather A's values into the permuted factor storage: lu[k] = (T) val[src[k]].
