@@ -37,6 +37,7 @@ extern "C" {
 #define VFV_BAD_INPUT 3     /* invalid argument (sizes, indices, options) */
 #define VFV_CUDA_ERROR 4    /* CUDA runtime failure or no device */
 #define VFV_TIMEOUT 5       /* a bounded device wait gave up (see vfv_gmres_opts::wait_limit) */
+#define VFV_IO_ERROR 6      /* an output file could not be written (the reference's WriteVtu / WriteCsv, error.rs:116-127) */
 
 /* ---- preconditioners / precisions / orderings */
 #define VFV_PRECOND_NONE 0
@@ -198,6 +199,22 @@ int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out);
  * other input is refused with VFV_BAD_INPUT rather than rounded. */
 int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out);
 void vfv_mesh_destroy(vfv_mesh* m);
+
+/* ---- output (host): the reference's VTU and CSV files, byte for byte (numbers as Rust's {:.9}).
+ * path is the whole file name (the reference forms "<name>_<ts:04>.<type>", scl_dom.rs:60-62 and
+ * write_vtu.rs:7). VFV_IO_ERROR when the file cannot be written, VFV_BAD_INPUT for bad arguments. */
+/* A field over the mesh's vertices (points, then nodes) with its tetrahedra: write_scldom_vtu
+ * (ncomp 1) and write_vecdom_vtu (ncomp 3), src/base/write_vtu.rs:5,192. values: [n_tot][ncomp]. */
+int vfv_mesh_write_vtu(const vfv_mesh* m, const double* values, int ncomp, const char* path);
+/* The same field as CSV lines: write_scldom_csv / write_vecdom_csv, src/base/write_csv.rs:5,68. */
+int vfv_mesh_write_csv(const vfv_mesh* m, const double* values, int ncomp, const char* path);
+/* A field on n vertices at pos[n][3] (a boundary's or interface's nodes), one vertex cell each:
+ * write_sclbnd_vtu / write_vecbnd_vtu / write_vecitf_vtu (write_vtu.rs:71,259,322); values NULL writes
+ * the empty value array of write_sclitf_vtu (write_vtu.rs:133). */
+int vfv_points_write_vtu(int64_t n, const double* pos, const double* values, int ncomp, const char* path);
+/* The same as CSV lines: write_sclbnd_csv, write_sclitf_csv, write_vecbnd_csv, write_vecitf_csv
+ * (write_csv.rs:30,49,93,112). */
+int vfv_points_write_csv(int64_t n, const double* pos, const double* values, int ncomp, const char* path);
 /* Recomputes the mesh's Voronoi dual from its tetrahedra on the device of ctx (Tetrahedron::update_tet,
  * src/base/geom_tet.rs:122-293: face pieces, sorted-edge sums, control volumes, boundary sub-faces,
  * least-squares weights); the result equals the host dual bit for bit and replaces it. */

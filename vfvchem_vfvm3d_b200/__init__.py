@@ -22,6 +22,8 @@ from .errors import (  # noqa: F401
     LinearGmresBadInput,
     LinearGmresCudaError,
     DeviceWaitTimeout,
+    OutputWriteError,
+    OutputTypeError,
     LinearGmresNonPositiveTolerance,
     LinearGmresNonPositiveRestart,
     LinearGmresNonPositiveMaxOuter,
@@ -34,8 +36,10 @@ from .linear import LinearGmres, Triplet, SparseMatrix  # noqa: F401
 from .transport import TransientTransportGpu  # noqa: F401
 from .flow import SteadyFlowGpu  # noqa: F401
 from . import _lib  # noqa: F401
+from . import output  # noqa: F401
 
 __all__ = [
     "Context", "Pattern", "GmresOptions", "SolveInfo", "Mesh", "SteadyHeatGpu", "LinearGmres", "Triplet",
     "SparseMatrix", "VFVChemError", "LinearGmresDidNotConverge", "default_context", "TransientTransportGpu", "SteadyFlowGpu",
+    "OutputWriteError", "OutputTypeError", "output",
 ]

@@ -97,6 +97,10 @@ SIGNATURES = [
     ("vfv_mesh_jitter_cubes", C.c_int, [C.c_int, _I32P, _U64P, C.c_double, C.POINTER(C.c_void_p)]),
     ("vfv_mesh_info", C.c_int, [_P, _I64P, _I64P, _I64P, _I64P, _I64P]),
     ("vfv_mesh_export", C.c_int, [_P, _DP, _I32P, _I32P]),
+    ("vfv_mesh_write_vtu", C.c_int, [_P, _DP, C.c_int, C.c_char_p]),
+    ("vfv_mesh_write_csv", C.c_int, [_P, _DP, C.c_int, C.c_char_p]),
+    ("vfv_points_write_vtu", C.c_int, [C.c_int64, _DP, _DP, C.c_int, C.c_char_p]),
+    ("vfv_points_write_csv", C.c_int, [C.c_int64, _DP, _DP, C.c_int, C.c_char_p]),
     ("vfv_mesh_export_dual", C.c_int, [_P, _I64P, _I32P, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _I64P, _I32P, _I32P, _DP, _DP, _DP]),
     ("vfv_heat_create", C.c_int, [_P, _P, C.c_int32, _I32P, _PP]),
     ("vfv_heat_destroy", None, [_P]),

@@ -1,5 +1,6 @@
 // Mesh handles of libvfvgpu: seeded jittered cubes, meshes from given vertices, and the export of
 // the Delaunay tetrahedra and the Voronoi dual (host code: csrc/host/mesh.cpp).
+#include "host/write_out.hpp"
 #include "internal.cuh"
 
 #include <algorithm>
@@ -201,6 +202,38 @@ int vfv_mesh_export_dual(const vfv_mesh* m, int64_t* nbr_ptr, int32_t* nbr_idx, 
     cp(bnd_norm, d.bnd_norm);
     cp(bnd_wgt, d.bnd_wgt);
     return VFV_OK;
+}
+
+// output files (host): argument checks here, the formats in host/write_out.cpp
+static int write_rc(const std::string& e, bool io) {
+    if (e.empty()) return VFV_OK;
+    return set_err(nullptr, io ? VFV_IO_ERROR : VFV_BAD_INPUT, e);
+}
+
+int vfv_mesh_write_vtu(const vfv_mesh* m, const double* values, int ncomp, const char* path) {
+    if (!m || !path || (ncomp != 1 && ncomp != 3)) return set_err(nullptr, VFV_BAD_INPUT, "invalid argument");
+    const Mesh& g = m->m;
+    const std::string e = write_vtu_tets(path, g.n_tot(), g.pos.data(), g.n_tet(), g.tets.data(), values, ncomp);
+    return write_rc(e, e.rfind("cannot write", 0) == 0);
+}
+
+int vfv_mesh_write_csv(const vfv_mesh* m, const double* values, int ncomp, const char* path) {
+    if (!m || !path || !values || (ncomp != 1 && ncomp != 3)) return set_err(nullptr, VFV_BAD_INPUT, "invalid argument");
+    const Mesh& g = m->m;
+    const std::string e = write_csv(path, g.n_tot(), g.pos.data(), values, ncomp);
+    return write_rc(e, e.rfind("cannot write", 0) == 0);
+}
+
+int vfv_points_write_vtu(int64_t n, const double* pos, const double* values, int ncomp, const char* path) {
+    if (!path || n < 0 || (n > 0 && !pos) || (ncomp != 1 && ncomp != 3)) return set_err(nullptr, VFV_BAD_INPUT, "invalid argument");
+    const std::string e = write_vtu_points(path, n, pos, values, ncomp);
+    return write_rc(e, e.rfind("cannot write", 0) == 0);
+}
+
+int vfv_points_write_csv(int64_t n, const double* pos, const double* values, int ncomp, const char* path) {
+    if (!path || n < 0 || (n > 0 && (!pos || !values)) || (ncomp != 1 && ncomp != 3)) return set_err(nullptr, VFV_BAD_INPUT, "invalid argument");
+    const std::string e = write_csv(path, n, pos, values, ncomp);
+    return write_rc(e, e.rfind("cannot write", 0) == 0);
 }
 
 }  // extern "C"

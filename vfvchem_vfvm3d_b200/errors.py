@@ -35,6 +35,18 @@ class DeviceWaitTimeout(VFVChemError):
     code = 5
 
 
+class OutputWriteError(VFVChemError, OSError):
+    """``WriteVtu`` / ``WriteCsv { file_path, source }`` (error.rs:116-127): the file could not be
+    written (status 6)."""
+
+    code = 6
+
+
+class OutputTypeError(VFVChemError, ValueError):
+    """``ScalarUnknownOutputType`` / ``ScalarUnsupportedOutputType`` and their Vector twins
+    (error.rs:78-100): an output path without an extension, or one other than csv or vtu."""
+
+
 class LinearGmresNonPositiveThreads(LinearGmresBadInput):
     """``LinearGmresNonPositiveThreads { num_thread }`` (linear_gmres.rs:26-28)."""
 
@@ -52,7 +64,7 @@ class LinearGmresNonPositiveMaxOuter(LinearGmresBadInput):
 
 
 _BY_CODE = {1: LinearGmresDidNotConverge, 2: LinearGmresNonFinite, 3: LinearGmresBadInput, 4: LinearGmresCudaError,
-            5: DeviceWaitTimeout}
+            5: DeviceWaitTimeout, 6: OutputWriteError}
 
 
 def raise_for(code: int, message: str) -> None:
