@@ -193,10 +193,11 @@ int vfv_ilu0_ordering(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, int32_t* perm
 
 /* ---- mesh (host, once per mesh): jittered unit cube, Delaunay, Voronoi dual */
 int vfv_mesh_jitter_cube(int n, uint64_t seed, double jitter, vfv_mesh** out);
-/* a mesh from given vertices (points first, then nodes with a boundary id each). The Delaunay
- * predicates are exact integer arithmetic on the 2^-18 lattice: every coordinate must be a finite
- * multiple of 2^-18 and the bounding box at most 1.75 on each axis (scale the domain into it);
- * other input is refused with VFV_BAD_INPUT rather than rounded. */
+/* a mesh from given vertices (points first, then nodes with a boundary id each; the vertices' hull
+ * must be their bounding box). The Delaunay predicates give exact signs for any finite coordinates
+ * (the reference's robust orient3d / insphere, delaunay.rs:1,10): integer arithmetic for vertices
+ * on the 2^-18 lattice within a box of 1.75, else filtered double arithmetic with an exact
+ * big-integer fallback. Coordinates must be finite and at most 1e50 in magnitude (VFV_BAD_INPUT). */
 int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, const int32_t* node_bnd, vfv_mesh** out);
 void vfv_mesh_destroy(vfv_mesh* m);
 

@@ -67,12 +67,13 @@ def test_mesh_rejects_bad_input(lib_built):
     vpos, vbnd, _ = ref.export()
     m = Mesh.from_vertices(vpos, ref.n_pts, vbnd)  # on the 2^-18 lattice, inside the exact range
     assert m.n_tet == ref.n_tet
-    off = vpos.copy()
-    off[0, 0] += 2.0 ** -20  # an interior point between lattice points: refused, not rounded
-    with pytest.raises(VFVChemError, match="multiples of 2"):
-        Mesh.from_vertices(off, ref.n_pts, vbnd)
-    with pytest.raises(VFVChemError, match="bounding box"):  # the exact integer predicates would overflow
-        Mesh.from_vertices(vpos * 2.0, ref.n_pts, vbnd)
+    bad = vpos.copy()
+    bad[3, 1] = np.nan
+    with pytest.raises(VFVChemError, match="finite"):
+        Mesh.from_vertices(bad, ref.n_pts, vbnd)
+    bad[3, 1] = 1e60
+    with pytest.raises(VFVChemError, match="finite"):
+        Mesh.from_vertices(bad, ref.n_pts, vbnd)
 
 
 def test_linear_gmres_constructor_checks():

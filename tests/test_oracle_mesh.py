@@ -84,3 +84,92 @@ def test_dual_agrees_with_product_and_numpy_restatement(lib_built, n):
     for c in range(3):
         np.add.at(an[c], v, d["area"] * d["norm"][c])
     assert np.max(np.abs(an[:, :npts])) < 1e-12
+
+
+def _box_jitter(n, seed, scale=1.0, shift=0.0):
+    """A jittered n^3 grid in raw doubles (no lattice), faces jittered in plane, corners fixed, then
+    scaled and shifted: the hull is the box, the vertices are in general position."""
+    rng = np.random.default_rng(seed)
+    g = np.linspace(0.0, 1.0, n)
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    p = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    h = 1.0 / (n - 1)
+    inner = (p > 0) & (p < 1)
+    p = p + inner * rng.uniform(-0.3, 0.3, p.shape) * h
+    return p * scale + shift
+
+
+def _points_and_nodes(pos):
+    """Interior vertices first, then the hull's with one boundary id each (x faces over y over z),
+    the vertex order and boundary rule of the generated cubes; returns (pos, n_pts, node_bnd)."""
+    lo, hi = pos.min(0), pos.max(0)
+    bid = np.full(len(pos), -1)
+    for c in (2, 1, 0):  # x faces win: assigned last
+        bid[pos[:, c] == lo[c]] = 2 * c
+        bid[pos[:, c] == hi[c]] = 2 * c + 1
+    inner = bid < 0
+    return np.concatenate([pos[inner], pos[~inner]]), int(inner.sum()), bid[~inner].astype(np.int32)
+
+
+def _exact_checks(pos, tets):
+    """Exact rational checks of a tetrahedralisation: positive orientation, volumes summing to the
+    box, and no vertex strictly inside any circumsphere."""
+    from fractions import Fraction as F
+    P = [[F(float(c)) for c in q] for q in pos]
+
+    def sub(a, b):
+        return [a[0] - b[0], a[1] - b[1], a[2] - b[2]]
+
+    def det3(a, b, c):
+        return a[0] * (b[1] * c[2] - b[2] * c[1]) - a[1] * (b[0] * c[2] - b[2] * c[0]) + a[2] * (b[0] * c[1] - b[1] * c[0])
+
+    vol = F(0)
+    for t in tets:
+        a, b, c, d = (P[i] for i in t)
+        o = det3(sub(a, d), sub(b, d), sub(c, d))
+        assert o > 0
+        vol += o / 6
+        for j, e in enumerate(P):
+            if j in t:
+                continue
+            q = [sub(a, e), sub(b, e), sub(c, e), sub(d, e)]
+            lf = [v[0] * v[0] + v[1] * v[1] + v[2] * v[2] for v in q]
+            r = (lf[1] * det3(q[0], q[2], q[3]) - lf[0] * det3(q[1], q[2], q[3]) + lf[3] * det3(q[0], q[1], q[2])
+                 - lf[2] * det3(q[0], q[1], q[3]))
+            assert r <= 0  # not strictly inside
+    lo = [min(q[i] for q in P) for i in range(3)]
+    hi = [max(q[i] for q in P) for i in range(3)]
+    assert vol == (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2])
+
+
+@pytest.mark.parametrize("scale,shift", [(1.0, 0.0), (3.7, 0.0), (1e-3, 123.456), (250.0, -1e4)])
+def test_delaunay_of_raw_doubles_equals_qhull(lib_built, scale, shift):
+    """Vertices off the 2^-18 lattice and far outside the unit box (a domain in metres, offset):
+    the double predicates with their exact fallback give Qhull's tetrahedra."""
+    from vfvchem_vfvm3d_b200 import Mesh
+    pos, n_pts, bnd = _points_and_nodes(_box_jitter(6, 11, scale, shift))
+    m = Mesh.from_vertices(pos, n_pts, bnd)
+    _, _, tets = m.export()
+    # Qhull rounds in doubles, so it gets the exactly translated copy (each difference of two
+    # coordinates within a factor of two is exact); the Delaunay tetrahedra do not change
+    rel = pos - pos.min(0)
+    assert np.array_equal(rel + pos.min(0), pos)
+    st = np.sort(Delaunay(rel).simplices, axis=1)
+    a, b, c, d = (rel[st[:, i]] for i in range(4))
+    vol = np.abs(np.einsum("ij,ij->i", a - d, np.cross(b - d, c - d)))
+    st = st[vol > 1e-12 * vol.max()]
+    assert _tetset(tets) == _tetset(st)
+    assert m.dual()["nbr_ptr"][-1] == m.n_dir  # the Voronoi dual builds on it
+
+
+def test_delaunay_of_cospherical_doubles_is_exact(lib_built):
+    """A regular grid of spacing 0.1 (off the lattice; every cell's 8 corners cospherical): the exact
+    fallback settles every tie; the result is a valid Delaunay tetrahedralisation, checked in
+    rationals."""
+    from vfvchem_vfvm3d_b200 import Mesh
+    g = np.arange(4) * 0.1
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    pos, n_pts, bnd = _points_and_nodes(np.stack([x.ravel(), y.ravel(), z.ravel()], 1))
+    m = Mesh.from_vertices(pos, n_pts, bnd)
+    _, _, tets = m.export()
+    _exact_checks(pos, tets)

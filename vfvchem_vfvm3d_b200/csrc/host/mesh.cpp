@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <array>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -147,6 +148,226 @@ inline V3 circumsphere3(V3 a, V3 b, V3 c, V3 d) {
     return add3(a, scale3(0.5 / dot3(u, cross3(v, w)), num));
 }
 
+// ---------------------------------------------------------------- exact predicates on doubles
+// For vertices off the 2^-18 lattice. A double is an integer times a power of two, so the
+// coordinates of one predicate call are exact integers at their smallest exponent; the sign of the
+// same determinant as orient_i / insphere_i is then computed on sign-magnitude integers (32-bit
+// limbs, schoolbook products). Scaling by a power of two keeps the sign.
+struct DP { double x, y, z; };
+
+struct BigInt {
+    std::vector<uint32_t> mag;  // little-endian limbs, no leading zero limb
+    int sign = 0;               // -1, 0, 1
+};
+
+int cmp_mag(const std::vector<uint32_t>& a, const std::vector<uint32_t>& b) {
+    if (a.size() != b.size()) return a.size() < b.size() ? -1 : 1;
+    for (size_t i = a.size(); i-- > 0;)
+        if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+    return 0;
+}
+
+void trim(std::vector<uint32_t>& m) {
+    while (!m.empty() && m.back() == 0) m.pop_back();
+}
+
+std::vector<uint32_t> add_mag(const std::vector<uint32_t>& a, const std::vector<uint32_t>& b) {
+    const std::vector<uint32_t>& l = a.size() >= b.size() ? a : b;
+    const std::vector<uint32_t>& r = a.size() >= b.size() ? b : a;
+    std::vector<uint32_t> o(l.size() + 1);
+    uint64_t carry = 0;
+    for (size_t i = 0; i < l.size(); ++i) {
+        const uint64_t t = (uint64_t)l[i] + (i < r.size() ? r[i] : 0u) + carry;
+        o[i] = (uint32_t)t;
+        carry = t >> 32;
+    }
+    o[l.size()] = (uint32_t)carry;
+    trim(o);
+    return o;
+}
+
+std::vector<uint32_t> sub_mag(const std::vector<uint32_t>& a, const std::vector<uint32_t>& b) {  // |a| >= |b|
+    std::vector<uint32_t> o(a.size());
+    int64_t borrow = 0;
+    for (size_t i = 0; i < a.size(); ++i) {
+        int64_t t = (int64_t)a[i] - (i < b.size() ? (int64_t)b[i] : 0) - borrow;
+        borrow = t < 0;
+        if (t < 0) t += (int64_t)1 << 32;
+        o[i] = (uint32_t)t;
+    }
+    trim(o);
+    return o;
+}
+
+BigInt big_add(const BigInt& a, const BigInt& b) {
+    if (a.sign == 0) return b;
+    if (b.sign == 0) return a;
+    BigInt o;
+    if (a.sign == b.sign) {
+        o.mag = add_mag(a.mag, b.mag);
+        o.sign = a.sign;
+        return o;
+    }
+    const int c = cmp_mag(a.mag, b.mag);
+    if (c == 0) return o;
+    o.mag = c > 0 ? sub_mag(a.mag, b.mag) : sub_mag(b.mag, a.mag);
+    o.sign = c > 0 ? a.sign : b.sign;
+    return o;
+}
+
+BigInt big_neg(BigInt a) {
+    a.sign = -a.sign;
+    return a;
+}
+
+BigInt big_sub(const BigInt& a, const BigInt& b) { return big_add(a, big_neg(b)); }
+
+BigInt big_mul(const BigInt& a, const BigInt& b) {
+    BigInt o;
+    if (a.sign == 0 || b.sign == 0) return o;
+    std::vector<uint64_t> acc(a.mag.size() + b.mag.size() + 1, 0);
+    for (size_t i = 0; i < a.mag.size(); ++i) {
+        uint64_t carry = 0;
+        for (size_t j = 0; j < b.mag.size(); ++j) {
+            const uint64_t t = (uint64_t)a.mag[i] * b.mag[j] + (acc[i + j] & 0xffffffffu) + carry;
+            acc[i + j] = t & 0xffffffffu;
+            carry = t >> 32;
+        }
+        size_t k = i + b.mag.size();
+        while (carry) {
+            const uint64_t t = acc[k] + carry;
+            acc[k] = t & 0xffffffffu;
+            carry = t >> 32;
+            ++k;
+        }
+    }
+    o.mag.resize(acc.size());
+    for (size_t i = 0; i < acc.size(); ++i) o.mag[i] = (uint32_t)acc[i];
+    trim(o.mag);
+    o.sign = a.sign * b.sign;
+    return o;
+}
+
+// exponent of the lowest mantissa bit of a nonzero finite double (x = M 2^E, M odd or 53-bit)
+int low_exp(double x) {
+    int e = 0;
+    (void)std::frexp(x, &e);
+    return e - 53;
+}
+
+// x / 2^e0 as an exact integer (x a multiple of 2^e0)
+BigInt big_from(double x, int e0) {
+    BigInt o;
+    if (x == 0.0) return o;
+    int e = 0;
+    const double f = std::frexp(std::fabs(x), &e);
+    const uint64_t m = (uint64_t)std::ldexp(f, 53);  // exact: 53-bit integer
+    const int sh = e - 53 - e0;                       // >= 0
+    o.mag.assign((size_t)(sh / 32) + 3, 0u);
+    const int q = sh / 32, r = sh % 32;
+    const unsigned __int128 v = (unsigned __int128)m << r;
+    o.mag[(size_t)q] = (uint32_t)v;
+    o.mag[(size_t)q + 1] = (uint32_t)(v >> 32);
+    o.mag[(size_t)q + 2] = (uint32_t)(v >> 64);
+    trim(o.mag);
+    o.sign = x < 0 ? -1 : 1;
+    return o;
+}
+
+// the coordinates of k points as integers at their smallest exponent, relative to the last point
+template <int K>
+void big_diffs(const DP* const (&p)[K], BigInt (&d)[K - 1][3]) {
+    int e0 = INT_MAX;
+    for (int i = 0; i < K; ++i)
+        for (double x : {p[i]->x, p[i]->y, p[i]->z})
+            if (x != 0.0) e0 = std::min(e0, low_exp(x));
+    if (e0 == INT_MAX) e0 = 0;
+    const BigInt lx = big_from(p[K - 1]->x, e0), ly = big_from(p[K - 1]->y, e0), lz = big_from(p[K - 1]->z, e0);
+    for (int i = 0; i < K - 1; ++i) {
+        d[i][0] = big_sub(big_from(p[i]->x, e0), lx);
+        d[i][1] = big_sub(big_from(p[i]->y, e0), ly);
+        d[i][2] = big_sub(big_from(p[i]->z, e0), lz);
+    }
+}
+
+BigInt big_det3(const BigInt* a, const BigInt* b, const BigInt* c) {
+    const BigInt t0 = big_sub(big_mul(b[1], c[2]), big_mul(b[2], c[1]));
+    const BigInt t1 = big_sub(big_mul(b[0], c[2]), big_mul(b[2], c[0]));
+    const BigInt t2 = big_sub(big_mul(b[0], c[1]), big_mul(b[1], c[0]));
+    return big_add(big_sub(big_mul(a[0], t0), big_mul(a[1], t1)), big_mul(a[2], t2));
+}
+
+int orient_exact(const DP& a, const DP& b, const DP& c, const DP& d) {
+    const DP* const p[4] = {&a, &b, &c, &d};
+    BigInt q[3][3];
+    big_diffs<4>(p, q);
+    return big_det3(q[0], q[1], q[2]).sign;
+}
+
+int insphere_exact(const DP& a, const DP& b, const DP& c, const DP& d, const DP& e) {
+    const DP* const p[5] = {&a, &b, &c, &d, &e};
+    BigInt q[4][3];
+    big_diffs<5>(p, q);
+    BigInt l[4];
+    for (int i = 0; i < 4; ++i) l[i] = big_add(big_add(big_mul(q[i][0], q[i][0]), big_mul(q[i][1], q[i][1])), big_mul(q[i][2], q[i][2]));
+    const BigInt m_bcd = big_det3(q[1], q[2], q[3]), m_acd = big_det3(q[0], q[2], q[3]);
+    const BigInt m_abd = big_det3(q[0], q[1], q[3]), m_abc = big_det3(q[0], q[1], q[2]);
+    // the cofactor expansion of insphere_i
+    const BigInt r = big_sub(big_add(big_sub(big_mul(l[1], m_acd), big_mul(l[0], m_bcd)), big_mul(l[3], m_abc)), big_mul(l[2], m_abd));
+    return r.sign;
+}
+
+// Filtered predicates on doubles: the determinant in double from rounded differences. The bound
+// 1e-14 * permanent (~45 eps) covers the rounding of the differences as well (Shewchuk 1997 bounds
+// this evaluation order by 7 eps for orientation and 16 eps for the in-sphere test); a permanent
+// small enough for underflow to matter also goes to the exact evaluation.
+constexpr double kTinyPermanent = 1e-250;
+
+inline int orient_sgn(const DP& a, const DP& b, const DP& c, const DP& d) {
+    const double ax = a.x - d.x, ay = a.y - d.y, az = a.z - d.z;
+    const double bx = b.x - d.x, by = b.y - d.y, bz = b.z - d.z;
+    const double cx = c.x - d.x, cy = c.y - d.y, cz = c.z - d.z;
+    const double det = ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx);
+    const double perm = std::fabs(ax) * (std::fabs(by * cz) + std::fabs(bz * cy)) + std::fabs(ay) * (std::fabs(bx * cz) + std::fabs(bz * cx)) +
+                        std::fabs(az) * (std::fabs(bx * cy) + std::fabs(by * cx));
+    const double bound = 1e-14 * perm;
+    if (perm > kTinyPermanent) {
+        if (det > bound) return 1;
+        if (det < -bound) return -1;
+    }
+    return orient_exact(a, b, c, d);
+}
+
+inline int insphere_sgn(const DP& a, const DP& b, const DP& c, const DP& d, const DP& e) {
+    const double ax = a.x - e.x, ay = a.y - e.y, az = a.z - e.z;
+    const double bx = b.x - e.x, by = b.y - e.y, bz = b.z - e.z;
+    const double cx = c.x - e.x, cy = c.y - e.y, cz = c.z - e.z;
+    const double dx = d.x - e.x, dy = d.y - e.y, dz = d.z - e.z;
+    const double la = ax * ax + ay * ay + az * az, lb = bx * bx + by * by + bz * bz;
+    const double lc = cx * cx + cy * cy + cz * cz, ld = dx * dx + dy * dy + dz * dz;
+    auto det3d = [](double px, double py, double pz, double qx, double qy, double qz, double rx, double ry, double rz, double& perm) {
+        perm = std::fabs(px) * (std::fabs(qy * rz) + std::fabs(qz * ry)) + std::fabs(py) * (std::fabs(qx * rz) + std::fabs(qz * rx)) +
+               std::fabs(pz) * (std::fabs(qx * ry) + std::fabs(qy * rx));
+        return px * (qy * rz - qz * ry) - py * (qx * rz - qz * rx) + pz * (qx * ry - qy * rx);
+    };
+    double p_bcd, p_acd, p_abd, p_abc;
+    const double m_bcd = det3d(bx, by, bz, cx, cy, cz, dx, dy, dz, p_bcd);
+    const double m_acd = det3d(ax, ay, az, cx, cy, cz, dx, dy, dz, p_acd);
+    const double m_abd = det3d(ax, ay, az, bx, by, bz, dx, dy, dz, p_abd);
+    const double m_abc = det3d(ax, ay, az, bx, by, bz, cx, cy, cz, p_abc);
+    const double det = lb * m_acd - la * m_bcd + ld * m_abc - lc * m_abd;
+    const double perm = lb * p_acd + la * p_bcd + ld * p_abc + lc * p_abd;
+    const double bound = 1e-14 * perm;
+    if (perm > kTinyPermanent) {
+        if (det > bound) return 1;
+        if (det < -bound) return -1;
+    }
+    return insphere_exact(a, b, c, d, e);
+}
+
+inline bool same_pt(const IP& a, const IP& b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+inline bool same_pt(const DP& a, const DP& b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+
 inline uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
     v &= 0x1fffffULL;
     v = (v | (v << 32)) & 0x1f00000000ffffULL;
@@ -204,29 +425,13 @@ Mesh make_jitter_cube(int n, uint64_t seed, double jitter) {
 }
 
 // ---------------------------------------------------------------- Delaunay
-std::string delaunay(Mesh& mesh) {
-    const int64_t N = mesh.n_tot();
-    if (N < 4) return "delaunay: fewer than four vertices";
-    if (N > (int64_t)0x7ffffff0) return "delaunay: too many vertices for 32-bit ids";
-    std::vector<IP> P(N + 4);
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int64_t v = 0; v < N; ++v) {
-        const double* p = &mesh.pos[3 * v];
-        for (int c = 0; c < 3; ++c) {
-            lo[c] = std::min(lo[c], p[c]);
-            hi[c] = std::max(hi[c], p[c]);
-            if (!(std::fabs(p[c]) < 8.0)) return "delaunay: coordinates must lie within [-8, 8]";
-        }
-        P[v] = to_ip(p);
-    }
-    const double size = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
-    const double cen[3] = {0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2])};
-    const double dirs[4][3] = {{1, 1, 1}, {1, -1, -1}, {-1, 1, -1}, {-1, -1, 1}};
-    for (int s = 0; s < 4; ++s) {
-        const double q[3] = {cen[0] + 10.0 * size * dirs[s][0], cen[1] + 10.0 * size * dirs[s][1], cen[2] + 10.0 * size * dirs[s][2]};
-        P[N + s] = to_ip(q);
-    }
+namespace {
 
+// Bowyer-Watson insertion over the points P (the mesh's vertices, then the four super vertices)
+// with the exact predicates of their type.
+template <typename Pt>
+std::string bowyer_watson(Mesh& mesh, const std::vector<Pt>& P, const double lo[3], const double hi[3], double size) {
+    const int64_t N = mesh.n_tot();
     std::vector<std::array<int32_t, 4>> tv, ta;
     std::vector<uint8_t> alive, incav;
     std::vector<int32_t> freel;
@@ -250,7 +455,7 @@ std::string delaunay(Mesh& mesh) {
     }
     std::sort(order.begin(), order.end());
 
-    auto tet_pts = [&](int32_t t, IP q[4]) {
+    auto tet_pts = [&](int32_t t, Pt q[4]) {
         for (int c = 0; c < 4; ++c) q[c] = P[tv[t][c]];
     };
 
@@ -263,10 +468,10 @@ std::string delaunay(Mesh& mesh) {
     std::vector<int32_t> newt;
     int32_t last = 0;
     unsigned turn = 0;
-    IP q[4];
+    Pt q[4];
     for (int64_t oi = 0; oi < N; ++oi) {
         const int32_t vid = order[oi].second;
-        const IP p = P[vid];
+        const Pt p = P[vid];
         // locate by a visibility walk; fall back to a scan if the walk runs long
         int32_t t = last;
         int64_t steps = 0;
@@ -302,10 +507,8 @@ std::string delaunay(Mesh& mesh) {
             }
             if (!moved) break;
         }
-        for (int k = 0; k < 4; ++k) {
-            const IP& w = P[tv[t][k]];
-            if (w.x == p.x && w.y == p.y && w.z == p.z) return "delaunay: duplicate vertex";
-        }
+        for (int k = 0; k < 4; ++k)
+            if (same_pt(P[tv[t][k]], p)) return "delaunay: duplicate vertex";
         // cavity: tetrahedra whose circumsphere strictly contains p
         cav.clear();
         cav.push_back(t);
@@ -445,6 +648,48 @@ std::string delaunay(Mesh& mesh) {
     const double hull = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
     if (std::fabs(vol - hull) > 1e-9 * hull) return "delaunay: tetrahedra do not fill the bounding box (hull is not a box)";
     return "";
+}
+
+}  // namespace
+
+// Vertices on the 2^-18 lattice within the range of the 128-bit predicates (the generated cubes)
+// take the integer predicates; any other finite coordinates the filtered double predicates with an
+// exact fallback. Both give the exact signs, so the same input gives the same tetrahedra.
+std::string delaunay(Mesh& mesh) {
+    const int64_t N = mesh.n_tot();
+    if (N < 4) return "delaunay: fewer than four vertices";
+    if (N > (int64_t)0x7ffffff0) return "delaunay: too many vertices for 32-bit ids";
+    constexpr double kMaxBoxLattice = 1.75;  // the integer predicates' range (with the super vertices)
+    constexpr double kMaxCoord = 1e50;       // double predicates: products of degree 5 stay finite
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    bool lattice = true;
+    for (int64_t v = 0; v < N; ++v)
+        for (int c = 0; c < 3; ++c) {
+            const double x = mesh.pos[3 * v + c];
+            if (!(std::fabs(x) <= kMaxCoord)) return "delaunay: coordinates must be finite and within 1e50 in magnitude";
+            lo[c] = std::min(lo[c], x);
+            hi[c] = std::max(hi[c], x);
+            const double q = std::ldexp(x, kQuantBits);
+            if (q != std::nearbyint(q) || !(std::fabs(x) < 8.0)) lattice = false;
+        }
+    for (int c = 0; c < 3; ++c)
+        if (hi[c] - lo[c] > kMaxBoxLattice) lattice = false;
+    const double size = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
+    const double cen[3] = {0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2])};
+    const double dirs[4][3] = {{1, 1, 1}, {1, -1, -1}, {-1, 1, -1}, {-1, -1, 1}};
+    double sup[4][3];
+    for (int s = 0; s < 4; ++s)
+        for (int c = 0; c < 3; ++c) sup[s][c] = cen[c] + 10.0 * size * dirs[s][c];
+    if (lattice) {
+        std::vector<IP> P(N + 4);
+        for (int64_t v = 0; v < N; ++v) P[v] = to_ip(&mesh.pos[3 * v]);
+        for (int s = 0; s < 4; ++s) P[N + s] = to_ip(sup[s]);
+        return bowyer_watson(mesh, P, lo, hi, size);
+    }
+    std::vector<DP> P(N + 4);
+    for (int64_t v = 0; v < N; ++v) P[v] = DP{mesh.pos[3 * v], mesh.pos[3 * v + 1], mesh.pos[3 * v + 2]};
+    for (int s = 0; s < 4; ++s) P[N + s] = DP{sup[s][0], sup[s][1], sup[s][2]};
+    return bowyer_watson(mesh, P, lo, hi, size);
 }
 
 // ---------------------------------------------------------------- Voronoi dual

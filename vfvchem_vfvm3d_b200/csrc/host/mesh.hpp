@@ -63,8 +63,10 @@ struct Dual {
 // point in (k, j, i) order with i fastest.
 Mesh make_jitter_cube(int n, uint64_t seed, double jitter);
 
-// Delaunay tetrahedralisation by Bowyer-Watson insertion with exact integer predicates.
-// Fills mesh.tets. Returns an empty string on success, else the error message.
+// Delaunay tetrahedralisation by Bowyer-Watson insertion with exact predicates: integer ones for
+// vertices on the 2^-18 lattice within a box of 1.75 (the generated cubes), filtered double ones
+// with an exact big-integer fallback for any other finite coordinates. Fills mesh.tets. Returns an
+// empty string on success, else the error message.
 std::string delaunay(Mesh& mesh);
 
 // Voronoi dual of the tetrahedralisation (geom_tet.rs:122-293). Returns "" on success. The face

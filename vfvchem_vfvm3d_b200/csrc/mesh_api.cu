@@ -45,25 +45,13 @@ int vfv_mesh_from_vertices(int64_t n_pts, int64_t n_nds, const double* pos, cons
     if (!out || !pos || (n_nds > 0 && !node_bnd)) return set_err(nullptr, VFV_BAD_INPUT, "NULL argument");
     *out = nullptr;
     if (n_pts < 0 || n_nds < 0 || n_pts + n_nds < 4) return set_err(nullptr, VFV_BAD_INPUT, "need at least four vertices");
-    // The Delaunay predicates are exact integer arithmetic on the 2^-18 lattice, within the range
-    // that a bounding box of at most kMaxBoxExtent per axis (plus the super-tetrahedron) spans;
-    // anything else would be rounded or overflow silently, so it is refused.
-    constexpr double kMaxBoxExtent = 1.75;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    // The Delaunay predicates are exact for any finite coordinates (integer arithmetic on the 2^-18
+    // lattice for the generated cubes, filtered double arithmetic with an exact fallback otherwise);
+    // magnitudes are bounded so that the filters' degree-5 products stay finite.
     for (int64_t v = 0; v < n_pts + n_nds; ++v)
-        for (int c = 0; c < 3; ++c) {
-            const double x = pos[3 * v + c];
-            const double q = std::ldexp(x, kQuantBits);
-            if (!std::isfinite(x) || q != std::nearbyint(q))
-                return set_err(nullptr, VFV_BAD_INPUT, "vertex " + std::to_string(v) + ": coordinates must be finite multiples of 2^-" +
-                                                           std::to_string(kQuantBits) + " (round them to that lattice first)");
-            lo[c] = std::min(lo[c], x);
-            hi[c] = std::max(hi[c], x);
-        }
-    for (int c = 0; c < 3; ++c)
-        if (hi[c] - lo[c] > kMaxBoxExtent)
-            return set_err(nullptr, VFV_BAD_INPUT, "the vertices' bounding box exceeds 1.75 on an axis: scale the domain into a box of at "
-                                                   "most that size");
+        for (int c = 0; c < 3; ++c)
+            if (!(std::fabs(pos[3 * v + c]) <= 1e50))
+                return set_err(nullptr, VFV_BAD_INPUT, "vertex " + std::to_string(v) + ": coordinates must be finite and within 1e50 in magnitude");
     auto* mh = new vfv_mesh();
     mh->m.n_pts = n_pts;
     mh->m.n_nds = n_nds;
