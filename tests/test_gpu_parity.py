@@ -502,3 +502,20 @@ def test_larger_mesh_properties(gpu_ctx):
     assert np.max(np.abs(x - pos[:, 0])) < 1e-8
     rp, ci, va = h.pattern.export()
     assert np.linalg.norm(oracle.spmv(rp.astype(np.int64), ci, va, x) - b) <= 1e-10 * np.linalg.norm(b)
+
+
+def test_host_solve_into_given_array(gpu_ctx, c1h_system, c1_hetero):
+    """Pattern.solve(..., out=) writes x into the caller's array (pinned memory here) with the same
+    bits as a new array; a wrong array is refused."""
+    import torch
+    from vfvchem_vfvm3d_b200 import GmresOptions, Pattern
+    (rp, ci, va), b, _ = c1h_system
+    p = Pattern.from_csr(gpu_ctx, rp.astype(np.int32), ci)
+    p.set_values(va)
+    o = GmresOptions(tol=1e-12, restart=30, max_outer=500, precond=2, precision=1, inner_rtol=1e-6)
+    x, _ = p.solve(b, c1_hetero.T0, o)
+    buf = torch.empty(c1_hetero.n, dtype=torch.float64).pin_memory().numpy()
+    x2, _ = p.solve(b, c1_hetero.T0, o, out=buf)
+    assert x2 is buf and np.array_equal(x, buf)
+    with pytest.raises(ValueError):
+        p.solve(b, c1_hetero.T0, o, out=np.empty(c1_hetero.n, np.float32))

@@ -169,12 +169,18 @@ class Pattern:
                                                        L.dptr(va)))
         return rp, ci, va
 
-    def solve(self, b: np.ndarray, x0: np.ndarray | None = None, opts: GmresOptions | None = None):
-        """Host-array solve (``vfv_solve``); returns (x, SolveInfo)."""
+    def solve(self, b: np.ndarray, x0: np.ndarray | None = None, opts: GmresOptions | None = None, out: np.ndarray | None = None):
+        """Host-array solve (``vfv_solve``); returns (x, SolveInfo). ``out``: a contiguous float64
+        array of n entries to receive x (e.g. in pinned memory), else a new array."""
         opts = opts or GmresOptions()
         b = np.ascontiguousarray(b, dtype=np.float64)
         x0 = np.zeros(self.n) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64)
-        x = np.empty(self.n)
+        if out is None:
+            x = np.empty(self.n)
+        else:
+            if out.dtype != np.float64 or out.shape != (self.n,) or not out.flags.c_contiguous or not out.flags.writeable:
+                raise ValueError("out must be a writeable contiguous float64 array of n entries")
+            x = out
         info = L.SolveInfo()
         o = opts.to_c()
         code = L.load().vfv_solve(self.ctx.handle, self._h, L.dptr(b), L.dptr(x0), L.dptr(x), C.byref(o), C.byref(info))
