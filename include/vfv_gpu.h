@@ -183,9 +183,9 @@ int vfv_ilu0_sweep_layout(const vfv_pattern* p, int ilu_order, int32_t* col_byte
  * from a fixed 2 MiB device array inside the library, so n is limited to 262,144 rows (larger
  * patterns are rejected with VFV_BAD_INPUT). The pattern's ILU(0) storage must already exist:
  * call vfv_ilu0_apply_device (or an ILU(0) solve) on it once first. The first call on each device
- * looks up the array's device address (make it before any stream capture). Every call synchronises
- * the context's stream before it returns. All calls in the process share the one array on a
- * device: calls that overlap on the GPU race. */
+ * looks up the array's device address. Every call synchronises the context's stream before it
+ * returns. All calls in the process share the one array on a device: calls that overlap on the GPU
+ * race. */
 int vfv_ilu0_apply_device_noalloc(vfv_ctx* ctx, vfv_pattern* p, int ilu_order, const double* r, double* z, int32_t* levels);
 /* the symmetric permutation the ILU(0) factor lives on: perm[n] (new -> old) and the row ranges of
  * its levels lev_ptr[nlev+1] (any pointer may be NULL; call once with NULLs to learn nlev) */
