@@ -173,3 +173,23 @@ def test_delaunay_of_cospherical_doubles_is_exact(lib_built):
     m = Mesh.from_vertices(pos, n_pts, bnd)
     _, _, tets = m.export()
     _exact_checks(pos, tets)
+
+
+def test_delaunay_of_ulp_perturbed_grid_is_exact(lib_built):
+    """Interior vertices of a 0.1-spaced grid moved by one ulp (the hull stays the box): every
+    circumsphere test is within rounding of zero, so the big-integer fallback decides nearly all of
+    them; the result is checked in rationals."""
+    from vfvchem_vfvm3d_b200 import Mesh
+    g = np.arange(5) * 0.1
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    p = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    rng = np.random.default_rng(21)
+    inner = np.all((p > 0) & (p < g[-1]), axis=1)
+    steps = rng.integers(-1, 2, size=(int(inner.sum()), 3))
+    q = p[inner]
+    q = np.where(steps > 0, np.nextafter(q, np.inf), np.where(steps < 0, np.nextafter(q, -np.inf), q))
+    p[inner] = q
+    pos, n_pts, bnd = _points_and_nodes(p)
+    m = Mesh.from_vertices(pos, n_pts, bnd)
+    _, _, tets = m.export()
+    _exact_checks(pos, tets)
