@@ -159,7 +159,10 @@ def test_delaunay_of_raw_doubles_equals_qhull(lib_built, scale, shift):
     vol = np.abs(np.einsum("ij,ij->i", a - d, np.cross(b - d, c - d)))
     st = st[vol > 1e-12 * vol.max()]
     assert _tetset(tets) == _tetset(st)
-    assert m.dual()["nbr_ptr"][-1] == m.n_dir  # the Voronoi dual builds on it
+    d = m.dual()  # the Voronoi dual builds on it: control volumes fill the box
+    assert d["nbr_ptr"][-1] == m.n_dir
+    box = np.prod(pos.max(0) - pos.min(0))
+    assert abs(d["cvol"].sum() - box) <= 1e-9 * box
 
 
 def test_delaunay_of_cospherical_doubles_is_exact(lib_built):
