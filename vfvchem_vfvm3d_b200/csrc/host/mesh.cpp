@@ -380,12 +380,6 @@ inline uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
 
 }  // namespace
 
-int orient_sign(const double* a, const double* b, const double* c, const double* d) {
-    return sgn(orient_i(to_ip(a), to_ip(b), to_ip(c), to_ip(d)));
-}
-int insphere_sign(const double* a, const double* b, const double* c, const double* d, const double* e) {
-    return sgn(insphere_i(to_ip(a), to_ip(b), to_ip(c), to_ip(d), to_ip(e)));
-}
 
 // ---------------------------------------------------------------- mesh generator
 Mesh make_jitter_cube(int n, uint64_t seed, double jitter) {

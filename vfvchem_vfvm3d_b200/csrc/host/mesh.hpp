@@ -79,10 +79,6 @@ std::string build_dual(const Mesh& mesh, Dual& dual, double piece_store_bytes = 
 // with the device dual. Returns "" on success.
 std::string boundary_subfaces(const Mesh& mesh, const std::vector<uint8_t>& bface, Dual& dual);
 
-// exact orientation / in-sphere signs on the quantised grid (exported for tests)
-int orient_sign(const double* a, const double* b, const double* c, const double* d);
-int insphere_sign(const double* a, const double* b, const double* c, const double* d, const double* e);
-
 constexpr int kQuantBits = 18;  // coordinates are multiples of 2^-18
 
 }  // namespace vfv
